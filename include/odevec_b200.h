@@ -1,0 +1,120 @@
+/* odevec_b200: C ABI of the B200 OdeVec solve path.
+ *
+ * This is the boundary a Fortran, C or Python caller binds in place of the
+ * reference's solver module src/odevec.F90.  Plain pointers and sizes only.
+ *
+ *   reference (src/odevec.F90)                     this ABI
+ *   InitOdevec(this)                  :94-154      odevec_init
+ *   this%RelativeTolerance, %AbsoluteTolerance,
+ *   %MinimalTimestep, %CheckNegatives  :48-52       odevec_opts
+ *   SolveODE(this,time,dt,t_stop,y,
+ *            GetRHS,GetJac,GetLU,Mask) :158-214     odevec_solve (device arrays)
+ *                                                  odevec_solve_host (host arrays)
+ *   CloseOdevec(this)                 :1058-1074   odevec_close
+ *   print + stop on failure   :114-124,272-287,380-390,585-597
+ *                                                  per-cell status codes below
+ *
+ * The network routines GetRHS/GetJac/GetLU are compiled into the library by
+ * the preprocessor (one "variant" per network, packaging and ordering) and
+ * chosen by name at odevec_init.
+ *
+ * Layout: y holds neq species of ncells cells, species-major ("structure of
+ * arrays"): y[s * ncells + c] -- the reference's y(nvector, neq) in Fortran
+ * column-major order.  t, dt, t_stop, mask and status have one entry per
+ * cell; stats has OV_NSTATS int32 entries per cell (cell-major).
+ *
+ * Cells are solved independently (group_size 1) or in lockstep groups of 32
+ * consecutive cells sharing time, step size, order and Jacobian decisions
+ * through max-norms over the group (group_size 32), which is the
+ * reference's semantics with nvector = 32.  A lockstep group needs equal t,
+ * dt and t_stop in all its cells. */
+#ifndef ODEVEC_B200_H
+#define ODEVEC_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- per-cell status (replaces the reference's `stop`) ---- */
+#define OV_OK 0
+#define OV_ERR_DTMIN_PREDICTOR 1 /* step below dt_min after a negative prediction, :272-275 :284-287 */
+#define OV_ERR_CONV_FAILURES 2   /* more than 10 Newton failures in one step, :380-383 */
+#define OV_ERR_DTMIN_CONV 3      /* step below dt_min after a Newton failure, :387-390 */
+#define OV_ERR_MAX_STEPS 4       /* predictor attempts exceeded opts.max_attempts (no reference counterpart) */
+#define OV_ERR_ORDER 5           /* impossible order change, :585-586 :596-597 */
+#define OV_ERR_GROUP_MISMATCH 6  /* lockstep group with differing t, dt or t_stop */
+
+/* ---- API return codes ---- */
+#define OV_API_OK 0
+#define OV_API_EINVAL (-1)      /* bad argument */
+#define OV_API_ENONET (-2)      /* unknown network variant */
+#define OV_API_ECUDA (-3)       /* CUDA runtime error (see odevec_last_error) */
+#define OV_API_ENOMEM (-4)      /* allocation failed */
+#define OV_API_EUNSUPPORTED (-5) /* option combination not compiled in */
+#define OV_API_ETOOBIG (-6)     /* more cells than the solver was created for */
+
+/* stats per cell: accepted steps, predictor attempts, error-test failures,
+   Newton failures, Newton iterations (right-hand-side evaluations in the
+   corrector), Jacobian+LU evaluations, final order, reserved */
+#define OV_NSTATS 8
+
+/* precision forms */
+#define OV_PREC_FP64 0     /* FP64 throughout, no fused multiply-add: same bits as the CPU oracle */
+#define OV_PREC_FP64_FMA 1 /* FP64 throughout with fused multiply-add */
+#define OV_PREC_FP32_LU 2  /* Jacobian LU and triangular solves in FP32 on the error-weight-scaled
+                              matrix; state, residual, norms and control in FP64 */
+
+typedef struct odevec_opts {
+    double rtol;              /* RelativeTolerance */
+    double atol;              /* AbsoluteTolerance */
+    double dt_min;            /* MinimalTimestep; negative: the variant's --dt_min */
+    int32_t check_negatives;  /* CheckNegatives */
+    int32_t group_size;       /* 1 or 32; 0: the variant's --nvector (1 if not 32) */
+    int32_t precision;        /* OV_PREC_* */
+    int32_t max_attempts;     /* cap on predictor attempts per cell or group; 0: 1000000 */
+} odevec_opts;
+
+typedef struct odevec_solver odevec_solver;
+
+/* network variants compiled into the library */
+int32_t odevec_num_networks(void);
+const char* odevec_network_tag(int32_t i);
+/* info: neq, nnz, nrea, dense, idx_tgas, default group size */
+int32_t odevec_network_info(const char* tag, int32_t* info);
+
+/* InitOdevec: create a solver for up to max_cells cells of one network variant
+   on the current CUDA device.  Allocates the device work counter and, for
+   odevec_solve_host, staging buffers for max_cells cells. */
+int32_t odevec_init(const char* network, int64_t max_cells, const odevec_opts* opts,
+                    odevec_solver** out);
+int32_t odevec_set_options(odevec_solver* s, const odevec_opts* opts);
+
+/* SolveODE on device arrays, asynchronous on `stream` (a cudaStream_t, NULL =
+   default stream).  y, t, dt are read and overwritten: on return t[c] =
+   t_stop[c], dt[c] = the last internal step, y = the solution at t_stop.
+   mask (nullable): cells with mask 0 are left untouched except t = t_stop.
+   status, stats: nullable outputs. */
+int32_t odevec_solve(odevec_solver* s, int64_t ncells, double* y, double* t, double* dt,
+                     const double* t_stop, const uint8_t* mask, int32_t* status, int32_t* stats,
+                     void* stream);
+
+/* SolveODE on host arrays: copies the inputs to the solver's device buffers,
+   solves, copies y, t, dt, status and stats back, and synchronises.  This is
+   the drop-in for a CPU caller such as the reference's Fortran drivers. */
+int32_t odevec_solve_host(odevec_solver* s, int64_t ncells, double* y, double* t, double* dt,
+                          const double* t_stop, const uint8_t* mask, int32_t* status,
+                          int32_t* stats);
+
+/* CloseOdevec */
+int32_t odevec_close(odevec_solver* s);
+
+/* message of the last failed call on this thread */
+const char* odevec_last_error(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* ODEVEC_B200_H */

@@ -1,0 +1,777 @@
+/* The OdeVec BDF integrator as one persistent CUDA kernel (sm_100a).
+ *
+ * One thread integrates one cell.  A warp is either 32 independent cells
+ * (G = 1: per-cell time, step, order and Jacobian decisions) or one lockstep
+ * group of 32 cells that share them through max-norms over the warp
+ * (G = 32: the reference's semantics with nvector = 32, reductions with
+ * __shfl_xor_sync).  The grid is persistent: idle lanes take the next cells
+ * from a global counter (warp-aggregated atomicAdd), so a warp keeps all 32
+ * lanes busy while cells of very different stiffness finish at different
+ * times.
+ *
+ * The reference's nested loops (src/odevec.F90: step loop :207, predictor
+ * retry loop :259, corrector loop :321) are flattened into a per-lane state
+ * machine.  Each trip of the kernel's main loop performs for every lane at
+ * most one predictor (with its Jacobian and LU), one right-hand-side
+ * evaluation and one Newton update, so lanes in different phases still
+ * execute the expensive right-hand side, solve and factorisation code
+ * together, and the cheap control code diverges.  The arithmetic per cell is
+ * that of src/odevec.F90 operation by operation; with --fmad=false it is
+ * bit-identical to the CPU oracle.
+ *
+ * Per-cell state lives in thread-local arrays with compile-time indices
+ * (Nordsieck history y_NS(0:5), en, en_old, error weights, packed LU);
+ * loops over the runtime order are unrolled to the maximum order with
+ * predicates so no array is indexed dynamically.  Small networks stay in
+ * registers; larger ones spill to local memory (L1).
+ *
+ * Every loop is bounded: at most max_attempts predictor attempts per cell
+ * (status OV_ERR_MAX_STEPS), at most 4 Newton iterations per attempt and 10
+ * consecutive Newton failures (OV_ERR_CONV_FAILURES), so a stiff or broken
+ * cell ends with a status code instead of holding the GPU. */
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "../../include/odevec_b200.h"
+#include "ov_common.h"
+#include "ov_launch.h"
+#include "rates_primordial.h"
+
+#ifndef OV_MODE_NS
+#error "OV_MODE_NS (the arithmetic-mode namespace) must be defined"
+#endif
+
+namespace ov {
+namespace OV_MODE_NS {
+
+constexpr int MAXQ = 5;           /* maxorder, pre_odevec.py:83 */
+constexpr unsigned FULL = 0xffffffffu;
+
+enum Phase : int {
+    PH_IDLE = 0,     /* no cell */
+    PH_START = 1,    /* cell loaded: initial right-hand side pending */
+    PH_PRED = 2,     /* next: predictor attempt */
+    PH_NEWTON = 3,   /* next: right-hand side + Newton update */
+    PH_RESTART = 4,  /* next: right-hand side at the predicted state (3 error-test failures) */
+    PH_DONE = 5,     /* finished (status says how) */
+    PH_EXHAUSTED = 6 /* no cells left */
+};
+
+/* Nordsieck l-vectors l(q, 0:q), q = 1..6 (src/odevec.F90:127-134) */
+static __constant__ double c_lcoef[7][7] = {
+    {0, 0, 0, 0, 0, 0, 0},
+    {1.0, 1.0, 0.0, 0.0, 0.0, 0.0, 0.0},
+    {2.0 / 3.0, 1.0, 1.0 / 3.0, 0.0, 0.0, 0.0, 0.0},
+    {6.0 / 11.0, 1.0, 6.0 / 11.0, 1.0 / 11.0, 0.0, 0.0, 0.0},
+    {12.0 / 25.0, 1.0, 7.0 / 10.0, 1.0 / 5.0, 1.0 / 50.0, 0.0, 0.0},
+    {60.0 / 137.0, 1.0, 225.0 / 274.0, 85.0 / 274.0, 15.0 / 274.0, 1.0 / 274.0, 0.0},
+    {20.0 / 49.0, 1.0, 58.0 / 63.0, 5.0 / 12.0, 25.0 / 252.0, 1.0 / 84.0, 1.0 / 1764.0}};
+
+__device__ __forceinline__ double lcoef(int q, int k) { return c_lcoef[q][k]; }
+
+/* tau (src/odevec.F90:1034-1054) */
+__device__ __forceinline__ double tau(int order, int order2)
+{
+    double faculty = 1.0;
+#pragma unroll
+    for (int i = 1; i <= MAXQ + 1; ++i)
+        if (i <= order)
+            faculty = faculty * i;
+    if (order - 1 == order2)
+        return (order2 + 1.0) / faculty;
+    return (order2 + 1.0) / (faculty * lcoef(order, order));
+}
+
+/* NaN and masked-out values never win a max (as the oracle's comparison loop) */
+__device__ __forceinline__ double max_operand(double v) { return v > -HUGE_VAL ? v : -HUGE_VAL; }
+
+template <int G>
+__device__ __forceinline__ double group_max(double v)
+{
+    v = max_operand(v);
+    if (G == 32) {
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1)
+            v = fmax(v, __shfl_xor_sync(FULL, v, o));
+    }
+    return v;
+}
+
+template <int G>
+__device__ __forceinline__ bool group_any(bool b)
+{
+    if (G == 32)
+        return __any_sync(FULL, b);
+    return b;
+}
+
+template <class Net, int G, class LUT>
+struct Cell {
+    static constexpr int N = Net::NEQ;
+    static constexpr int NNZ = Net::NNZ;
+    static constexpr int NR = Net::NREA > 0 ? Net::NREA : 1;
+    static constexpr bool SCALED = sizeof(LUT) == 4;
+
+    double yns[MAXQ + 1][N];
+    double en[N], eno[N], w2[N], y[N], f[N];
+    LUT a[NNZ];
+    double rT[NR];
+    double sc[SCALED ? N : 1], isc[SCALED ? N : 1];
+
+    double t, h, told, tstop, crate, jchg, cerr;
+    int q, swu, lju, fet, fc, it;
+    bool ujac, nuo, first, msk;
+    int status, attempts, steps, ltef, convf, newt, jacs;
+
+    /* WeightedNorm1 (src/odevec.F90:669-684) */
+    __device__ __forceinline__ double wnorm(const double* e) const
+    {
+        double s = 0.0;
+#pragma unroll
+        for (int j = 0; j < N; ++j)
+            s = s + e[j] * e[j] * w2[j];
+        double v = msk ? sqrt(s / N) : -HUGE_VAL;
+        return group_max<G>(v);
+    }
+
+    /* WeightedNorm2 of y_NS(:,:,col) for a runtime column */
+    __device__ __forceinline__ double wnorm_ns(int col) const
+    {
+        double s = 0.0;
+#pragma unroll
+        for (int j = 0; j < N; ++j) {
+            double e = 0.0;
+#pragma unroll
+            for (int k = 0; k <= MAXQ; ++k)
+                if (k == col)
+                    e = yns[k][j];
+            s = s + e * e * w2[j];
+        }
+        double v = msk ? sqrt(s / N) : -HUGE_VAL;
+        return group_max<G>(v);
+    }
+
+    /* CalcErrorWeightInvSquared (src/odevec.F90:706-716) */
+    __device__ __forceinline__ void weights(double rtol, double atol)
+    {
+#pragma unroll
+        for (int j = 0; j < N; ++j) {
+            double w = 1.0 / (rtol * fabs(y[j]) + atol);
+            w2[j] = w * w;
+        }
+    }
+
+    /* PredictSolution (src/odevec.F90:769-793) */
+    __device__ __forceinline__ void predict()
+    {
+#pragma unroll
+        for (int l = 0; l < MAXQ; ++l)
+#pragma unroll
+            for (int k = MAXQ; k >= 1; --k)
+                if (l <= q - 1 && k <= q && k >= l + 1) {
+#pragma unroll
+                    for (int j = 0; j < N; ++j)
+                        yns[k - 1][j] = yns[k][j] + yns[k - 1][j];
+                }
+#pragma unroll
+        for (int j = 0; j < N; ++j)
+            en[j] = 0.0;
+    }
+
+    /* ResetSystem (src/odevec.F90:526-544) */
+    __device__ __forceinline__ void reset()
+    {
+#pragma unroll
+        for (int k = 0; k < MAXQ; ++k)
+#pragma unroll
+            for (int jj = MAXQ; jj >= 1; --jj)
+                if (k <= q - 1 && jj <= q && jj >= k + 1) {
+#pragma unroll
+                    for (int j = 0; j < N; ++j)
+                        yns[jj - 1][j] = yns[jj - 1][j] - yns[jj][j];
+                }
+    }
+
+    /* SetStepSize (src/odevec.F90:720-743) */
+    __device__ __forceinline__ void set_step(double dt_scale)
+    {
+        double dtt = 1.0;
+#pragma unroll
+        for (int k = 1; k <= MAXQ; ++k)
+            if (k <= q) {
+                dtt = dt_scale * dtt;
+#pragma unroll
+                for (int j = 0; j < N; ++j)
+                    yns[k][j] = yns[k][j] * dtt;
+            }
+        h = h * dt_scale;
+        jchg = jchg * dt_scale;
+    }
+
+    /* UpdateNordsieck (src/odevec.F90:747-765) */
+    __device__ __forceinline__ void update_nordsieck()
+    {
+#pragma unroll
+        for (int k = 0; k <= MAXQ; ++k)
+            if (k <= q) {
+                const double c = lcoef(q, k);
+#pragma unroll
+                for (int j = 0; j < N; ++j)
+                    yns[k][j] = yns[k][j] + en[j] * c;
+            }
+    }
+
+    /* CalcStepSizeOrder (src/odevec.F90:547-618); returns dt_scale.  The
+       literals 1.3, 1.2, 1.4 and 1.1 are single precision in the reference. */
+    __device__ __forceinline__ double step_size_order()
+    {
+        const int order = q;
+        double down, same, up;
+        if (order == 1)
+            down = 0.0;
+        else
+            down = 1.0 / ((double)1.3f * ov_pow(wnorm_ns(order) / tau(order, order - 1), 1.0 / order)
+                          + 1e-6);
+        same = 1.0 / ((double)1.2f * ov_pow(wnorm(en) / tau(order, order), 1.0 / (order + 1.0)) + 1e-6);
+        if (order == MAXQ || nuo)
+            up = 0.0;
+        else {
+            double d[N];
+#pragma unroll
+            for (int j = 0; j < N; ++j)
+                d[j] = en[j] - eno[j];
+            up = 1.0 / ((double)1.4f * ov_pow(wnorm(d) / tau(order, order + 1), 1.0 / (order + 2.0))
+                        + 1e-6);
+        }
+        int loc = 1;
+        double mx = down;
+        if (same > mx) { mx = same; loc = 2; }
+        if (up > mx) { mx = up; loc = 3; }
+        double s = mx;
+        if (s >= (double)1.1f) {
+            if (loc == 1) {
+                if (order != 1)
+                    q = order - 1;
+                else
+                    status = OV_ERR_ORDER;
+            } else if (loc == 2) {
+                s = same;
+            } else {
+                if (order != MAXQ) {
+                    const double c = lcoef(order, order);
+#pragma unroll
+                    for (int k = 2; k <= MAXQ; ++k)
+                        if (k == order + 1) {
+#pragma unroll
+                            for (int j = 0; j < N; ++j)
+                                yns[k][j] = c * en[j] / (order + 1.0);
+                        }
+                    q = order + 1;
+                } else
+                    status = OV_ERR_ORDER;
+            }
+        } else {
+            s = same;
+        }
+        double upper;
+        if (first) {
+            upper = 1e4;
+            first = false;
+        } else
+            upper = 10.0;
+        s = upper < s ? upper : s;
+        jchg = jchg * s;
+        swu = 0;
+        nuo = false;
+        return s;
+    }
+
+    /* CheckConvergence (src/odevec.F90:622-665), den in d */
+    __device__ __forceinline__ void check_convergence(const double* d, bool& failed, bool& converged)
+    {
+        const double err = wnorm(d);
+        double rate_tmp = 0.0;
+        if (it != 0) {
+            rate_tmp = err / cerr;
+            crate = fmax(0.2 * crate, rate_tmp);
+        }
+        const double r15 = 1.5 * crate;
+        const double crit = err * (1.0 < r15 ? 1.0 : r15) / (tau(q, q) / (2.0 * (q + 2.0)));
+        bool nan = false;
+#pragma unroll
+        for (int j = 0; j < N; ++j)
+            nan |= (d[j] != d[j]) | (w2[j] != w2[j]);
+        if (group_any<G>(nan)) {
+            failed = true;
+            return;
+        }
+        if (crit < 1.0) {
+            converged = true;
+            return;
+        }
+        if (it >= 2 && crate > 2.0 * rate_tmp)
+            failed = true;
+        else if (it == 3)
+            failed = true;
+        else {
+            failed = false;
+            cerr = err;
+            it = it + 1;
+        }
+    }
+
+    __device__ __forceinline__ bool any_negative_yns0() const
+    {
+        bool neg = false;
+#pragma unroll
+        for (int j = 0; j < N; ++j)
+            neg |= yns[0][j] < 0.0;
+        return group_any<G>(msk && neg);
+    }
+
+    __device__ __forceinline__ bool any_negative_y() const
+    {
+        bool neg = false;
+#pragma unroll
+        for (int j = 0; j < N; ++j)
+            neg |= y[j] < 0.0;
+        return group_any<G>(msk && neg);
+    }
+
+    /* GetJac + LUDecompose (src/odevec.F90:301-315) */
+    __device__ __forceinline__ void jacobian_lu()
+    {
+        double k[NR];
+        Net::rates_k(y, rT, k);
+        if constexpr (!SCALED) {
+            Net::jac(y, k, lcoef(q, 0), h, a);
+        } else {
+            /* scale by powers of two close to the error weights (exact in
+               FP64), then round to FP32 */
+#pragma unroll
+            for (int j = 0; j < N; ++j) {
+                int e = (int)((ov_d2bits(w2[j]) >> 52) & 0x7ff) - 1023;
+                int hexp = e >= 0 ? e / 2 : -((-e + 1) / 2);
+                hexp = hexp > 480 ? 480 : (hexp < -480 ? -480 : hexp);
+                sc[j] = ov_pow2i(hexp);
+                isc[j] = ov_pow2i(-hexp);
+            }
+            double P[NNZ];
+            Net::jac(y, k, lcoef(q, 0), h, P);
+            Net::template store_scaled<LUT>(P, a, sc, isc);
+        }
+        Net::template lu_factor<LUT>(a);
+    }
+
+    /* residual, solve, Newton update (src/odevec.F90:323-352) */
+    __device__ __forceinline__ void newton_update(double* den)
+    {
+        double res[N];
+#pragma unroll
+        for (int j = 0; j < N; ++j)
+            res[j] = h * f[j] - (yns[1][j] + en[j]);
+        if constexpr (SCALED)
+            Net::template lu_solve<LUT>(a, res, den, sc, isc);
+        else
+            Net::template lu_solve<LUT>(a, res, den, nullptr, nullptr);
+        const double l0 = lcoef(q, 0);
+#pragma unroll
+        for (int j = 0; j < N; ++j) {
+            en[j] = en[j] + den[j];
+            if (msk)
+                y[j] = yns[0][j] + l0 * en[j];
+        }
+    }
+
+    /* CalcInitialStepSize (src/odevec.F90:216-238), f holds f(y) */
+    __device__ __forceinline__ double initial_step(double rtol, double atol)
+    {
+        weights(rtol, atol);
+        const double tol = rtol;
+        const double W0 = fabs(t) > fabs(tstop) ? fabs(t) : fabs(tstop);
+        double s = 0.0;
+#pragma unroll
+        for (int j = 0; j < N; ++j)
+            s = s + f[j] * f[j] * (w2[j] * tol * tol);
+        const double mx = group_max<G>(msk ? s : -HUGE_VAL);
+        const double d = sqrt(tol / (1.0 / (W0 * W0) + mx / N));
+        const double span = fabs(tstop - t);
+        return d < span ? d : span;
+    }
+
+    /* InterpolateSolution (src/odevec.F90:998-1030) */
+    __device__ __forceinline__ void interpolate()
+    {
+        const double rel_t = (tstop - t) / h;
+#pragma unroll
+        for (int j = 0; j < N; ++j) {
+            double acc = 0.0;
+#pragma unroll
+            for (int k = 0; k <= MAXQ; ++k)
+                if (k == q)
+                    acc = yns[k][j];
+#pragma unroll
+            for (int k = MAXQ - 1; k >= 0; --k)
+                if (k < q)
+                    acc = yns[k][j] + rel_t * acc;
+            if (msk)
+                y[j] = acc;
+        }
+    }
+};
+
+template <class Net, int G, class LUT>
+__global__ void __launch_bounds__(128) bdf_kernel(const LaunchArgs A)
+{
+    using C = Cell<Net, G, LUT>;
+    constexpr int N = C::N;
+    const int lane = threadIdx.x & 31;
+    const int64_t ncells = A.ncells;
+
+    C c;
+    int ph = PH_IDLE;
+    int64_t cell = -1;
+    bool write_y = false;
+
+    for (;;) {
+        /* ---- 1. idle lanes take new cells ---------------------------- */
+        if (G == 1) {
+            const unsigned need = __ballot_sync(FULL, ph == PH_IDLE);
+            if (need) {
+                const int leader = __ffs(need) - 1;
+                unsigned long long base = 0;
+                if (lane == leader)
+                    base = atomicAdd(A.queue, (unsigned long long)__popc(need));
+                base = __shfl_sync(FULL, base, leader);
+                if (ph == PH_IDLE) {
+                    cell = (int64_t)(base + __popc(need & ((1u << lane) - 1u)));
+                    ph = cell < ncells ? PH_START : PH_EXHAUSTED;
+                }
+            }
+            if (__all_sync(FULL, ph == PH_EXHAUSTED))
+                break;
+        } else {
+            if (ph == PH_IDLE) { /* warp-uniform */
+                unsigned long long g = 0;
+                if (lane == 0)
+                    g = atomicAdd(A.queue, 1ull);
+                g = __shfl_sync(FULL, g, 0);
+                cell = (int64_t)g * 32 + lane;
+                ph = (int64_t)g * 32 < ncells ? PH_START : PH_EXHAUSTED;
+            }
+            if (ph == PH_EXHAUSTED)
+                break;
+        }
+
+        /* ---- load + SolveODE set-up (src/odevec.F90:169-198) --------- */
+        if (ph == PH_START) {
+#pragma unroll
+            for (int j = 0; j < N; ++j)
+                c.y[j] = A.y[(int64_t)j * ncells + cell];
+            c.t = A.t[cell];
+            c.h = A.dt[cell];
+            c.tstop = A.t_stop[cell];
+            c.msk = A.mask ? (A.mask[cell] != 0) : true;
+            c.status = OV_OK;
+            c.attempts = c.steps = c.ltef = c.convf = c.newt = c.jacs = 0;
+            c.first = true;
+            c.q = 1;
+            c.swu = 0;
+            c.crate = 0.7;
+            c.jchg = 0.0;
+            c.nuo = false;
+            c.fet = 0;
+            c.fc = 0;
+            c.ujac = true;
+            c.lju = 0;
+            c.cerr = 0.0;
+            c.it = 0;
+#pragma unroll
+            for (int k = 0; k <= MAXQ; ++k)
+#pragma unroll
+                for (int j = 0; j < N; ++j)
+                    c.yns[k][j] = 0.0;
+#pragma unroll
+            for (int j = 0; j < N; ++j)
+                c.eno[j] = 0.0;
+            write_y = false;
+            bool skip = !group_any<G>(c.msk);
+            if (G == 32) {
+                const bool bad = c.t != __shfl_sync(FULL, c.t, 0) || c.h != __shfl_sync(FULL, c.h, 0)
+                                 || c.tstop != __shfl_sync(FULL, c.tstop, 0);
+                if (__any_sync(FULL, bad)) {
+                    c.status = OV_ERR_GROUP_MISMATCH;
+                    ph = PH_DONE;
+                }
+            }
+            if (ph == PH_START) {
+                c.weights(A.rtol, A.atol);
+                if (skip) {
+                    c.t = c.tstop; /* src/odevec.F90:187-191 */
+                    ph = PH_DONE;
+                } else {
+                    if (Net::NREA > 0)
+                        Net::rates_T(c.y, c.rT);
+#pragma unroll
+                    for (int j = 0; j < N; ++j)
+                        c.yns[0][j] = c.y[j];
+                }
+            }
+        }
+
+        /* ---- 2. predictor attempt (src/odevec.F90:259-315) ----------- */
+        if (ph == PH_PRED) {
+            if (++c.attempts > A.max_attempts) {
+                c.status = OV_ERR_MAX_STEPS;
+                ph = PH_DONE;
+            } else {
+                c.t = c.t + c.h;
+                c.predict();
+                if (A.check_neg && c.any_negative_yns0()) {
+                    c.t = c.told;
+                    c.reset();
+                    c.set_step(0.25);
+                    if (c.h <= A.dt_min) {
+                        c.status = OV_ERR_DTMIN_PREDICTOR;
+                        ph = PH_DONE;
+                    }
+                    /* else: another predictor attempt on the next trip */
+                } else {
+                    if (c.msk) {
+#pragma unroll
+                        for (int j = 0; j < N; ++j)
+                            c.y[j] = c.yns[0][j];
+                    }
+                    if (c.ujac) {
+                        c.jacobian_lu();
+                        c.jacs++;
+                        c.ujac = false;
+                        c.lju = 0;
+                        c.crate = 0.7;
+                        c.jchg = 1.0;
+                    }
+                    c.it = 0;
+                    ph = PH_NEWTON;
+                }
+            }
+        }
+
+        /* ---- 3. right-hand side ------------------------------------- */
+        if (ph == PH_START || ph == PH_NEWTON || ph == PH_RESTART) {
+            double k[C::NR];
+            Net::rates_k(c.y, c.rT, k);
+            Net::rhs(c.y, k, c.f);
+        }
+
+        /* ---- 4. consume it ------------------------------------------ */
+        if (ph == PH_START) {
+            /* src/odevec.F90:201-210 */
+#pragma unroll
+            for (int j = 0; j < N; ++j)
+                c.yns[1][j] = c.h * c.f[j];
+            c.h = c.initial_step(A.rtol, A.atol);
+            if (c.t < c.tstop) {
+                c.told = c.t;
+                ph = PH_PRED;
+            } else {
+                write_y = true;
+                c.interpolate();
+                c.t = c.tstop;
+                ph = PH_DONE;
+            }
+        } else if (ph == PH_RESTART) {
+            /* src/odevec.F90:417-421, 434-439 */
+#pragma unroll
+            for (int j = 0; j < N; ++j)
+                c.yns[1][j] = c.h * c.f[j];
+            c.ujac = true;
+            const double s = c.step_size_order();
+            if (c.status) {
+                ph = PH_DONE;
+            } else {
+                c.set_step(s);
+                c.fet++;
+                ph = PH_PRED;
+            }
+        } else if (ph == PH_NEWTON) {
+            c.newt++;
+            double den[N];
+            c.newton_update(den);
+            bool failed = false, converged = false;
+            c.check_convergence(den, failed, converged);
+            if (A.check_neg && c.any_negative_y()) {
+                failed = true;
+                converged = false;
+            }
+            if (failed && !converged) {
+                /* src/odevec.F90:375-393 */
+                c.t = c.told;
+                c.fc++;
+                c.convf++;
+                if (c.fc > 10) {
+                    c.status = OV_ERR_CONV_FAILURES;
+                    ph = PH_DONE;
+                } else {
+                    c.it = 0;
+                    c.reset();
+                    c.set_step(0.25);
+                    if (c.h < A.dt_min) {
+                        c.status = OV_ERR_DTMIN_CONV;
+                        ph = PH_DONE;
+                    } else {
+                        c.ujac = true;
+                        ph = PH_PRED;
+                    }
+                }
+            } else if (converged) {
+                c.fc = 0;
+                /* local truncation error test (src/odevec.F90:400-455) */
+                const double error = c.wnorm(c.en) / tau(c.q, c.q);
+                c.weights(A.rtol, A.atol);
+                if (error > 1.0) {
+                    c.ltef++;
+                    if (c.fet >= 3) {
+                        c.t = c.told;
+                        c.q = 1;
+                        if (c.msk) {
+#pragma unroll
+                            for (int j = 0; j < N; ++j)
+                                c.y[j] = c.yns[0][j];
+                        }
+                        ph = PH_RESTART;
+                    } else {
+                        c.t = c.told;
+                        c.reset();
+                        c.ujac = true;
+                        c.swu = 0;
+                        c.nuo = true;
+                        const double s = c.step_size_order();
+                        if (c.status) {
+                            ph = PH_DONE;
+                        } else {
+                            c.set_step(s);
+                            c.fet++;
+                            ph = PH_PRED;
+                        }
+                    }
+                } else {
+                    c.swu++;
+                    c.lju++;
+                    c.update_nordsieck();
+                    if (c.swu == c.q + 1) {
+                        const double s = c.step_size_order();
+                        if (!c.status)
+                            c.set_step(s);
+                    }
+                    if (c.status) {
+                        ph = PH_DONE;
+                    } else {
+                        c.fet = 0;
+                        c.steps++;
+                        /* src/odevec.F90:458-464; 1.0 and 0.3 are single precision */
+                        if (c.lju >= 20)
+                            c.ujac = true;
+                        else if (fabs(c.jchg - (double)1.0f) > (double)0.3f)
+                            c.ujac = true;
+#pragma unroll
+                        for (int j = 0; j < N; ++j)
+                            c.eno[j] = c.en[j];
+                        if (c.t < c.tstop) {
+                            c.told = c.t;
+                            ph = PH_PRED;
+                        } else {
+                            write_y = true;
+                            c.interpolate();
+                            c.t = c.tstop;
+                            ph = PH_DONE;
+                        }
+                    }
+                }
+            }
+            /* else: next Newton iteration on the next trip */
+        }
+
+        /* ---- 5. store finished cells -------------------------------- */
+        if (ph == PH_DONE) {
+            const bool ok = c.status == OV_OK;
+            if (!ok || write_y) {
+                if (c.msk) {
+#pragma unroll
+                    for (int j = 0; j < N; ++j)
+                        A.y[(int64_t)j * ncells + cell] = c.y[j];
+                }
+            }
+            A.t[cell] = c.t;
+            if (c.status != OV_ERR_GROUP_MISMATCH)
+                A.dt[cell] = c.h;
+            if (A.status)
+                A.status[cell] = c.status;
+            if (A.stats) {
+                int32_t* s = A.stats + cell * OV_NSTATS;
+                s[0] = c.steps;
+                s[1] = c.attempts;
+                s[2] = c.ltef;
+                s[3] = c.convf;
+                s[4] = c.newt;
+                s[5] = c.jacs;
+                s[6] = c.q;
+                s[7] = 0;
+            }
+            ph = PH_IDLE;
+        }
+    }
+}
+
+/* Launch helper: persistent grid of (SMs x resident blocks) unless given. */
+template <class Net, int G, class LUT>
+cudaError_t launch(const LaunchArgs& a, int block, int grid, cudaStream_t stream)
+{
+    auto kern = bdf_kernel<Net, G, LUT>;
+    if (block <= 0)
+        block = 128;
+    if (grid <= 0) {
+        static int cached_grid[2] = {0, 0};
+        int dev = 0;
+        cudaGetDevice(&dev);
+        if (cached_grid[0] == 0 || cached_grid[1] != block) {
+            int sms = 0, per_sm = 0;
+            cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, block, 0);
+            cached_grid[0] = sms * (per_sm > 0 ? per_sm : 1);
+            cached_grid[1] = block;
+        }
+        grid = cached_grid[0];
+        const int64_t warps_needed = (a.ncells + 31) / 32;
+        const int64_t blocks_needed = (warps_needed * 32 + block - 1) / block;
+        if (blocks_needed < grid)
+            grid = (int)blocks_needed;
+        if (grid < 1)
+            grid = 1;
+    }
+    kern<<<grid, block, 0, stream>>>(a);
+    return cudaGetLastError();
+}
+
+}  // namespace OV_MODE_NS
+}  // namespace ov
+
+/* Defines the launcher of one network variant in the current mode. */
+#define OV_DEFINE_LAUNCHER(cid, FP32)                                                            \
+    namespace ov {                                                                               \
+    namespace OV_MODE_NS {                                                                       \
+    cudaError_t launch_##cid(const LaunchArgs& a, int G, int lu, int block, int grid,             \
+                             cudaStream_t s)                                                     \
+    {                                                                                            \
+        if (G == 1 && lu == 0)                                                                   \
+            return launch<ov_net_##cid, 1, double>(a, block, grid, s);                           \
+        if (G == 32 && lu == 0)                                                                  \
+            return launch<ov_net_##cid, 32, double>(a, block, grid, s);                          \
+        if (FP32 && G == 1 && lu == 1)                                                           \
+            return launch<ov_net_##cid, 1, float>(a, block, grid, s);                            \
+        if (FP32 && G == 32 && lu == 1)                                                          \
+            return launch<ov_net_##cid, 32, float>(a, block, grid, s);                           \
+        return cudaErrorNotSupported;                                                            \
+    }                                                                                            \
+    }                                                                                            \
+    }

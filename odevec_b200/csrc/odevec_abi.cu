@@ -1,0 +1,302 @@
+/* C ABI of the B200 OdeVec solve path (declarations: include/odevec_b200.h).
+ *
+ * odevec_init    <- InitOdevec  (src/odevec.F90:94-154)
+ * odevec_solve   <- SolveODE    (src/odevec.F90:158-214), device arrays
+ * odevec_solve_host <- SolveODE with host arrays (copies in and out)
+ * odevec_close   <- CloseOdevec (src/odevec.F90:1058-1074)
+ *
+ * Errors never terminate the process: API misuse returns a negative code,
+ * per-cell integration failures are status codes (the reference calls
+ * `stop`, src/odevec.F90:114-124, 272-287, 380-390, 585-597). */
+#include <cuda_runtime.h>
+
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <new>
+
+#include "../../include/odevec_b200.h"
+#include "ov_launch.h"
+#include "gen/includes_c.inc"
+
+/* launchers, one per variant and arithmetic mode (kernels_<cid>_<mode>.cu) */
+#define OV_NET(cid, TAG)                                                                       \
+    namespace ov {                                                                             \
+    namespace exact {                                                                          \
+    cudaError_t launch_##cid(const LaunchArgs&, int, int, int, int, cudaStream_t);             \
+    }                                                                                          \
+    namespace fma {                                                                            \
+    cudaError_t launch_##cid(const LaunchArgs&, int, int, int, int, cudaStream_t);             \
+    }                                                                                          \
+    }
+#include "gen/registry.inc"
+#undef OV_NET
+
+namespace {
+
+struct NetEntry {
+    const char* tag;
+    const int* sizes;       /* neq, nnz, nrea, dense, idx_tgas */
+    const double* defaults; /* nvector, dt_min */
+    ov::launch_fn exact;
+    ov::launch_fn fma;
+};
+
+#define OV_NET(cid, TAG) {TAG, ov_##cid##_sizes, ov_##cid##_defaults, ov::exact::launch_##cid, ov::fma::launch_##cid},
+const NetEntry g_nets[] = {
+#include "gen/registry.inc"
+};
+#undef OV_NET
+constexpr int g_nnets = (int)(sizeof g_nets / sizeof g_nets[0]);
+
+thread_local char g_err[512] = "";
+
+int32_t fail(int32_t code, const char* fmt, ...)
+{
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(g_err, sizeof g_err, fmt, ap);
+    va_end(ap);
+    return code;
+}
+
+int find_net(const char* tag)
+{
+    if (!tag)
+        return -1;
+    for (int i = 0; i < g_nnets; ++i)
+        if (std::strcmp(g_nets[i].tag, tag) == 0)
+            return i;
+    return -1;
+}
+
+}  // namespace
+
+struct odevec_solver {
+    int net;
+    int64_t max_cells;
+    odevec_opts opts; /* resolved */
+    int device;
+    unsigned long long* d_queue;
+    /* staging for odevec_solve_host */
+    double *d_y, *d_t, *d_dt, *d_tstop;
+    uint8_t* d_mask;
+    int32_t *d_status, *d_stats;
+    cudaStream_t stream;
+};
+
+static int32_t resolve_opts(const NetEntry& e, const odevec_opts* in, odevec_opts* out)
+{
+    odevec_opts o;
+    if (in)
+        o = *in;
+    else {
+        std::memset(&o, 0, sizeof o);
+        o.rtol = 1e-4;
+        o.atol = 1e-20;
+        o.dt_min = -1.0;
+    }
+    if (!(o.rtol > 0.0) || !(o.atol >= 0.0))
+        return fail(OV_API_EINVAL, "rtol must be > 0 and atol >= 0 (got %g, %g)", o.rtol, o.atol);
+    if (o.dt_min < 0.0)
+        o.dt_min = e.defaults[1];
+    if (o.group_size == 0)
+        o.group_size = (int)e.defaults[0] == 32 ? 32 : 1;
+    if (o.group_size != 1 && o.group_size != 32)
+        return fail(OV_API_EINVAL, "group_size must be 1 or 32 (got %d)", o.group_size);
+    if (o.precision < OV_PREC_FP64 || o.precision > OV_PREC_FP32_LU)
+        return fail(OV_API_EINVAL, "unknown precision %d", o.precision);
+    if (o.max_attempts <= 0)
+        o.max_attempts = 1000000;
+    *out = o;
+    return OV_API_OK;
+}
+
+extern "C" {
+
+int32_t odevec_num_networks(void) { return g_nnets; }
+
+const char* odevec_network_tag(int32_t i) { return (i >= 0 && i < g_nnets) ? g_nets[i].tag : nullptr; }
+
+int32_t odevec_network_info(const char* tag, int32_t* info)
+{
+    const int i = find_net(tag);
+    if (i < 0)
+        return fail(OV_API_ENONET, "unknown network variant '%s'", tag ? tag : "(null)");
+    if (!info)
+        return fail(OV_API_EINVAL, "info is null");
+    for (int k = 0; k < 5; ++k)
+        info[k] = g_nets[i].sizes[k];
+    info[5] = (int)g_nets[i].defaults[0] == 32 ? 32 : 1;
+    return OV_API_OK;
+}
+
+const char* odevec_last_error(void) { return g_err; }
+
+int32_t odevec_init(const char* network, int64_t max_cells, const odevec_opts* opts, odevec_solver** out)
+{
+    if (!out)
+        return fail(OV_API_EINVAL, "out is null");
+    *out = nullptr;
+    const int ni = find_net(network);
+    if (ni < 0)
+        return fail(OV_API_ENONET, "unknown network variant '%s'", network ? network : "(null)");
+    if (max_cells < 0)
+        return fail(OV_API_EINVAL, "max_cells < 0");
+    odevec_opts o;
+    int32_t rc = resolve_opts(g_nets[ni], opts, &o);
+    if (rc)
+        return rc;
+    odevec_solver* s = new (std::nothrow) odevec_solver();
+    if (!s)
+        return fail(OV_API_ENOMEM, "out of host memory");
+    s->net = ni;
+    s->max_cells = max_cells;
+    s->opts = o;
+    cudaError_t e = cudaGetDevice(&s->device);
+    if (e == cudaSuccess)
+        e = cudaMalloc(&s->d_queue, 256);
+    const int neq = g_nets[ni].sizes[0];
+    if (e == cudaSuccess && max_cells > 0) {
+        const size_t nc = (size_t)max_cells;
+        if (e == cudaSuccess) e = cudaMalloc(&s->d_y, sizeof(double) * nc * neq);
+        if (e == cudaSuccess) e = cudaMalloc(&s->d_t, sizeof(double) * nc);
+        if (e == cudaSuccess) e = cudaMalloc(&s->d_dt, sizeof(double) * nc);
+        if (e == cudaSuccess) e = cudaMalloc(&s->d_tstop, sizeof(double) * nc);
+        if (e == cudaSuccess) e = cudaMalloc(&s->d_mask, nc);
+        if (e == cudaSuccess) e = cudaMalloc(&s->d_status, sizeof(int32_t) * nc);
+        if (e == cudaSuccess) e = cudaMalloc(&s->d_stats, sizeof(int32_t) * nc * OV_NSTATS);
+    }
+    if (e == cudaSuccess)
+        e = cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking);
+    if (e != cudaSuccess) {
+        odevec_close(s);
+        return fail(e == cudaErrorMemoryAllocation ? OV_API_ENOMEM : OV_API_ECUDA, "odevec_init: %s",
+                    cudaGetErrorString(e));
+    }
+    *out = s;
+    return OV_API_OK;
+}
+
+int32_t odevec_set_options(odevec_solver* s, const odevec_opts* opts)
+{
+    if (!s || !opts)
+        return fail(OV_API_EINVAL, "null argument");
+    odevec_opts o;
+    int32_t rc = resolve_opts(g_nets[s->net], opts, &o);
+    if (rc)
+        return rc;
+    s->opts = o;
+    return OV_API_OK;
+}
+
+int32_t odevec_solve(odevec_solver* s, int64_t ncells, double* y, double* t, double* dt,
+                     const double* t_stop, const uint8_t* mask, int32_t* status, int32_t* stats,
+                     void* stream)
+{
+    if (!s)
+        return fail(OV_API_EINVAL, "solver is null");
+    if (ncells < 0)
+        return fail(OV_API_EINVAL, "ncells < 0");
+    if (ncells == 0)
+        return OV_API_OK;
+    if (!y || !t || !dt || !t_stop)
+        return fail(OV_API_EINVAL, "y, t, dt and t_stop are required");
+    const odevec_opts& o = s->opts;
+    if (o.group_size == 32 && ncells % 32)
+        return fail(OV_API_EINVAL, "group_size 32 needs ncells divisible by 32 (got %lld)",
+                    (long long)ncells);
+    const NetEntry& e = g_nets[s->net];
+    ov::LaunchArgs a;
+    a.ncells = ncells;
+    a.y = y;
+    a.t = t;
+    a.dt = dt;
+    a.t_stop = t_stop;
+    a.mask = mask;
+    a.status = status;
+    a.stats = stats;
+    a.queue = s->d_queue;
+    a.rtol = o.rtol;
+    a.atol = o.atol;
+    a.dt_min = o.dt_min;
+    a.check_neg = o.check_negatives ? 1 : 0;
+    a.max_attempts = o.max_attempts;
+    cudaStream_t st = (cudaStream_t)stream;
+    cudaError_t err = cudaMemsetAsync(s->d_queue, 0, sizeof(unsigned long long), st);
+    if (err != cudaSuccess)
+        return fail(OV_API_ECUDA, "odevec_solve: %s", cudaGetErrorString(err));
+    const int lu = o.precision == OV_PREC_FP32_LU ? 1 : 0;
+    ov::launch_fn fn = o.precision == OV_PREC_FP64 ? e.exact : e.fma;
+    err = fn(a, o.group_size, lu, 0, 0, st);
+    if (err == cudaErrorNotSupported)
+        return fail(OV_API_EUNSUPPORTED, "variant %s: group %d precision %d not compiled", e.tag,
+                    o.group_size, o.precision);
+    if (err != cudaSuccess)
+        return fail(OV_API_ECUDA, "odevec_solve launch: %s", cudaGetErrorString(err));
+    return OV_API_OK;
+}
+
+int32_t odevec_solve_host(odevec_solver* s, int64_t ncells, double* y, double* t, double* dt,
+                          const double* t_stop, const uint8_t* mask, int32_t* status, int32_t* stats)
+{
+    if (!s)
+        return fail(OV_API_EINVAL, "solver is null");
+    if (ncells < 0)
+        return fail(OV_API_EINVAL, "ncells < 0");
+    if (ncells == 0)
+        return OV_API_OK;
+    if (ncells > s->max_cells)
+        return fail(OV_API_ETOOBIG, "ncells %lld exceeds max_cells %lld given to odevec_init",
+                    (long long)ncells, (long long)s->max_cells);
+    if (!y || !t || !dt || !t_stop)
+        return fail(OV_API_EINVAL, "y, t, dt and t_stop are required");
+    const int neq = g_nets[s->net].sizes[0];
+    const size_t n = (size_t)ncells;
+    cudaStream_t st = s->stream;
+    cudaError_t e = cudaSetDevice(s->device);
+    /* one copy per array; y is contiguous [neq][ncells] */
+    if (e == cudaSuccess) e = cudaMemcpyAsync(s->d_y, y, sizeof(double) * n * neq, cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(s->d_t, t, sizeof(double) * n, cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(s->d_dt, dt, sizeof(double) * n, cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(s->d_tstop, t_stop, sizeof(double) * n, cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess && mask) e = cudaMemcpyAsync(s->d_mask, mask, n, cudaMemcpyHostToDevice, st);
+    if (e != cudaSuccess)
+        return fail(OV_API_ECUDA, "odevec_solve_host copy-in: %s", cudaGetErrorString(e));
+    int32_t rc = odevec_solve(s, ncells, s->d_y, s->d_t, s->d_dt, s->d_tstop, mask ? s->d_mask : nullptr,
+                              s->d_status, stats ? s->d_stats : nullptr, st);
+    if (rc)
+        return rc;
+    e = cudaMemcpyAsync(y, s->d_y, sizeof(double) * n * neq, cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(t, s->d_t, sizeof(double) * n, cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(dt, s->d_dt, sizeof(double) * n, cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess && status)
+        e = cudaMemcpyAsync(status, s->d_status, sizeof(int32_t) * n, cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess && stats)
+        e = cudaMemcpyAsync(stats, s->d_stats, sizeof(int32_t) * n * OV_NSTATS, cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess)
+        e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess)
+        return fail(OV_API_ECUDA, "odevec_solve_host: %s", cudaGetErrorString(e));
+    return OV_API_OK;
+}
+
+int32_t odevec_close(odevec_solver* s)
+{
+    if (!s)
+        return OV_API_OK;
+    cudaFree(s->d_queue);
+    cudaFree(s->d_y);
+    cudaFree(s->d_t);
+    cudaFree(s->d_dt);
+    cudaFree(s->d_tstop);
+    cudaFree(s->d_mask);
+    cudaFree(s->d_status);
+    cudaFree(s->d_stats);
+    if (s->stream)
+        cudaStreamDestroy(s->stream);
+    delete s;
+    return OV_API_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,187 @@
+/* Common definitions shared by the CUDA kernels and the CPU oracle.
+ *
+ * Elementary functions.  The solver needs exp, log, log10 and pow in two
+ * places: the PRIMORDIAL rate laws (src/odevec_commons.F90:101-384) and the
+ * step-size factors of the order selection (src/odevec.F90:561-572).  The
+ * CPU library and the CUDA library implement these differently, so the same
+ * program gives results that differ in the last bit on the two processors,
+ * and one such bit can change an accept/reject decision of the integrator.
+ * The functions below are written once, with plain IEEE-754 double
+ * operations only, and compiled for both, so the GPU path and the CPU
+ * oracle evaluate bit-identical values.  Methods:
+ *
+ *   ov_exp  - Cody & Waite argument reduction x = k ln2 + r, |r| <= ln2/2,
+ *             with ln2 split into a 32-bit head and a tail (W. J. Cody and
+ *             W. Waite, "Software Manual for the Elementary Functions",
+ *             1980), then the Taylor series of e^r to degree 13 (truncation
+ *             error below 5e-18) in Horner form, then scaling by 2^k.
+ *   ov_log  - x = 2^e (1+f) with 1+f in [sqrt(1/2), sqrt(2)); with
+ *             u = f/(2+f), log(1+f) = 2 atanh(u) = f - u (f - R),
+ *             R = sum_{j>=1} 2 u^(2j) / (2j+1), summed to j = 11
+ *             (|u| <= 0.1716, truncation below 1e-18).
+ *   ov_pow  - exp(y log x) for x > 0, with the usual special cases.
+ *
+ * Measured against the C library: |error| <= 2 ulp for exp and log over
+ * their ranges (tests/test_math.py).  Division and square root are IEEE
+ * correctly rounded on both processors and are used directly.
+ *
+ * Floating-point contraction must be off for both compilers (gcc
+ * -ffp-contract=off, nvcc --fmad=false) wherever bit parity is expected. */
+#ifndef OV_COMMON_H
+#define OV_COMMON_H
+
+#include <math.h>
+#include <stdint.h>
+#include <string.h>
+
+#if defined(__CUDACC__)
+#define OV_HD __host__ __device__
+#define OV_INLINE __forceinline__
+#else
+#define OV_HD
+#define OV_INLINE inline
+#endif
+#define OV_RESTRICT __restrict__
+
+OV_HD static OV_INLINE double ov_bits2d(uint64_t b)
+{
+#if defined(__CUDA_ARCH__)
+    return __longlong_as_double((long long)b);
+#else
+    double d;
+    memcpy(&d, &b, sizeof d);
+    return d;
+#endif
+}
+
+OV_HD static OV_INLINE uint64_t ov_d2bits(double d)
+{
+#if defined(__CUDA_ARCH__)
+    return (uint64_t)__double_as_longlong(d);
+#else
+    uint64_t b;
+    memcpy(&b, &d, sizeof b);
+    return b;
+#endif
+}
+
+/* 2^m for -1022 <= m <= 1023 */
+OV_HD static OV_INLINE double ov_pow2i(int m)
+{
+    return ov_bits2d((uint64_t)(m + 1023) << 52);
+}
+
+/* p * 2^k for p in [0.5, 2] and -1080 < k < 1030, one rounding at most */
+OV_HD static OV_INLINE double ov_scale2(double p, int k)
+{
+    if (k > 1000)
+        return p * ov_pow2i(1000) * ov_pow2i(k - 1000);
+    if (k < -1000)
+        return p * ov_pow2i(k + 1000) * ov_pow2i(-1000);
+    return p * ov_pow2i(k);
+}
+
+#define OV_LN2_HI 0x1.62e42fee00000p-1  /* ln 2 truncated to 32 bits */
+#define OV_LN2_LO 0x1.a39ef35793c76p-33 /* ln 2 - OV_LN2_HI, rounded */
+#define OV_INV_LN2 0x1.71547652b82fep+0
+#define OV_INV_LN10 0x1.bcb7b1526e50ep-2
+#define OV_SQRT2 0x1.6a09e667f3bcdp+0
+
+OV_HD static OV_INLINE double ov_exp(double x)
+{
+    if (x != x)
+        return x;
+    if (x > 709.782712893384)
+        return INFINITY;
+    if (x < -745.1332191019412)
+        return 0.0;
+    /* nearest integer of x/ln2 (|x/ln2| < 2^11, so the shift trick is exact) */
+    const double shift = 6755399441055744.0; /* 1.5 * 2^52 */
+    double kd = (x * OV_INV_LN2 + shift) - shift;
+    int k = (int)kd;
+    double r = (x - kd * OV_LN2_HI) - kd * OV_LN2_LO;
+    double p = 1.0 / 6227020800.0;            /* 1/13! */
+    p = 1.0 / 479001600.0 + r * p;            /* 1/12! */
+    p = 1.0 / 39916800.0 + r * p;             /* 1/11! */
+    p = 1.0 / 3628800.0 + r * p;
+    p = 1.0 / 362880.0 + r * p;
+    p = 1.0 / 40320.0 + r * p;
+    p = 1.0 / 5040.0 + r * p;
+    p = 1.0 / 720.0 + r * p;
+    p = 1.0 / 120.0 + r * p;
+    p = 1.0 / 24.0 + r * p;
+    p = 1.0 / 6.0 + r * p;
+    p = 0.5 + r * p;
+    p = 1.0 + r * p;
+    p = 1.0 + r * p;
+    return ov_scale2(p, k);
+}
+
+OV_HD static OV_INLINE double ov_log(double x)
+{
+    if (x != x)
+        return x;
+    if (x < 0.0)
+        return NAN;
+    if (x == 0.0)
+        return -INFINITY;
+    if (x == INFINITY)
+        return x;
+    int e = 0;
+    uint64_t b = ov_d2bits(x);
+    if ((b >> 52) == 0) { /* subnormal */
+        x *= 18014398509481984.0; /* 2^54 */
+        e = -54;
+        b = ov_d2bits(x);
+    }
+    e += (int)(b >> 52) - 1023;
+    double m = ov_bits2d((b & 0x000fffffffffffffULL) | 0x3ff0000000000000ULL); /* [1,2) */
+    if (m > OV_SQRT2) {
+        m *= 0.5;
+        e += 1;
+    }
+    double f = m - 1.0; /* exact */
+    double u = f / (2.0 + f);
+    double z = u * u;
+    double R = 2.0 / 23.0;
+    R = 2.0 / 21.0 + z * R;
+    R = 2.0 / 19.0 + z * R;
+    R = 2.0 / 17.0 + z * R;
+    R = 2.0 / 15.0 + z * R;
+    R = 2.0 / 13.0 + z * R;
+    R = 2.0 / 11.0 + z * R;
+    R = 2.0 / 9.0 + z * R;
+    R = 2.0 / 7.0 + z * R;
+    R = 2.0 / 5.0 + z * R;
+    R = 2.0 / 3.0 + z * R;
+    R = z * R;
+    double ed = (double)e;
+    double lm = f - u * (f - R);
+    return ed * OV_LN2_HI + (lm + ed * OV_LN2_LO);
+}
+
+OV_HD static OV_INLINE double ov_log10(double x)
+{
+    return ov_log(x) * OV_INV_LN10;
+}
+
+OV_HD static OV_INLINE double ov_pow(double x, double y)
+{
+    if (y == 0.0 || x == 1.0)
+        return 1.0;
+    if (x != x || y != y)
+        return x + y;
+    if (x == 0.0)
+        return y > 0.0 ? 0.0 : INFINITY;
+    if (x < 0.0) {
+        double yi = floor(y);
+        if (yi != y)
+            return NAN;
+        double a = ov_exp(y * ov_log(-x));
+        double h = 0.5 * y;
+        return (floor(h) == h) ? a : -a;
+    }
+    return ov_exp(y * ov_log(x));
+}
+
+#endif /* OV_COMMON_H */

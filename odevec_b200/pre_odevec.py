@@ -1,0 +1,596 @@
+#!/usr/bin/env python
+"""OdeVec preprocessor: SymPy network -> straight-line C / CUDA network code.
+
+Same command line as the reference (``pre_odevec.py:383-450``): ``--nvector``,
+``--example``, ``--krome_setupfile``, ``--LUmethod``, ``--dt_min``,
+``--heatcool``, ``--ordering``, ``--packaging``; and the same pipeline
+(``pre_odevec.py:463-540``):
+
+1. ``J = rhs.jacobian(y)``                              (``pre_odevec.py:467``)
+2. ``P = I - dt*beta*J``                                (``pre_odevec.py:474-475``)
+3. reordering CMK / INVERT / FF                         (``pre_odevec.py:265-361``)
+4. LU fill pattern of the reordered ``P``                (``pre_odevec.py:494``)
+5. CSC arrays ``row_index``, ``u_col_start`` (column starts) and
+   ``l_col_start`` (diagonal positions)                 (``pre_odevec.py:523-540``)
+
+Instead of substituting ``#ODEVEC_*`` pragmas in Fortran templates it writes,
+per network variant ``<tag>``:
+
+* ``csrc/gen/net_<tag>.h`` - plain C, callable from host and device
+  (``OV_HD``): the right-hand side ``f = rhs(y, k)`` in species order and the
+  iteration matrix ``P`` at the LU pattern positions in CSC storage order
+  (fill-ins written as 0, as ``pre_odevec.py:173-180`` does), plus the
+  permutation and CSC arrays as constants.
+* ``csrc/gen/net_<tag>.cuh`` - CUDA: a traits struct for the solver kernel and
+  the numeric LU factorisation and the two triangular solves unrolled into
+  straight-line code over the fill pattern, with the permutation folded into
+  the solve's loads and stores.  The operation order is exactly that of the
+  reference loops: right-looking Doolittle for DENSE packaging
+  (``src/odevec.F90:898-922``, solve ``:797-849``) and left-looking Crout for
+  CSC (``src/odevec.F90:929-971``, solve ``:853-891``).  DENSE stores only the
+  structurally non-zero entries; the skipped terms are exact zeros, so the
+  results equal the full n x n loops.
+
+Expressions are printed term by term without common-subexpression rewriting,
+in SymPy's canonical order, which is the order ``fcode`` prints them in the
+reference; integer powers are expanded into products as gfortran expands them
+(``x*x``, ``x*(x*x)``, ...).  Compiled without floating-point contraction the
+emitted code therefore evaluates the same IEEE operations as the reference's
+generated Fortran.
+
+The LU pattern is computed structurally (boolean elimination without
+pivoting); ``--lu_pattern=symbolic`` instead runs SymPy's symbolic
+``LUdecomposition_Simple`` like the reference, which can only drop entries
+that cancel exactly.  For the shipped networks both give the reference's
+pattern (checked in the tests).
+"""
+from __future__ import annotations
+
+import argparse
+import dataclasses
+import os
+import re
+import sys
+from typing import Dict, List, Optional, Sequence, Tuple
+
+import numpy as np
+import sympy as sp
+from mpmath.libmp import prec_to_dps, to_str as mlib_to_str
+from sympy.printing.c import C99CodePrinter
+
+from . import networks
+
+GEN_DIR = os.path.join(os.path.dirname(os.path.abspath(__file__)), "csrc", "gen")
+MAXORDER = 5  # pre_odevec.py:83
+
+
+# ----------------------------------------------------------------- ordering
+def _pattern_of(P: sp.SparseMatrix) -> np.ndarray:
+    n = P.shape[0]
+    pat = np.zeros((n, n), dtype=bool)
+    for (i, j), v in P.todok().items():
+        if v != 0:
+            pat[i, j] = True
+    return pat
+
+
+def ordering_cmk(P: sp.SparseMatrix) -> np.ndarray:
+    """Reverse Cuthill-McKee of the transposed pattern with SciPy's
+    ``reverse_cuthill_mckee(symmetric_mode=False)``, as ``pre_odevec.py:292-302``."""
+    from scipy import sparse
+    from scipy.sparse import csgraph
+    pat = _pattern_of(P)
+    rows, cols = np.nonzero(pat)
+    # the reference swaps the (row, col) of P.col_list() when building the matrix
+    M = sparse.csc_matrix((np.ones(len(rows), dtype=int), (cols, rows)), shape=pat.shape)
+    return np.asarray(csgraph.reverse_cuthill_mckee(M, symmetric_mode=False), dtype=int)
+
+
+def ordering_invert(P: sp.SparseMatrix) -> np.ndarray:
+    """Reversed indices (``pre_odevec.py:317-334``)."""
+    return np.arange(P.shape[0])[::-1].copy()
+
+
+def ordering_ff(P: sp.SparseMatrix) -> np.ndarray:
+    """Fewest non-zeros first: key = nnz(column i) + nnz(row i) - 1, ascending
+    (``pre_odevec.py:337-361``).  Ties keep index order (stable sort)."""
+    pat = _pattern_of(P)
+    key = pat.sum(axis=0) + pat.sum(axis=1) - 1
+    return np.argsort(key, kind="stable").astype(int)
+
+
+ORDERINGS = {"CMK": ordering_cmk, "INVERT": ordering_invert, "FF": ordering_ff}
+
+
+# --------------------------------------------------------------- LU pattern
+def structural_lu_pattern(pat: np.ndarray) -> np.ndarray:
+    """Fill pattern of Gaussian elimination without pivoting."""
+    lu = pat.copy()
+    n = lu.shape[0]
+    for k in range(n):
+        rows = np.nonzero(lu[k + 1:, k])[0] + k + 1
+        cols = np.nonzero(lu[k, k + 1:])[0] + k + 1
+        if len(rows) and len(cols):
+            lu[np.ix_(rows, cols)] = True
+    return lu
+
+
+def symbolic_lu_pattern(P_order: sp.Matrix) -> np.ndarray:
+    LU, _ = sp.Matrix(P_order).LUdecomposition_Simple()
+    n = LU.shape[0]
+    pat = np.zeros((n, n), dtype=bool)
+    for i in range(n):
+        for j in range(n):
+            pat[i, j] = LU[i, j] != 0
+    return pat
+
+
+# ------------------------------------------------------------------- system
+@dataclasses.dataclass
+class System:
+    net: networks.Network
+    tag: str
+    packaging: str            # "DENSE" | "CSC"
+    ordering: str             # "None" | "CMK" | "INVERT" | "FF"
+    perm: List[int]           # storage row i holds species perm[i]
+    P: sp.Matrix              # I - dt*beta*J in species order
+    P_order: sp.Matrix        # permuted
+    lu_pat: np.ndarray        # bool n x n, storage order
+    row_index: List[int]
+    u_col_start: List[int]
+    l_col_start: List[int]
+    p_nnz: int
+    nvector: int = 1
+    dt_min: float = 1e-10
+    lu_method: int = 1
+
+    @property
+    def neq(self) -> int:
+        return self.net.neq
+
+    @property
+    def nnz(self) -> int:
+        return len(self.row_index)
+
+    def pos(self) -> Dict[Tuple[int, int], int]:
+        """(row, col) in storage order -> index into the packed value array."""
+        out = {}
+        for j in range(self.neq):
+            for kk in range(self.u_col_start[j], self.u_col_start[j + 1]):
+                out[(self.row_index[kk], j)] = kk
+        return out
+
+
+def build_system(net: networks.Network, ordering: str = "None", packaging: str = "DENSE",
+                 lu_pattern: str = "structural", nvector: int = 1, dt_min: float = 1e-10,
+                 lu_method: int = 1, tag: Optional[str] = None) -> System:
+    packaging = packaging.upper()
+    if packaging in ("COO", "CSR"):
+        raise SystemExit("# Error: %s packaging is not supported" % packaging)  # pre_odevec.py:515-518
+    if packaging not in ("DENSE", "CSC"):
+        raise SystemExit("# Error: This format is not known.")
+    if lu_method not in (1,):
+        raise SystemExit("# Error: --LUmethod=%d is not supported by the CUDA emitter "
+                         "(1 = symbolic Jacobian + numeric LU)" % lu_method)
+    n = net.neq
+    jac = net.rhs.jacobian(net.y)
+    dt, beta = sp.symbols("dt beta")
+    P = sp.SparseMatrix(sp.eye(n) - dt * beta * jac)
+    if ordering in (None, "None", "NONE", ""):
+        ordering = "None"
+        perm = np.arange(n)
+    else:
+        if ordering not in ORDERINGS:
+            raise SystemExit("# Error: unknown ordering %r" % ordering)
+        perm = ORDERINGS[ordering](P)
+    perm = [int(v) for v in perm]
+    P_order = sp.zeros(n, n)
+    for i in range(n):
+        for j in range(n):
+            P_order[i, j] = P[perm[i], perm[j]]
+    pat = _pattern_of(sp.SparseMatrix(P_order))
+    if lu_pattern == "symbolic" and packaging == "CSC":
+        # the dense factorisation touches every structurally non-zero entry,
+        # so DENSE always uses the structural pattern
+        lu = symbolic_lu_pattern(P_order)
+        lu |= np.eye(n, dtype=bool)
+    else:
+        lu = structural_lu_pattern(pat | np.eye(n, dtype=bool))
+    if (pat & ~lu).any():
+        raise SystemExit("# Error: P has entries outside the LU pattern (exact cancellation); "
+                         "use --lu_pattern=structural")
+    row_index, u_col_start, l_col_start = [], [], []
+    for j in range(n):
+        u_col_start.append(len(row_index))
+        for i in range(n):
+            if lu[i, j]:
+                if i == j:
+                    l_col_start.append(len(row_index))
+                row_index.append(i)
+    u_col_start.append(len(row_index))
+    if tag is None:
+        tag = "%s_%s_%s" % (net.name, packaging, ordering.upper())
+    return System(net, tag, packaging, ordering, perm, sp.Matrix(P), P_order, lu,
+                  row_index, u_col_start, l_col_start, int(pat.sum()), nvector, dt_min, lu_method)
+
+
+# ------------------------------------------------------------------ printer
+# addition chain x^n = x^(n-t[n]) * x^t[n] (the way gfortran expands x**n)
+_POWI = [0, 1, 1, 2, 2, 3, 3, 4, 4, 6, 5, 6, 6, 10, 7, 9]
+
+
+class NetPrinter(C99CodePrinter):
+    """C printer mapping the reference's symbol names onto array accesses."""
+
+    _sym = re.compile(r"^(y|k)\(:,(\d+)\)$")
+
+    def __init__(self, ymap: Dict[sp.Symbol, str], kname: str = "k"):
+        super().__init__()
+        self.ymap = ymap
+        self.kname = kname
+
+    def _print_Symbol(self, expr):
+        if expr in self.ymap:
+            return self.ymap[expr]
+        m = self._sym.match(expr.name)
+        if m and m.group(1) == "k":
+            return "%s[%d]" % (self.kname, int(m.group(2)) - 1)
+        if expr.name in ("dt", "beta"):
+            return expr.name
+        raise ValueError("unexpected symbol %s" % expr.name)
+
+    def _print_Float(self, expr):
+        # the decimal string fcode writes: the Float's own precision (15
+        # significant digits for a double), so the compiled constant is the
+        # same double as the reference's generated Fortran constant
+        s = mlib_to_str(expr._mpf_, prec_to_dps(expr._prec), strip_zeros=True)
+        if s in ("+inf", "inf", "-inf", "nan"):
+            raise ValueError("non-finite constant in network expression")
+        if "e" not in s and "." not in s:
+            s += ".0"
+        return s
+
+    def _print_Integer(self, expr):
+        return "%d.0" % int(expr)
+
+    def _print_Rational(self, expr):
+        return "(%d.0/%d.0)" % (expr.p, expr.q)
+
+    def _powi(self, base: str, n: int) -> str:
+        cache = {1: base}
+
+        def rec(m):
+            if m in cache:
+                return cache[m]
+            if m < len(_POWI):
+                s = "(%s*%s)" % (rec(m - _POWI[m]), rec(_POWI[m]))
+            else:
+                s = "(%s*%s)" % (rec(m - 1), base)
+            cache[m] = s
+            return s
+        return rec(n)
+
+    def _print_Pow(self, expr):
+        b, e = expr.as_base_exp()
+        bs = self.parenthesize(b, 1000)
+        if e.is_Integer:
+            n = int(e)
+            if n > 0:
+                return self._powi(bs, n)
+            if n < 0:
+                return "(1.0/%s)" % self._powi(bs, -n)
+            return "1.0"
+        if e == sp.Rational(1, 2):
+            return "sqrt(%s)" % self._print(b)
+        return "ov_pow(%s, %s)" % (self._print(b), self._print(sp.Float(float(e))))
+
+
+def _cexpr(expr, pr: NetPrinter) -> str:
+    expr = sp.sympify(expr)
+    if expr == 0:
+        return "0.0"
+    return pr.doprint(expr)
+
+
+def _cid(tag: str) -> str:
+    return re.sub(r"[^A-Za-z0-9_]", "_", tag).lower()
+
+
+# ----------------------------------------------------------------- emitters
+def emit_c_header(sysm: System) -> str:
+    net = sysm.net
+    n, nnz = sysm.neq, sysm.nnz
+    cid = _cid(sysm.tag)
+    ymap = {s: "y[%d]" % i for i, s in enumerate(net.y)}
+    pr = NetPrinter(ymap)
+    pos = sysm.pos()
+    L = []
+    g = "OV_NET_%s_H" % cid.upper()
+    L.append("/* Generated by odevec_b200.pre_odevec -- do not edit.")
+    L.append(" * network %s, packaging %s, ordering %s, neq %d, LU nnz %d (P nnz %d)."
+             % (net.name, sysm.packaging, sysm.ordering, n, nnz, sysm.p_nnz))
+    L.append(" * rhs(): f = dy/dt in species order (rate array k as in the reference).")
+    L.append(" * jac(): P = I - dt*beta*J at the LU pattern positions, CSC storage order")
+    L.append(" *        of the permuted matrix; fill-in positions are 0.  */")
+    L.append("#ifndef %s" % g)
+    L.append("#define %s" % g)
+    L.append('#include "../ov_common.h"')
+    if net.rates:
+        L.append('#include "../rates_%s.h"' % net.rates)
+    L.append("")
+    L.append("#define OV_%s_NEQ %d" % (cid.upper(), n))
+    L.append("#define OV_%s_NNZ %d" % (cid.upper(), nnz))
+    L.append("#define OV_%s_NREA %d" % (cid.upper(), net.nrea if net.rates else 0))
+    L.append("#define OV_%s_DENSE %d" % (cid.upper(), 1 if sysm.packaging == "DENSE" else 0))
+    L.append("#define OV_%s_NVECTOR %d" % (cid.upper(), sysm.nvector))
+    L.append("#define OV_%s_DT_MIN %r" % (cid.upper(), float(sysm.dt_min)))
+    L.append("#define OV_%s_IDX_TGAS %d" % (cid.upper(), net.idx_tgas if net.idx_tgas is not None else -1))
+
+    def arr(name, vals):
+        L.append("static const int ov_%s_%s[%d] = {%s};" % (cid, name, len(vals),
+                                                          ", ".join(str(v) for v in vals)))
+    arr("sizes", [n, nnz, net.nrea if net.rates else 0, 1 if sysm.packaging == "DENSE" else 0,
+                  net.idx_tgas if net.idx_tgas is not None else -1])
+    L.append("static const double ov_%s_defaults[2] = {%d.0, %r}; /* nvector, dt_min */"
+             % (cid, sysm.nvector, float(sysm.dt_min)))
+    arr("perm", sysm.perm)
+    arr("row_index", sysm.row_index)
+    arr("u_col_start", sysm.u_col_start)
+    arr("l_col_start", sysm.l_col_start)
+    L.append("")
+    L.append("OV_HD static OV_INLINE void ov_%s_rhs(const double* OV_RESTRICT y, "
+             "const double* OV_RESTRICT k, double* OV_RESTRICT f)" % cid)
+    L.append("{")
+    L.append("  (void)k;")
+    for i in range(n):
+        L.append("  f[%d] = %s;" % (i, _cexpr(net.rhs[i], pr)))
+    L.append("}")
+    L.append("")
+    L.append("OV_HD static OV_INLINE void ov_%s_jac(const double* OV_RESTRICT y, "
+             "const double* OV_RESTRICT k, double beta, double dt, double* OV_RESTRICT a)" % cid)
+    L.append("{")
+    L.append("  (void)y; (void)k; (void)beta; (void)dt;")
+    for j in range(n):
+        for kk in range(sysm.u_col_start[j], sysm.u_col_start[j + 1]):
+            i = sysm.row_index[kk]
+            L.append("  a[%d] = %s;  /* (%d,%d) */" % (kk, _cexpr(sysm.P_order[i, j], pr), i, j))
+    L.append("}")
+    L.append("")
+    L.append("#endif")
+    return "\n".join(L) + "\n"
+
+
+def _lu_factor_lines(sysm: System) -> List[str]:
+    """Straight-line numeric LU in the reference's operation order."""
+    n = sysm.neq
+    pos = sysm.pos()
+    out = []
+    if sysm.packaging == "DENSE":
+        # right-looking Doolittle (src/odevec.F90:906-921)
+        for k in range(n - 1):
+            for j in range(k + 1, n):
+                if (j, k) in pos:
+                    out.append("a[%d] = a[%d] / a[%d];" % (pos[(j, k)], pos[(j, k)], pos[(k, k)]))
+            for j in range(k + 1, n):
+                if (k, j) not in pos:
+                    continue
+                for m in range(k + 1, n):
+                    if (m, k) in pos:
+                        out.append("a[%d] = a[%d] - a[%d]*a[%d];"
+                                   % (pos[(m, j)], pos[(m, j)], pos[(m, k)], pos[(k, j)]))
+    else:
+        # left-looking Crout on the CSC pattern (src/odevec.F90:937-969)
+        ri, ucs, lcs = sysm.row_index, sysm.u_col_start, sysm.l_col_start
+        for k in range(n):
+            colpos = {ri[kk]: kk for kk in range(ucs[k], ucs[k + 1])}
+            for kk in range(ucs[k], lcs[k]):
+                j = ri[kk]
+                out.append("a[%d] = a[%d] / a[%d];" % (kk, kk, lcs[j]))
+                for jj in range(lcs[j] + 1, ucs[j + 1]):
+                    r = ri[jj]
+                    if r in colpos:
+                        out.append("a[%d] = a[%d] - a[%d]*a[%d];" % (colpos[r], colpos[r], kk, jj))
+    return out
+
+
+def _lu_solve_lines(sysm: System) -> List[str]:
+    """Straight-line solve P_order x = r with the permutation folded in:
+    reads r[perm[i]] and writes x[perm[i]] (species order)."""
+    n = sysm.neq
+    pos = sysm.pos()
+    p = sysm.perm
+    out = []
+    for i in range(n):
+        out.append("T d%d = (T)(r[%d]*OV_SC(%d));" % (i, p[i], p[i]))
+    if sysm.packaging == "DENSE":
+        # forward, unit lower (src/odevec.F90:814-826): d_k = r_k - sum_{j<k} L_kj d_j
+        for k in range(n):
+            terms = [j for j in range(k) if (k, j) in pos]
+            if terms:
+                s = "a[%d]*d%d" % (pos[(k, terms[0])], terms[0])
+                for j in terms[1:]:
+                    s = "(%s + a[%d]*d%d)" % (s, pos[(k, j)], j)
+                out.append("d%d = d%d - %s;" % (k, k, s))
+        # backward (src/odevec.F90:835-847): x_k = (d_k - sum_{j>k} U_kj x_j) / U_kk
+        for k in range(n - 1, -1, -1):
+            terms = [j for j in range(k + 1, n) if (k, j) in pos]
+            if terms:
+                s = "a[%d]*d%d" % (pos[(k, terms[0])], terms[0])
+                for j in terms[1:]:
+                    s = "(%s + a[%d]*d%d)" % (s, pos[(k, j)], j)
+                out.append("d%d = (d%d - %s) / a[%d];" % (k, k, s, pos[(k, k)]))
+            else:
+                out.append("d%d = d%d / a[%d];" % (k, k, pos[(k, k)]))
+    else:
+        ri, ucs, lcs = sysm.row_index, sysm.u_col_start, sysm.l_col_start
+        # forward (src/odevec.F90:864-876)
+        for k in range(n):
+            out.append("d%d = d%d / a[%d];" % (k, k, lcs[k]))
+            for kk in range(lcs[k] + 1, ucs[k + 1]):
+                out.append("d%d = d%d - d%d*a[%d];" % (ri[kk], ri[kk], k, kk))
+        # backward (src/odevec.F90:878-889)
+        for k in range(n - 1, -1, -1):
+            for kk in range(ucs[k], lcs[k]):
+                out.append("d%d = d%d - d%d*a[%d];" % (ri[kk], ri[kk], k, kk))
+    for i in range(n):
+        out.append("x[%d] = (double)d%d*OV_ISC(%d);" % (p[i], i, p[i]))
+    return out
+
+
+def emit_cuda_header(sysm: System) -> str:
+    net = sysm.net
+    cid = _cid(sysm.tag)
+    n = sysm.neq
+    L = []
+    g = "OV_NET_%s_CUH" % cid.upper()
+    L.append("/* Generated by odevec_b200.pre_odevec -- do not edit.")
+    L.append(" * CUDA traits of network variant %s for the BDF kernel: straight-line" % sysm.tag)
+    L.append(" * LU factorisation and solve over the fill pattern (%s). */" %
+             ("right-looking Doolittle" if sysm.packaging == "DENSE" else "left-looking Crout, CSC"))
+    L.append("#pragma once")
+    L.append('#include "net_%s.h"' % cid)
+    L.append("")
+    L.append("struct ov_net_%s {" % cid)
+    L.append("  static constexpr int NEQ = %d;" % n)
+    L.append("  static constexpr int NNZ = %d;" % sysm.nnz)
+    L.append("  static constexpr int NREA = %d;" % (net.nrea if net.rates else 0))
+    L.append("  static constexpr int IDX_TGAS = %d;" % (net.idx_tgas if net.idx_tgas is not None else -1))
+    L.append("  static constexpr bool DENSE = %s;" % ("true" if sysm.packaging == "DENSE" else "false"))
+    L.append('  static constexpr const char* TAG = "%s";' % sysm.tag)
+    L.append("  OV_HD static OV_INLINE void rhs(const double* y, const double* k, double* f) "
+             "{ ov_%s_rhs(y, k, f); }" % cid)
+    L.append("  OV_HD static OV_INLINE void jac(const double* y, const double* k, double beta, "
+             "double dt, double* a) { ov_%s_jac(y, k, beta, dt, a); }" % cid)
+    if net.rates:
+        L.append("  OV_HD static OV_INLINE void rates_T(const double* y, double* r) "
+                 "{ ov_rates_%s_T(y[%d], r); }" % (net.rates, net.idx_tgas))
+        L.append("  OV_HD static OV_INLINE void rates_k(const double* y, const double* r, double* k) "
+                 "{ ov_rates_%s_k(y, %d, r, k); }" % (net.rates, n))
+    else:
+        L.append("  OV_HD static OV_INLINE void rates_T(const double*, double*) {}")
+        L.append("  OV_HD static OV_INLINE void rates_k(const double*, const double*, double*) {}")
+    L.append("  /* a = D P D^-1 rounded to T, D = diag(sc) in species order (isc = 1/sc) */")
+    L.append("  template <class T> OV_HD static OV_INLINE void store_scaled(const double* OV_RESTRICT P, "
+             "T* OV_RESTRICT a, const double* OV_RESTRICT sc, const double* OV_RESTRICT isc) {")
+    for j in range(n):
+        for kk in range(sysm.u_col_start[j], sysm.u_col_start[j + 1]):
+            i = sysm.row_index[kk]
+            L.append("    a[%d] = (T)(P[%d]*sc[%d]*isc[%d]);" % (kk, kk, sysm.perm[i], sysm.perm[j]))
+    L.append("  }")
+    L.append("  /* in-place numeric LU of the packed matrix a[NNZ] */")
+    L.append("  template <class T> OV_HD static OV_INLINE void lu_factor(T* OV_RESTRICT a) {")
+    for s in _lu_factor_lines(sysm):
+        L.append("    " + s)
+    L.append("  }")
+    L.append("  /* x = P^-1 r with P = LU in a[]; r and x in species order.  sc/isc scale")
+    L.append("     species i by sc[i] on the way in and isc[i] on the way out (pass")
+    L.append("     nullptr for none); T is the precision of the solve. */")
+    L.append("  template <class T> OV_HD static OV_INLINE void lu_solve(const T* OV_RESTRICT a, "
+             "const double* OV_RESTRICT r, double* OV_RESTRICT x, const double* OV_RESTRICT sc, "
+             "const double* OV_RESTRICT isc) {")
+    L.append("#define OV_SC(i) (sc ? sc[i] : 1.0)")
+    L.append("#define OV_ISC(i) (isc ? isc[i] : 1.0)")
+    for s in _lu_solve_lines(sysm):
+        L.append("    " + s)
+    L.append("#undef OV_SC")
+    L.append("#undef OV_ISC")
+    L.append("  }")
+    L.append("  static constexpr int perm[%d] = {%s};" % (n, ", ".join(map(str, sysm.perm))))
+    L.append("};")
+    return "\n".join(L) + "\n"
+
+
+def write_variant(sysm: System, outdir: str = GEN_DIR) -> Tuple[str, str]:
+    os.makedirs(outdir, exist_ok=True)
+    cid = _cid(sysm.tag)
+    h = os.path.join(outdir, "net_%s.h" % cid)
+    cu = os.path.join(outdir, "net_%s.cuh" % cid)
+    with open(h, "w") as fh:
+        fh.write(emit_c_header(sysm))
+    with open(cu, "w") as fh:
+        fh.write(emit_cuda_header(sysm))
+    write_registry(outdir)
+    return h, cu
+
+
+def write_registry(outdir: str = GEN_DIR) -> str:
+    """X-macro list of every emitted variant: OV_NET(cid, "TAG")."""
+    tags = []
+    for f in sorted(os.listdir(outdir)):
+        m = re.match(r"net_(.*)\.cuh$", f)
+        if m:
+            txt = open(os.path.join(outdir, f)).read()
+            t = re.search(r'TAG = "([^"]+)"', txt).group(1)
+            tags.append((m.group(1), t))
+    path = os.path.join(outdir, "registry.inc")
+    with open(path, "w") as fh:
+        fh.write("/* Generated by odevec_b200.pre_odevec: every emitted network variant. */\n")
+        for cid, t in tags:
+            fh.write('OV_NET(%s, "%s")\n' % (cid, t))
+    with open(os.path.join(outdir, "includes.inc"), "w") as fh:
+        fh.write("/* Generated by odevec_b200.pre_odevec. */\n")
+        for cid, _ in tags:
+            fh.write('#include "net_%s.cuh"\n' % cid)
+    with open(os.path.join(outdir, "includes_c.inc"), "w") as fh:
+        fh.write("/* Generated by odevec_b200.pre_odevec. */\n")
+        for cid, _ in tags:
+            fh.write('#include "net_%s.h"\n' % cid)
+    return path
+
+
+# ---------------------------------------------------------------------- CLI
+def parse_args(argv=None):
+    p = argparse.ArgumentParser(
+        description="Preprocessor for OdeVec on B200: emits straight-line C/CUDA network code.")
+    p.add_argument("--example", default="PRIMORDIAL", help="ROBER | OREGO | PRIMORDIAL | KROME")
+    p.add_argument("--krome_setupfile", default=None, help="python dump of a KROME network")
+    p.add_argument("--LUmethod", type=int, default=1, help="1: symbolic Jacobian + numeric LU")
+    p.add_argument("--dt_min", default=1e-10, help="default minimal time step")
+    p.add_argument("--nvector", type=int, required=True,
+                   help="default lockstep group size (1 = per-cell control, 32 = one warp)")
+    p.add_argument("--heatcool", type=int, default=0)
+    p.add_argument("--equilibrium_H", type=int, default=0)
+    p.add_argument("--ordering", default="None", help="CMK | INVERT | FF | None")
+    p.add_argument("--packaging", default="DENSE", help="DENSE | CSC")
+    p.add_argument("--lu_pattern", default="structural", help="structural | symbolic")
+    p.add_argument("--name", default=None, help="network name used in the variant tag")
+    p.add_argument("--outdir", default=GEN_DIR)
+    p.add_argument("--sparsity_structure", default=False)
+    return p.parse_args(argv)
+
+
+def main(argv=None) -> System:
+    args = parse_args(argv)
+    if args.krome_setupfile is not None:
+        args.example = "KROME"
+    if args.heatcool:
+        raise SystemExit("# Error: --heatcool=1 needs KROME's heating/cooling functions, "
+                         "which this build does not provide")
+    if args.equilibrium_H == 1 and args.packaging != "DENSE":   # pre_odevec.py:455-460
+        raise SystemExit("args.equilibrium_H is only allowed with DENSE packaging.")
+    if args.equilibrium_H == 1 and args.ordering != "None":
+        raise SystemExit("args.equilibrium_H is only allowed without ordering.")
+    if args.equilibrium_H == 1 and args.LUmethod != 3:
+        raise SystemExit("args.equilibrium_H is currently only usable with LUmethod==3.")
+    print("#  Setting up system..")
+    print('#  Vector length "nvector":', args.nvector)
+    net = networks.load(args.example, args.krome_setupfile)
+    if args.name:
+        net.name = args.name
+    sysm = build_system(net, args.ordering, args.packaging, args.lu_pattern, args.nvector,
+                        float(args.dt_min), args.LUmethod)
+    n = net.neq
+    print("#  Permutation list", np.array(sysm.perm))
+    print("#  NNZs in Jacobian: %d | Sparsity: %s" % (sysm.p_nnz, 1 - sysm.p_nnz / (n * n)))
+    print("#  NNZs in LU-Matrix: %d | Sparsity: %s" % (sysm.nnz, 1 - sysm.nnz / (n * n)))
+    h, cu = write_variant(sysm, args.outdir)
+    print("#  Wrote out file: " + h)
+    print("#  Wrote out file: " + cu)
+    if str(args.sparsity_structure) == "True":
+        for i in range(n):
+            print("".join("X" if sysm.lu_pat[i, j] else "." for j in range(n)))
+    return sysm
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,44 @@
+"""The network variants compiled into the library by default.
+
+Each entry is a preprocessor command line (the reference's flags).  The
+defaults follow the reference drivers: ROBER with nvector=32 lockstep and
+dt_min=1e-20 (``tests/rober.f90:44``), OREGO per cell with the default
+dt_min, PRIMORDIAL per cell with dt_min=1e-20 (``tests/primordial.f90:45``)
+in dense, FF- and CMK-ordered CSC packaging, and the synthetic 64-species
+network read from a KROME-format dump.
+"""
+import os
+
+from . import pre_odevec
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+SYN64_DUMP = os.path.join(HERE, "data", "syn64_krome.py")
+
+SHIPPED = [
+    ["--example=ROBER", "--packaging=DENSE", "--nvector=32", "--dt_min=1e-20"],
+    ["--example=ROBER", "--packaging=CSC", "--nvector=32", "--dt_min=1e-20"],
+    ["--example=OREGO", "--packaging=CSC", "--ordering=CMK", "--nvector=1"],
+    ["--example=OREGO", "--packaging=DENSE", "--nvector=1"],
+    ["--example=PRIMORDIAL", "--packaging=DENSE", "--nvector=1", "--dt_min=1e-20"],
+    ["--example=PRIMORDIAL", "--packaging=CSC", "--ordering=FF", "--nvector=1", "--dt_min=1e-20"],
+    ["--example=PRIMORDIAL", "--packaging=CSC", "--ordering=CMK", "--nvector=1", "--dt_min=1e-20"],
+]
+
+
+def emit_all(outdir: str = pre_odevec.GEN_DIR, quiet: bool = True):
+    import contextlib
+    import io
+    os.makedirs(outdir, exist_ok=True)
+    systems = []
+    for argv in SHIPPED + ([["--krome_setupfile=" + SYN64_DUMP, "--name=SYN64", "--packaging=CSC",
+                             "--ordering=CMK", "--nvector=1", "--dt_min=1e-20"]]
+                           if os.path.exists(SYN64_DUMP) else []):
+        buf = io.StringIO()
+        with contextlib.redirect_stdout(buf) if quiet else contextlib.nullcontext():
+            systems.append(pre_odevec.main(argv + ["--outdir=" + outdir]))
+    return systems
+
+
+if __name__ == "__main__":
+    for s in emit_all(quiet=False):
+        print(s.tag, "nnz", s.nnz)

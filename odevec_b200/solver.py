@@ -1,0 +1,261 @@
+"""Python host side of the solve path: ctypes over libodevec_b200.so.
+
+Mirrors the reference's Fortran interface (src/odevec.F90):
+
+* ``Odevec`` - the ``type(odevec)`` object, with the caller-set fields
+  ``RelativeTolerance``, ``AbsoluteTolerance``, ``MinimalTimestep`` and
+  ``CheckNegatives`` (``src/odevec.F90:48-52``), plus ``nvector`` (the
+  lockstep group size, 1 or 32), ``neq`` and the precision form;
+* ``InitOdevec(ode)`` (``:94-154``), ``SolveODE(ode, time, dt, t_stop, y,
+  Mask=None)`` (``:158-214``) and ``CloseOdevec(ode)`` (``:1058-1074``).
+
+``SolveODE`` takes ``y`` as an ``(ncells, neq)`` or ``(neq, ncells)`` view
+of the reference's ``y(nvector, neq)`` array - species-major storage,
+``y[s * ncells + c]`` - either as a torch CUDA tensor (solved in place on
+the device, on torch's current stream) or as a NumPy array (copied to the
+GPU and back through ``odevec_solve_host``).  ``time`` and ``dt`` are
+updated like the Fortran ``intent(inout)`` arguments; scalars are broadcast
+to all cells.
+
+Where the reference stops the program (``print`` + ``stop``) this raises
+``OdevecError`` carrying the per-cell status codes, unless
+``raise_on_failure`` is False.  The product path always runs the CUDA
+kernels: importing this module or creating a solver fails loudly when the
+library is missing or no GPU is visible.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from typing import Optional
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIBPATH = os.path.join(HERE, "libodevec_b200.so")
+
+OV_OK = 0
+STATUS_NAMES = {
+    0: "OK",
+    1: "DT_MIN_PREDICTOR",
+    2: "CONV_FAILURES",
+    3: "DT_MIN_CONV",
+    4: "MAX_STEPS",
+    5: "ORDER",
+    6: "GROUP_MISMATCH",
+}
+OV_NSTATS = 8
+STAT_NAMES = ["steps", "attempts", "lte_fails", "conv_fails", "newton_iters", "jac_evals",
+              "order", "reserved"]
+PREC = {"fp64": 0, "fp64_fma": 1, "fp32_lu": 2}
+
+
+class OdevecError(RuntimeError):
+    def __init__(self, msg, status=None):
+        super().__init__(msg)
+        self.status = status
+
+
+class _Opts(ctypes.Structure):
+    _fields_ = [("rtol", ctypes.c_double), ("atol", ctypes.c_double), ("dt_min", ctypes.c_double),
+                ("check_negatives", ctypes.c_int32), ("group_size", ctypes.c_int32),
+                ("precision", ctypes.c_int32), ("max_attempts", ctypes.c_int32)]
+
+
+_lib = None
+
+
+def lib():
+    """The loaded C-ABI library (built in-tree by odevec_b200.build)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIBPATH):
+            raise OdevecError("libodevec_b200.so not found at %s: run `python -m odevec_b200.build`"
+                              % LIBPATH)
+        L = ctypes.CDLL(LIBPATH)
+        P, i32, i64 = ctypes.c_void_p, ctypes.c_int32, ctypes.c_int64
+        L.odevec_num_networks.restype = i32
+        L.odevec_network_tag.restype = ctypes.c_char_p
+        L.odevec_network_tag.argtypes = [i32]
+        L.odevec_network_info.argtypes = [ctypes.c_char_p, P]
+        L.odevec_network_info.restype = i32
+        L.odevec_init.argtypes = [ctypes.c_char_p, i64, ctypes.POINTER(_Opts), ctypes.POINTER(P)]
+        L.odevec_init.restype = i32
+        L.odevec_set_options.argtypes = [P, ctypes.POINTER(_Opts)]
+        L.odevec_set_options.restype = i32
+        L.odevec_solve.argtypes = [P, i64, P, P, P, P, P, P, P, P]
+        L.odevec_solve.restype = i32
+        L.odevec_solve_host.argtypes = [P, i64, P, P, P, P, P, P, P]
+        L.odevec_solve_host.restype = i32
+        L.odevec_close.argtypes = [P]
+        L.odevec_close.restype = i32
+        L.odevec_last_error.restype = ctypes.c_char_p
+        _lib = L
+    return _lib
+
+
+def _check(rc):
+    if rc != 0:
+        raise OdevecError("odevec: %s (code %d)" % (lib().odevec_last_error().decode(), rc))
+
+
+def networks():
+    L = lib()
+    return [L.odevec_network_tag(i).decode() for i in range(L.odevec_num_networks())]
+
+
+def network_info(tag):
+    info = np.zeros(6, np.int32)
+    _check(lib().odevec_network_info(tag.encode(), info.ctypes.data_as(ctypes.c_void_p)))
+    return {"neq": int(info[0]), "nnz": int(info[1]), "nrea": int(info[2]), "dense": bool(info[3]),
+            "idx_tgas": int(info[4]), "nvector": int(info[5])}
+
+
+class Odevec:
+    """The solver object (``type(odevec)``, src/odevec.F90:33-74)."""
+
+    def __init__(self, network: str, max_cells: int = 0, RelativeTolerance: float = 1e-4,
+                 AbsoluteTolerance: float = 1e-20, MinimalTimestep: Optional[float] = None,
+                 CheckNegatives: bool = False, nvector: Optional[int] = None,
+                 precision: str = "fp64", max_attempts: int = 0, raise_on_failure: bool = True):
+        info = network_info(network)
+        self.network = network
+        self.neq = info["neq"]
+        self.nnz = info["nnz"]
+        self.nrea = info["nrea"]
+        self.idx_tgas = info["idx_tgas"]
+        self.nvector = info["nvector"] if nvector is None else int(nvector)
+        self.max_cells = int(max_cells)
+        self.RelativeTolerance = RelativeTolerance
+        self.AbsoluteTolerance = AbsoluteTolerance
+        self.MinimalTimestep = MinimalTimestep
+        self.CheckNegatives = CheckNegatives
+        self.precision = precision
+        self.max_attempts = max_attempts
+        self.raise_on_failure = raise_on_failure
+        self.status = None
+        self.stats = None
+        self._h = None
+
+    def _opts(self):
+        o = _Opts()
+        o.rtol = float(self.RelativeTolerance)
+        o.atol = float(self.AbsoluteTolerance)
+        o.dt_min = -1.0 if self.MinimalTimestep is None else float(self.MinimalTimestep)
+        o.check_negatives = 1 if self.CheckNegatives else 0
+        o.group_size = int(self.nvector)
+        if self.precision not in PREC:
+            raise ValueError("precision must be one of %s" % list(PREC))
+        o.precision = PREC[self.precision]
+        o.max_attempts = int(self.max_attempts)
+        return o
+
+    @property
+    def handle(self):
+        if self._h is None:
+            raise OdevecError("InitOdevec has not been called")
+        return self._h
+
+
+def InitOdevec(ode: Odevec) -> Odevec:
+    """Creates the device-side solver (src/odevec.F90:94-154)."""
+    import torch
+    if not torch.cuda.is_available():
+        raise OdevecError("odevec_b200 needs a CUDA GPU; none is visible")
+    torch.cuda.init()
+    h = ctypes.c_void_p()
+    o = ode._opts()
+    _check(lib().odevec_init(ode.network.encode(), ode.max_cells, ctypes.byref(o), ctypes.byref(h)))
+    ode._h = h
+    return ode
+
+
+def CloseOdevec(ode: Odevec) -> None:
+    """Frees the device-side solver (src/odevec.F90:1058-1074)."""
+    if ode._h is not None:
+        lib().odevec_close(ode._h)
+        ode._h = None
+
+
+def _as_cells(a, ncells, name, torch_mod=None, device=None):
+    if torch_mod is not None:
+        if not torch_mod.is_tensor(a):
+            a = torch_mod.full((ncells,), float(a), dtype=torch_mod.float64, device=device)
+        elif a.dim() == 0 or a.numel() == 1:
+            a = a.reshape(1).to(device=device, dtype=torch_mod.float64).expand(ncells).contiguous()
+        if a.dtype != torch_mod.float64 or not a.is_contiguous() or a.numel() != ncells:
+            raise ValueError("%s must be a contiguous float64 tensor of %d cells" % (name, ncells))
+        return a
+    a = np.asarray(a, dtype=np.float64)
+    if a.ndim == 0 or a.size == 1:
+        return np.full(ncells, float(a), np.float64)
+    if a.size != ncells:
+        raise ValueError("%s must have %d entries" % (name, ncells))
+    return np.ascontiguousarray(a)
+
+
+def SolveODE(ode: Odevec, time, dt, t_stop, y, Mask=None, stream=None, want_stats=True):
+    """Integrates every cell from ``time`` to ``t_stop`` (src/odevec.F90:158-214).
+
+    ``y``: species-major storage of ``ncells x neq`` values: a torch CUDA
+    tensor or NumPy array of shape ``(neq, ncells)`` (C order), solved in
+    place.  ``time``/``dt``: scalars or per-cell arrays; returns
+    ``(time, dt)`` after the solve (``time == t_stop``).  ``Mask``: optional
+    per-cell booleans.  Per-cell status and statistics are left in
+    ``ode.status`` / ``ode.stats``.
+    """
+    h = ode.handle
+    is_torch = False
+    try:
+        import torch
+        is_torch = torch.is_tensor(y)
+    except ImportError:
+        torch = None
+    if y.ndim != 2 or y.shape[0] != ode.neq:
+        raise ValueError("y must have shape (neq=%d, ncells)" % ode.neq)
+    ncells = int(y.shape[1])
+    o = ode._opts()
+    _check(lib().odevec_set_options(h, ctypes.byref(o)))
+    if is_torch:
+        if not y.is_cuda or y.dtype != torch.float64 or not y.is_contiguous():
+            raise ValueError("y must be a contiguous float64 CUDA tensor")
+        dev = y.device
+        t = _as_cells(time, ncells, "time", torch, dev)
+        d = _as_cells(dt, ncells, "dt", torch, dev)
+        ts = _as_cells(t_stop, ncells, "t_stop", torch, dev)
+        m = None
+        if Mask is not None:
+            m = torch.as_tensor(Mask, device=dev).to(torch.uint8).contiguous()
+        status = torch.empty(ncells, dtype=torch.int32, device=dev)
+        stats = torch.empty((ncells, OV_NSTATS), dtype=torch.int32, device=dev) if want_stats else None
+        st = stream if stream is not None else torch.cuda.current_stream(dev)
+        ptr = lambda a: None if a is None else ctypes.c_void_p(a.data_ptr())
+        with torch.cuda.device(dev):
+            _check(lib().odevec_solve(h, ncells, ptr(y), ptr(t), ptr(d), ptr(ts), ptr(m),
+                                      ptr(status), ptr(stats), ctypes.c_void_p(st.cuda_stream)))
+        ode.status, ode.stats = status, stats
+        if ode.raise_on_failure:
+            bad = int((status != 0).sum().item())
+            if bad:
+                raise OdevecError("SolveODE: %d cells failed (first status %s)"
+                                  % (bad, STATUS_NAMES.get(int(status[status != 0][0].item()))), status)
+        return t, d
+    # host arrays: copy in, solve, copy out (odevec_solve_host)
+    if not isinstance(y, np.ndarray) or y.dtype != np.float64 or not y.flags.c_contiguous:
+        raise ValueError("y must be a C-contiguous float64 NumPy array or a CUDA tensor")
+    if ncells > ode.max_cells:
+        raise ValueError("ncells %d > max_cells %d given at InitOdevec" % (ncells, ode.max_cells))
+    t = _as_cells(time, ncells, "time").copy()
+    d = _as_cells(dt, ncells, "dt").copy()
+    ts = _as_cells(t_stop, ncells, "t_stop")
+    m = None if Mask is None else np.ascontiguousarray(Mask, dtype=np.uint8)
+    status = np.zeros(ncells, np.int32)
+    stats = np.zeros((ncells, OV_NSTATS), np.int32) if want_stats else None
+    p = lambda a: None if a is None else a.ctypes.data_as(ctypes.c_void_p)
+    _check(lib().odevec_solve_host(h, ncells, p(y), p(t), p(d), p(ts), p(m), p(status), p(stats)))
+    ode.status, ode.stats = status, stats
+    if ode.raise_on_failure and np.any(status != 0):
+        bad = int(np.sum(status != 0))
+        raise OdevecError("SolveODE: %d cells failed (first status %s)"
+                          % (bad, STATUS_NAMES.get(int(status[status != 0][0]))), status)
+    return t, d

@@ -1,0 +1,100 @@
+"""ctypes wrapper of the CPU oracle -- TEST INFRASTRUCTURE ONLY.
+
+Used by tests/, by ``__graft_entry__.smoke()`` as the checker and by
+``bench.py`` for the CPU baseline; never by the product path.
+"""
+import ctypes
+import os
+
+import numpy as np
+
+from . import build as _build
+
+OV_NSTATS = 8
+_lib = None
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        path = _build.build()
+        L = ctypes.CDLL(path)
+        d, i64, i32 = ctypes.c_double, ctypes.c_int64, ctypes.c_int
+        P = ctypes.c_void_p
+        L.ov_oracle_solve.argtypes = [ctypes.c_char_p, i64, i32, d, d, d, i32, i64, P, P, P, P, P,
+                                      P, P, i32]
+        L.ov_oracle_solve.restype = i32
+        L.ov_oracle_eval.argtypes = [ctypes.c_char_p, P, P, d, d, P, P]
+        L.ov_oracle_rates.argtypes = [d, P]
+        L.ov_oracle_netinfo.argtypes = [ctypes.c_char_p, P, P, P, P, P]
+        L.ov_oracle_num_nets.restype = i32
+        L.ov_oracle_net_tag.restype = ctypes.c_char_p
+        L.ov_oracle_net_tag.argtypes = [i32]
+        for f in ("ov_oracle_exp", "ov_oracle_log"):
+            getattr(L, f).argtypes = [d]
+            getattr(L, f).restype = d
+        L.ov_oracle_pow.argtypes = [d, d]
+        L.ov_oracle_pow.restype = d
+        _lib = L
+    return _lib
+
+
+def _p(a):
+    return None if a is None else a.ctypes.data_as(ctypes.c_void_p)
+
+
+def netinfo(tag):
+    L = lib()
+    info = np.zeros(5, dtype=np.int32)
+    if L.ov_oracle_netinfo(tag.encode(), _p(info), None, None, None, None) != 0:
+        raise KeyError(tag)
+    neq, nnz = int(info[0]), int(info[1])
+    perm = np.zeros(neq, np.int32)
+    ri = np.zeros(nnz, np.int32)
+    ucs = np.zeros(neq + 1, np.int32)
+    lcs = np.zeros(neq, np.int32)
+    L.ov_oracle_netinfo(tag.encode(), _p(info), _p(perm), _p(ri), _p(ucs), _p(lcs))
+    return {"neq": neq, "nnz": nnz, "nrea": int(info[2]), "dense": bool(info[3]),
+            "idx_tgas": int(info[4]), "perm": perm, "row_index": ri, "u_col_start": ucs,
+            "l_col_start": lcs}
+
+
+def tags():
+    L = lib()
+    return [L.ov_oracle_net_tag(i).decode() for i in range(L.ov_oracle_num_nets())]
+
+
+def solve(tag, y, t, dt, t_stop, rtol, atol, dt_min, group=1, check_negatives=False,
+          mask=None, max_attempts=1000000, nthreads=0):
+    """SolveODE on all cells.  y: (neq, ncells) float64, modified copy returned
+    with t, dt, status, stats."""
+    y = np.ascontiguousarray(y, dtype=np.float64).copy()
+    ncells = y.shape[1]
+    t = np.ascontiguousarray(np.broadcast_to(t, (ncells,)), dtype=np.float64).copy()
+    dt = np.ascontiguousarray(np.broadcast_to(dt, (ncells,)), dtype=np.float64).copy()
+    t_stop = np.ascontiguousarray(np.broadcast_to(t_stop, (ncells,)), dtype=np.float64).copy()
+    m = None if mask is None else np.ascontiguousarray(mask, dtype=np.uint8)
+    status = np.zeros(ncells, np.int32)
+    stats = np.zeros((ncells, OV_NSTATS), np.int32)
+    rc = lib().ov_oracle_solve(tag.encode(), ncells, group, rtol, atol, dt_min,
+                               int(bool(check_negatives)), max_attempts, _p(y), _p(t), _p(dt),
+                               _p(t_stop), _p(m), _p(status), _p(stats), nthreads)
+    if rc != 0:
+        raise ValueError("oracle solve failed rc=%d" % rc)
+    return y, t, dt, status, stats
+
+
+def evaluate(tag, y, k, beta, dt):
+    info = netinfo(tag)
+    y = np.ascontiguousarray(y, np.float64)
+    k = np.ascontiguousarray(k if len(k) else [0.0], np.float64)
+    f = np.zeros(info["neq"])
+    a = np.zeros(info["nnz"])
+    lib().ov_oracle_eval(tag.encode(), _p(y), _p(k), beta, dt, _p(f), _p(a))
+    return f, a
+
+
+def rates(T):
+    r = np.zeros(38)
+    lib().ov_oracle_rates(float(T), _p(r))
+    return r

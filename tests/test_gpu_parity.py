@@ -1,0 +1,177 @@
+"""GPU parity: the CUDA solve path against the CPU oracle.
+
+The FP64 form without fused multiply-add (precision "fp64") must reproduce
+the oracle bit for bit: final states, times, last step sizes, status codes
+and every per-cell counter.  The fused-multiply-add and FP32-LU forms are
+compared within tolerances stated in each test.  All calls go through the
+C ABI (odevec_solve / odevec_solve_host).
+"""
+import numpy as np
+import pytest
+
+from odevec_b200 import workloads as W
+
+pytestmark = pytest.mark.gpu
+
+
+def run_gpu(S, wl, precision="fp64", group=None, host=False, mask=None, check_negatives=False,
+            max_attempts=0, dt_min=None):
+    import torch
+    ode = S.Odevec(wl.network, max_cells=wl.ncells if host else 0, RelativeTolerance=wl.rtol,
+                   AbsoluteTolerance=wl.atol,
+                   MinimalTimestep=wl.dt_min if dt_min is None else dt_min,
+                   CheckNegatives=check_negatives, nvector=wl.group if group is None else group,
+                   precision=precision, max_attempts=max_attempts, raise_on_failure=False)
+    S.InitOdevec(ode)
+    try:
+        if host:
+            y = wl.y.copy()
+            t, dt = S.SolveODE(ode, wl.t0, wl.dt0, wl.t_stop, y, Mask=mask)
+            return y, t, dt, ode.status.copy(), ode.stats.copy()
+        y = torch.tensor(wl.y, device="cuda")
+        t, dt = S.SolveODE(ode, torch.tensor(wl.t0, device="cuda"), torch.tensor(wl.dt0, device="cuda"),
+                           torch.tensor(wl.t_stop, device="cuda"), y, Mask=mask)
+        torch.cuda.synchronize()
+        return (y.cpu().numpy(), t.cpu().numpy(), dt.cpu().numpy(), ode.status.cpu().numpy(),
+                ode.stats.cpu().numpy())
+    finally:
+        S.CloseOdevec(ode)
+
+
+def run_oracle(O, wl, group=None, mask=None, check_negatives=False, max_attempts=1000000,
+               dt_min=None, rtol=None, atol=None):
+    return O.solve(wl.network, wl.y, wl.t0, wl.dt0, wl.t_stop, wl.rtol if rtol is None else rtol,
+                   wl.atol if atol is None else atol, wl.dt_min if dt_min is None else dt_min,
+                   group=wl.group if group is None else group, check_negatives=check_negatives,
+                   mask=mask, max_attempts=max_attempts)
+
+
+def assert_bitwise(g, o, what=""):
+    names = ["y", "t", "dt", "status", "stats"]
+    for name, a, b in zip(names, g, o):
+        a = np.asarray(a)
+        b = np.asarray(b)
+        if name == "stats":
+            a = a[:, :7]
+            b = b[:, :7]
+        same = (a == b) | (np.isnan(a) & np.isnan(b)) if a.dtype.kind == "f" else (a == b)
+        if not np.all(same):
+            idx = np.argwhere(~same)[:5]
+            raise AssertionError("%s: %s differs at %s: gpu %s oracle %s" % (
+                what, name, idx.tolist(), a[tuple(idx[0])], b[tuple(idx[0])]))
+
+
+CASES = [
+    ("ROBER", dict(ncells=256), "ROBER_DENSE_NONE", 32),
+    ("ROBER", dict(ncells=256), "ROBER_CSC_NONE", 1),
+    ("OREGO", dict(ncells=512), "OREGO_CSC_CMK", 1),
+    ("OREGO", dict(ncells=256), "OREGO_DENSE_NONE", 1),
+    ("PRIMORDIAL", dict(ncells=512), "PRIMORDIAL_CSC_FF", 1),
+    ("PRIMORDIAL", dict(ncells=256), "PRIMORDIAL_CSC_CMK", 1),
+    ("PRIMORDIAL", dict(ncells=256), "PRIMORDIAL_DENSE_NONE", 1),
+    ("PRIMORDIAL", dict(ncells=256), "PRIMORDIAL_DENSE_NONE", 32),
+]
+
+
+@pytest.mark.parametrize("name,kw,network,group", CASES)
+def test_fp64_bit_exact_vs_oracle(gpu_lib, oracle, name, kw, network, group):
+    wl = W.BUILDERS[name](network=network, **kw)
+    if group == 32 and name == "PRIMORDIAL":
+        wl.t_stop[:] = 1e10  # lockstep groups need a common t_stop
+    g = run_gpu(gpu_lib, wl, "fp64", group=group)
+    o = run_oracle(oracle, wl, group=group)
+    assert np.all(o[3] == 0), "oracle failures: %s" % np.unique(o[3])
+    assert_bitwise(g, o, "%s/%s G=%d" % (name, network, group))
+
+
+def test_host_entry_point_matches_device(gpu_lib, oracle):
+    wl = W.primordial(ncells=300, network="PRIMORDIAL_CSC_FF")
+    g = run_gpu(gpu_lib, wl, "fp64", host=True)
+    o = run_oracle(oracle, wl)
+    assert_bitwise(g, o, "host path")
+
+
+def _relerr(a, b, floor):
+    m = np.abs(b) > floor
+    return np.max(np.abs(a[m] - b[m]) / np.abs(b[m])) if np.any(m) else 0.0
+
+
+@pytest.mark.parametrize("precision", ["fp64_fma", "fp32_lu"])
+def test_fast_forms_within_tolerance(gpu_lib, oracle, precision):
+    # FMA changes roundings and FP32-LU the Newton iterates, so step
+    # sequences differ; both must stay within 100*rtol of the exact form for
+    # species above 1e-12 of the cell's hydrogen density
+    wl = W.primordial(ncells=1024)
+    g = run_gpu(gpu_lib, wl, precision)
+    o = run_oracle(oracle, wl)
+    assert np.all(g[3] == 0)
+    floor = 1e-12 * np.max(wl.y[:12], axis=0)
+    err = np.max([_relerr(g[0][s], o[0][s], floor) for s in range(12)])
+    assert err < 100 * wl.rtol, err
+
+
+def test_mask_semantics(gpu_lib, oracle):
+    wl = W.orego(ncells=256)
+    mask = (np.arange(256) % 3 != 0).astype(np.uint8)
+    g = run_gpu(gpu_lib, wl, "fp64", mask=mask)
+    o = run_oracle(oracle, wl, mask=mask)
+    assert_bitwise(g, o, "mask")
+    off = mask == 0
+    assert np.all(g[0][:, off] == wl.y[:, off])       # untouched
+    assert np.all(g[1][off] == wl.t_stop[off])        # time = t_stop
+
+
+def test_lockstep_mask(gpu_lib, oracle):
+    wl = W.rober(ncells=128)
+    mask = np.ones(128, np.uint8)
+    mask[::5] = 0
+    mask[64:96] = 0     # one group fully masked
+    g = run_gpu(gpu_lib, wl, "fp64", mask=mask)
+    o = run_oracle(oracle, wl, mask=mask)
+    assert_bitwise(g, o, "lockstep mask")
+
+
+def test_check_negatives(gpu_lib, oracle):
+    wl = W.primordial(ncells=256, network="PRIMORDIAL_CSC_FF")
+    g = run_gpu(gpu_lib, wl, "fp64", check_negatives=True)
+    o = run_oracle(oracle, wl, check_negatives=True)
+    assert_bitwise(g, o, "check negatives")
+
+
+def test_status_max_attempts(gpu_lib, oracle):
+    wl = W.primordial(ncells=64)
+    g = run_gpu(gpu_lib, wl, "fp64", max_attempts=7)
+    o = run_oracle(oracle, wl, max_attempts=7)
+    assert np.all(g[3] == 4)  # OV_ERR_MAX_STEPS
+    assert_bitwise(g, o, "max attempts")
+
+
+def test_status_dt_min(gpu_lib, oracle):
+    # a minimal step far above the natural one: Newton failures shrink dt below it
+    wl = W.rober(ncells=64, network="ROBER_CSC_NONE")
+    wl.group = 1
+    g = run_gpu(gpu_lib, wl, "fp64", dt_min=1e3)
+    o = run_oracle(oracle, wl, dt_min=1e3)
+    assert_bitwise(g, o, "dt_min")
+
+
+def test_group_mismatch(gpu_lib, oracle):
+    wl = W.rober(ncells=64)
+    wl.t_stop[5] = 2e5
+    g = run_gpu(gpu_lib, wl, "fp64")
+    o = run_oracle(oracle, wl)
+    assert np.all(g[3][:32] == 6) and np.all(g[3][32:] == 0)
+    assert_bitwise(g, o, "group mismatch")
+
+
+def test_primordial_conservation_full_size_sample(gpu_lib):
+    # size-independent properties at a larger size: nuclei and charge
+    # conservation and positivity for every cell
+    wl = W.primordial(ncells=65536)
+    g = run_gpu(gpu_lib, wl, "fp32_lu")
+    assert np.all(g[3] == 0)
+    a = W.primordial_invariants(wl.y)
+    b = W.primordial_invariants(g[0])
+    for k in range(3):
+        assert np.max(np.abs(b[k] - a[k]) / a[k]) < 1e-8
+    assert np.max(np.abs(b[3]) / a[0]) < 1e-8
