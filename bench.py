@@ -1,0 +1,398 @@
+#!/usr/bin/env python
+"""Benchmark of the OdeVec solve path on B200.
+
+Metric: PRIMORDIAL cells/s to t_end at rtol 1e-6 (the 16-species primordial
+network, 1,048,576 cells per GPU, per-cell temperature and t_end), reported
+for the FP32-LU/FP64-residual form (``value``) beside the plain FP64 path
+and the FP64 path with fused multiply-add.  One step = one complete solve of
+all cells from the initial state to their t_end; inputs are reset from a
+device copy before each step (159 MB of inputs, larger than the 126 MB L2).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl product|reference]
+
+Multi-GPU (torchrun, one process per GPU): every rank integrates its own
+1,048,576 cells (weak scaling; cells are independent, no data exchange);
+timing is the maximum over ranks.  ``--impl reference`` times the CPU
+restatement of the reference solver (oracle/) on the host cores instead.
+"""
+import argparse
+import json
+import os
+import statistics
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "PRIMORDIAL cells/s to t_end at rtol 1e-6, FP32-LU vs FP64 path; p50/p99 latency"
+WORKLOAD = ("PRIMORDIAL 16-species/38-reaction network, %d cells per GPU, log-uniform n_H 1e-2..1e6, "
+            "T 10..1e4 K, t_end 1e8..1e13 s, rtol 1e-6, atol 1e-20")
+DATA = "synthetic: seeded inputs with the configuration's distributions (no public data set)"
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=5)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", default="product", choices=["product", "reference"])
+    p.add_argument("--ncells", type=int, default=1048576)
+    p.add_argument("--network", default="PRIMORDIAL_CSC_FF")
+    p.add_argument("--forms", default="fp32_lu,fp64,fp64_fma")
+    p.add_argument("--cpu-sample", type=int, default=65536)
+    p.add_argument("--accuracy-cells", type=int, default=256)
+    p.add_argument("--no-cpu", action="store_true")
+    return p.parse_args()
+
+
+def dist_env():
+    return (int(os.environ.get("RANK", 0)), int(os.environ.get("WORLD_SIZE", 1)),
+            int(os.environ.get("LOCAL_RANK", 0)))
+
+
+class ClockSampler:
+    """SM clock and throttle reasons sampled every 100 ms (NVML)."""
+
+    def __init__(self, index):
+        self.index = index
+        self.samples = []
+        self.reasons = set()
+        self.max_mhz = None
+        self._stop = threading.Event()
+        self._t = None
+
+    def _run(self):
+        try:
+            import pynvml as nv
+            nv.nvmlInit()
+            h = nv.nvmlDeviceGetHandleByIndex(self.index)
+            self.max_mhz = nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM)
+            names = {
+                "hw_slowdown": getattr(nv, "nvmlClocksThrottleReasonHwSlowdown", 0x8),
+                "sw_thermal_slowdown": getattr(nv, "nvmlClocksThrottleReasonSwThermalSlowdown", 0x20),
+                "hw_thermal_slowdown": getattr(nv, "nvmlClocksThrottleReasonHwThermalSlowdown", 0x40),
+                "sw_power_cap": getattr(nv, "nvmlClocksThrottleReasonSwPowerCap", 0x4),
+            }
+            while not self._stop.is_set():
+                self.samples.append(nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM))
+                r = nv.nvmlDeviceGetCurrentClocksThrottleReasons(h)
+                for k, bit in names.items():
+                    if r & bit:
+                        self.reasons.add(k)
+                self._stop.wait(0.1)
+        except Exception as e:  # NVML missing: report no samples
+            self.reasons.add("nvml_unavailable:%s" % type(e).__name__)
+
+    def __enter__(self):
+        self._t = threading.Thread(target=self._run, daemon=True)
+        self._t.start()
+        return self
+
+    def __exit__(self, *a):
+        self._stop.set()
+        self._t.join()
+
+    def summary(self):
+        return {"sm_mhz": statistics.median(self.samples) if self.samples else None,
+                "sm_max_mhz": self.max_mhz, "reasons": sorted(self.reasons),
+                "samples": len(self.samples)}
+
+
+def fma_peaks(torch):
+    """Measured FMA throughput (TFLOP/s) of this GPU, FP64 and FP32."""
+    import ctypes
+    from odevec_b200 import solver as S
+    L = S.lib()
+    L.odevec_probe_fma.argtypes = [ctypes.c_int32] * 4 + [ctypes.c_void_p] * 2 + [
+        ctypes.POINTER(ctypes.c_float), ctypes.POINTER(ctypes.c_double)]
+    sms = torch.cuda.get_device_properties(0).multi_processor_count
+    scratch = torch.zeros(sms * 64, dtype=torch.float64, device="cuda")
+    out = {}
+    for name, fp64, iters in (("fp64", 1, 4096), ("fp32", 0, 8192)):
+        best = 0.0
+        for _ in range(3):
+            ms, fl = ctypes.c_float(), ctypes.c_double()
+            S._check(L.odevec_probe_fma(fp64, sms * 8, 512, iters, ctypes.c_void_p(scratch.data_ptr()),
+                                        ctypes.c_void_p(torch.cuda.current_stream().cuda_stream),
+                                        ctypes.byref(ms), ctypes.byref(fl)))
+            best = max(best, fl.value / (ms.value * 1e-3) / 1e12)
+        out[name] = best
+    return out
+
+
+def traffic_per_cell():
+    """DRAM bytes per cell of the solve kernel from the committed ncu summary."""
+    path = os.path.join(ROOT, "profiles", "bdf_kernel_primordial_ncu.txt")
+    if not os.path.exists(path):
+        return None
+    for line in open(path):
+        if line.startswith("dram_bytes_per_cell:"):
+            return float(line.split(":")[1])
+    return None
+
+
+def oracle_rate(wl, ncells, threads):
+    from oracle import oracle as O
+    sub = slice(0, ncells)
+    t0 = time.perf_counter()
+    _, _, _, st, _ = O.solve(wl.network, wl.y[:, sub], wl.t0[sub], wl.dt0[sub], wl.t_stop[sub], wl.rtol,
+                             wl.atol, wl.dt_min, group=wl.group, nthreads=threads)
+    el = time.perf_counter() - t0
+    return ncells / el, el, int((st != 0).sum())
+
+
+def host_threads():
+    try:
+        return len(os.sched_getaffinity(0))
+    except AttributeError:
+        return os.cpu_count() or 1
+
+
+def run_reference(args):
+    rank, world, _ = dist_env()
+    if rank != 0:
+        return
+    from odevec_b200 import workloads as W
+    wl = W.primordial(ncells=args.cpu_sample, seed=3, network=args.network)
+    threads = host_threads()
+    for _ in range(args.warmup):
+        oracle_rate(wl, args.cpu_sample, threads)
+    times = []
+    for _ in range(args.steps):
+        _, el, _ = oracle_rate(wl, args.cpu_sample, threads)
+        times.append(el)
+    value = args.cpu_sample * len(times) / sum(times)
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "cells/s", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * sum(times) / len(times),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": DATA,
+        "config": {"workload": WORKLOAD % args.ncells, "network": args.network,
+                   "sample_cells_per_step": args.cpu_sample},
+        "cpu_baseline": {"value": value, "unit": "cells/s", "cores": threads, "kind": "port",
+                         "sample": "%d of the workload's cells per step, oracle/ (C restatement of "
+                                   "src/odevec.F90), per-cell control, OpenMP over cells" % args.cpu_sample},
+        "e2e": {"value": value, "unit": "cells/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def run_product(args):
+    import torch
+    import torch.distributed as dist
+    from odevec_b200 import metrics, solver as S, workloads as W
+
+    rank, world, local_rank = dist_env()
+    torch.cuda.set_device(local_rank)
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local_rank))
+    dev = torch.device("cuda", local_rank)
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    def max_over_ranks(v):
+        if world == 1:
+            return v
+        t = torch.tensor([v], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    wl = W.primordial(ncells=args.ncells, seed=3 + rank, network=args.network)
+    N = wl.ncells
+    y0 = torch.tensor(wl.y, device=dev)
+    t0 = torch.tensor(wl.t0, device=dev)
+    d0 = torch.tensor(wl.dt0, device=dev)
+    ts = torch.tensor(wl.t_stop, device=dev)
+    y = torch.empty_like(y0)
+    t = torch.empty_like(t0)
+    d = torch.empty_like(d0)
+    stream = torch.cuda.current_stream(dev)
+    forms = args.forms.split(",")
+    res = {}
+    clocks = None
+    for form in forms:
+        ode = S.Odevec(wl.network, max_cells=N, RelativeTolerance=wl.rtol, AbsoluteTolerance=wl.atol,
+                       MinimalTimestep=wl.dt_min, nvector=1, precision=form, raise_on_failure=False)
+        S.InitOdevec(ode)
+
+        def reset():
+            y.copy_(y0)
+            t.copy_(t0)
+            d.copy_(d0)
+
+        # untimed run with counters: failures and the algorithmic work
+        reset()
+        S.SolveODE(ode, t, d, ts, y, want_stats=True)
+        torch.cuda.synchronize()
+        stats = ode.stats.cpu().numpy()
+        fails = int((ode.status != 0).sum().item())
+        flops = float(metrics.flops_per_cell(wl.network, stats).sum())
+        for _ in range(args.warmup):
+            reset()
+            S.SolveODE(ode, t, d, ts, y, want_stats=False)
+        torch.cuda.synchronize()
+        barrier()
+        ev = [[torch.cuda.Event(enable_timing=True) for _ in range(3)] for _ in range(args.steps)]
+        with ClockSampler(local_rank) as cs:
+            for k in range(args.steps):
+                ev[k][0].record(stream)
+                reset()
+                ev[k][1].record(stream)
+                S.SolveODE(ode, t, d, ts, y, want_stats=False)
+                ev[k][2].record(stream)
+            torch.cuda.synchronize()
+        barrier()
+        total_s = ev[0][0].elapsed_time(ev[-1][2]) / 1e3
+        kern = [ev[k][1].elapsed_time(ev[k][2]) / 1e3 for k in range(args.steps)]
+        steps_ms = [ev[k][0].elapsed_time(ev[k][2]) for k in range(args.steps)]
+        total_s = max_over_ranks(total_s)
+        kern_mean = max_over_ranks(sum(kern) / len(kern))
+
+        # end to end through SolveODE with host buffers: pinned host -> device,
+        # solve, device -> host inside the timed region
+        yh = torch.tensor(wl.y).pin_memory()
+        th = torch.tensor(wl.t0).pin_memory()
+        dh = torch.tensor(wl.dt0).pin_memory()
+        tsh = torch.tensor(wl.t_stop).pin_memory()
+        yo = torch.empty_like(yh).pin_memory()
+        to = torch.empty_like(th).pin_memory()
+        do = torch.empty_like(dh).pin_memory()
+        sto = torch.empty(N, dtype=torch.int32).pin_memory()
+        e2e_steps = max(1, min(args.steps, 3))
+        barrier()
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(e2e_steps):
+            y.copy_(yh, non_blocking=True)
+            t.copy_(th, non_blocking=True)
+            d.copy_(dh, non_blocking=True)
+            ts.copy_(tsh, non_blocking=True)
+            S.SolveODE(ode, t, d, ts, y, want_stats=False)
+            yo.copy_(y, non_blocking=True)
+            to.copy_(t, non_blocking=True)
+            do.copy_(d, non_blocking=True)
+            sto.copy_(ode.status, non_blocking=True)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        e2e_s = max_over_ranks(e0.elapsed_time(e1) / 1e3)
+        barrier()
+        res[form] = {
+            "value": world * N * args.steps / total_s,
+            "ms_per_step": 1e3 * total_s / args.steps,
+            "kernel_ms": 1e3 * kern_mean,
+            "step_ms": steps_ms,
+            "flops_per_launch": flops,
+            "failed_cells": fails,
+            "mean_newton_iters": float(stats[:, 4].mean()),
+            "mean_jac_evals": float(stats[:, 5].mean()),
+            "mean_steps": float(stats[:, 0].mean()),
+            "fp64_share": metrics.fp64_fraction(wl.network, stats, form == "fp32_lu"),
+            "e2e": world * N * e2e_steps / e2e_s,
+            "clocks": cs.summary(),
+        }
+        if clocks is None:
+            clocks = cs.summary()
+        S.CloseOdevec(ode)
+    if rank != 0:
+        if world > 1:
+            dist.destroy_process_group()
+        return
+
+    head = forms[0]
+    r = res[head]
+    peaks = fma_peaks(torch)
+    achieved = r["flops_per_launch"] / (r["kernel_ms"] * 1e-3) / 1e12
+    tpc = traffic_per_cell()
+    alg_bytes = N * (16 * 8 * 2 + 3 * 8 + 2 * 8 + 4)
+    line = {
+        "metric": METRIC,
+        "value": r["value"],
+        "unit": "cells/s",
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": r["ms_per_step"],
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f64 state/residual/control, f32 LU" if head == "fp32_lu" else "f64",
+        "data": DATA,
+        "config": {"workload": WORKLOAD % N, "network": args.network, "form": head,
+                   "l2": "inputs %.0f MB per GPU > 126 MB L2" % (N * 19 * 8 / 1e6),
+                   "parallelism": "dp%d (independent cell shards, no exchange)" % world},
+        "roofline": {"bound": "fp64", "achieved": achieved, "peak": peaks["fp64"], "unit": "TFLOP/s",
+                     "frac": achieved / peaks["fp64"],
+                     "traffic": None if tpc is None else tpc * N,
+                     "algorithmic_flops_per_launch": r["flops_per_launch"],
+                     "algorithmic_bytes_per_launch": alg_bytes,
+                     "achieved_hbm_gbs": alg_bytes / (r["kernel_ms"] * 1e-3) / 1e9,
+                     "peak_source": "FP64 FMA-chain probe on this GPU (odevec_probe_fma); "
+                                    "MEASURED_PEAKS.json has no FP64 figure",
+                     "fp64_share_of_flops": r["fp64_share"], "fp32_peak": peaks["fp32"]},
+        "e2e": {"value": r["e2e"], "unit": "cells/s", "h2d_bytes_per_step": N * (16 + 3) * 8,
+                "d2h_bytes_per_step": N * ((16 + 2) * 8 + 4)},
+        "gpu_launches": args.steps,
+        "clocks": {k: v for k, v in r["clocks"].items() if k != "samples"},
+        "batch_latency_ms": {"p50": float(np.percentile(r["step_ms"], 50)),
+                             "p99": float(np.percentile(r["step_ms"], 99))},
+        "forms": {f: {k: v for k, v in res[f].items() if k not in ("step_ms", "clocks")} for f in forms},
+    }
+    if "fp64" in res and "fp32_lu" in res:
+        line["fp32lu_over_fp64"] = res["fp32_lu"]["value"] / res["fp64"]["value"]
+    if world == 1 and not args.no_cpu:
+        threads = host_threads()
+        v, el, f = oracle_rate(W.primordial(ncells=args.cpu_sample, seed=3, network=args.network),
+                               args.cpu_sample, threads)
+        line["cpu_baseline"] = {"value": v, "unit": "cells/s", "cores": threads, "kind": "port",
+                                "sample": "%d cells of the same workload (%.1f s)" % (args.cpu_sample, el)}
+    if world == 1 and args.accuracy_cells > 0:
+        line["accuracy"] = accuracy(args, wl, S, torch)
+    print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.destroy_process_group()
+
+
+def accuracy(args, wl, S, torch):
+    """Max relative error of each form at rtol 1e-6 against the oracle at
+    rtol 1e-12 (species above atol/rtol), on a sample of cells."""
+    from oracle import oracle as O
+    n = args.accuracy_cells
+    sub = slice(0, n)
+    ref, _, _, st, _ = O.solve(wl.network, wl.y[:, sub], wl.t0[sub], wl.dt0[sub], wl.t_stop[sub], 1e-12,
+                               1e-26, wl.dt_min, group=1, nthreads=host_threads())
+    out = {"oracle_rtol": 1e-12, "cells": n, "oracle_failures": int((st != 0).sum())}
+    for form in args.forms.split(","):
+        ode = S.Odevec(wl.network, RelativeTolerance=wl.rtol, AbsoluteTolerance=wl.atol,
+                       MinimalTimestep=wl.dt_min, nvector=1, precision=form, raise_on_failure=False)
+        S.InitOdevec(ode)
+        y = torch.tensor(wl.y[:, sub], device="cuda").contiguous()
+        S.SolveODE(ode, torch.tensor(wl.t0[sub], device="cuda"), torch.tensor(wl.dt0[sub], device="cuda"),
+                   torch.tensor(wl.t_stop[sub], device="cuda"), y)
+        g = y.cpu().numpy()
+        S.CloseOdevec(ode)
+        m = np.abs(ref[:12]) > wl.atol / wl.rtol
+        rel = np.abs(g[:12][m] - ref[:12][m]) / np.abs(ref[:12][m])
+        out[form] = {"max_rel_err": float(rel.max()), "median_rel_err": float(np.median(rel)),
+                     "max_over_rtol": float(rel.max() / wl.rtol)}
+    return out
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_product(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -57,7 +57,9 @@ extern "C" {
 
 /* stats per cell: accepted steps, predictor attempts, error-test failures,
    Newton failures, Newton iterations (right-hand-side evaluations in the
-   corrector), Jacobian+LU evaluations, final order, reserved */
+   corrector), Jacobian+LU evaluations, final order, and the number of
+   Nordsieck vector passes of the Pascal-triangle predictor and its undo
+   (sum of q(q+1)/2 over PredictSolution and ResetSystem calls) */
 #define OV_NSTATS 8
 
 /* precision forms */
@@ -112,6 +114,14 @@ int32_t odevec_close(odevec_solver* s);
 
 /* message of the last failed call on this thread */
 const char* odevec_last_error(void);
+
+/* Measurement utility, no counterpart in the reference: times `blocks` x
+   `threads` threads each running 8 independent FMA chains of `iters` steps
+   (FP64 if fp64 != 0, else FP32) on `stream`; scratch: >= blocks*8 bytes of
+   device memory (never written in practice).  Returns the duration in *ms
+   and the FLOPs executed in *flops. */
+int32_t odevec_probe_fma(int32_t fp64, int32_t blocks, int32_t threads, int32_t iters,
+                         void* scratch, void* stream, float* ms, double* flops);
 
 #ifdef __cplusplus
 }

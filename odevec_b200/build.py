@@ -96,6 +96,13 @@ def build(force: bool = False, jobs: int = 0, verbose: bool = False) -> str:
             objs.append(obj)
             if force or not os.path.exists(obj) or not os.path.exists(stamp) or open(stamp).read() != key:
                 tasks.append((src, obj, flags, obj + ".log", stamp, key))
+    probe_src = os.path.join(CSRC, "ov_probe.cu")
+    probe_obj = os.path.join(BUILD, "ov_probe.o")
+    pkey = _hash_files(hdrs + [probe_src], " ".join(COMMON))
+    if force or not os.path.exists(probe_obj) or not os.path.exists(probe_obj + ".key") or \
+            open(probe_obj + ".key").read() != pkey:
+        tasks.append((probe_src, probe_obj, ["--fmad=true"], probe_obj + ".log", probe_obj + ".key", pkey))
+    objs.append(probe_obj)
     abi_src = os.path.join(CSRC, "odevec_abi.cu")
     abi_obj = os.path.join(BUILD, "odevec_abi.o")
     key = _hash_files(hdrs + [abi_src, os.path.join(GEN, "registry.inc"),

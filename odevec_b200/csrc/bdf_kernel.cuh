@@ -122,7 +122,7 @@ struct Cell {
     double t, h, told, tstop, crate, jchg, cerr;
     int q, swu, lju, fet, fc, it;
     bool ujac, nuo, first, msk;
-    int status, attempts, steps, ltef, convf, newt, jacs;
+    int status, attempts, steps, ltef, convf, newt, jacs, ppass;
 
     /* WeightedNorm1 (src/odevec.F90:669-684) */
     __device__ __forceinline__ double wnorm(const double* e) const
@@ -165,6 +165,7 @@ struct Cell {
     /* PredictSolution (src/odevec.F90:769-793) */
     __device__ __forceinline__ void predict()
     {
+        ppass += q * (q + 1) / 2;
 #pragma unroll
         for (int l = 0; l < MAXQ; ++l)
 #pragma unroll
@@ -182,6 +183,7 @@ struct Cell {
     /* ResetSystem (src/odevec.F90:526-544) */
     __device__ __forceinline__ void reset()
     {
+        ppass += q * (q + 1) / 2;
 #pragma unroll
         for (int k = 0; k < MAXQ; ++k)
 #pragma unroll
@@ -474,7 +476,7 @@ __global__ void __launch_bounds__(128) bdf_kernel(const LaunchArgs A)
             c.tstop = A.t_stop[cell];
             c.msk = A.mask ? (A.mask[cell] != 0) : true;
             c.status = OV_OK;
-            c.attempts = c.steps = c.ltef = c.convf = c.newt = c.jacs = 0;
+            c.attempts = c.steps = c.ltef = c.convf = c.newt = c.jacs = c.ppass = 0;
             c.first = true;
             c.q = 1;
             c.swu = 0;
@@ -716,7 +718,7 @@ __global__ void __launch_bounds__(128) bdf_kernel(const LaunchArgs A)
                 s[4] = c.newt;
                 s[5] = c.jacs;
                 s[6] = c.q;
-                s[7] = 0;
+                s[7] = c.ppass;
             }
             ph = PH_IDLE;
         }

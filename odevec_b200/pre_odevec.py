@@ -500,6 +500,45 @@ def emit_cuda_header(sysm: System) -> str:
     return "\n".join(L) + "\n"
 
 
+def expr_flops(expr) -> int:
+    """Binary floating-point operations of an expression as the emitted code
+    evaluates it: n-1 per n-term sum or n-factor product (a coefficient of
+    -1 is a sign, not an operation), n-1 multiplications for x**n, one per
+    division or real power."""
+    expr = sp.sympify(expr)
+    if expr.is_Atom:
+        return 0
+    if expr.is_Add:
+        return len(expr.args) - 1 + sum(expr_flops(a) for a in expr.args)
+    if expr.is_Mul:
+        args = [a for a in expr.args if a not in (-1, 1)]
+        return max(len(args) - 1, 0) + sum(expr_flops(a) for a in args)
+    if expr.is_Pow:
+        b, e = expr.as_base_exp()
+        if e.is_Integer and int(e) > 0:
+            return int(e) - 1 + expr_flops(b)
+        return 1 + expr_flops(b)
+    return 1 + sum(expr_flops(a) for a in expr.args)
+
+
+def _line_flops(line: str) -> int:
+    rhs = line.split("=", 1)[1]
+    return rhs.count("*") + rhs.count("/") + rhs.count(" + ") + rhs.count(" - ")
+
+
+def flop_counts(sysm: System) -> Dict[str, int]:
+    """Static per-call FLOPs of the emitted routines."""
+    f_rhs = sum(expr_flops(e) for e in sysm.net.rhs)
+    pos = sysm.pos()
+    f_jac = sum(expr_flops(sysm.P_order[i, j]) for (i, j) in pos)
+    f_lu = sum(_line_flops(l) for l in _lu_factor_lines(sysm))
+    f_solve = sum(_line_flops(l) for l in _lu_solve_lines(sysm) if not l.startswith(("T d", "x[")))
+    # rates_k of the PRIMORDIAL rate model: 3 mul + 1 div for the floor, one add per rate
+    f_k = (4 + sysm.net.nrea) if sysm.net.rates else 0
+    return {"neq": sysm.neq, "nnz": sysm.nnz, "rhs": f_rhs, "jac": f_jac, "lu_factor": f_lu,
+            "lu_solve": f_solve, "rates_k": f_k}
+
+
 def write_variant(sysm: System, outdir: str = GEN_DIR) -> Tuple[str, str]:
     os.makedirs(outdir, exist_ok=True)
     cid = _cid(sysm.tag)
@@ -509,6 +548,12 @@ def write_variant(sysm: System, outdir: str = GEN_DIR) -> Tuple[str, str]:
         fh.write(emit_c_header(sysm))
     with open(cu, "w") as fh:
         fh.write(emit_cuda_header(sysm))
+    import json
+    fpath = os.path.join(outdir, "flops.json")
+    table = json.load(open(fpath)) if os.path.exists(fpath) else {}
+    table[sysm.tag] = flop_counts(sysm)
+    with open(fpath, "w") as fh:
+        json.dump(table, fh, indent=1, sort_keys=True)
     write_registry(outdir)
     return h, cu
 

@@ -107,7 +107,7 @@ typedef struct {
     const uint8_t* mask; /* group mask or NULL */
     int status;
     int64_t attempts;
-    int32_t steps, lte_fails, conv_fails, newton, jacs;
+    int32_t steps, lte_fails, conv_fails, newton, jacs, ppass;
 } ode_t;
 
 static inline double* NS(ode_t* o, int k) { return o->y_NS + (size_t)k * o->neq * o->G; }
@@ -215,6 +215,7 @@ static void calc_weights(ode_t* o, const double* y)
 static void predict(ode_t* o)
 {
     const size_t N = (size_t)o->neq * o->G;
+    o->ppass += o->order * (o->order + 1) / 2;
     for (int l = 0; l <= o->order - 1; ++l)
         for (int k = o->order; k >= l + 1; --k) {
             double *a = NS(o, k), *b = NS(o, k - 1);
@@ -229,6 +230,7 @@ static void predict(ode_t* o)
 static void reset_system(ode_t* o)
 {
     const size_t N = (size_t)o->neq * o->G;
+    o->ppass += o->order * (o->order + 1) / 2;
     for (int k = 0; k <= o->order - 1; ++k)
         for (int j = o->order; j >= k + 1; --j) {
             double *a = NS(o, j), *b = NS(o, j - 1);
@@ -772,7 +774,7 @@ int ov_oracle_solve(const char* tag, int64_t ncells, int G, double rtol, double 
             o.status = 0;
             o.order = 1; /* SolveODE starts at order 1 (src/odevec.F90:171) */
             o.attempts = 0;
-            o.steps = o.lte_fails = o.conv_fails = o.newton = o.jacs = 0;
+            o.steps = o.lte_fails = o.conv_fails = o.newton = o.jacs = o.ppass = 0;
             memset(o.y_NS, 0, sizeof(double) * N * NNS);
             memset(o.en_old, 0, sizeof(double) * N);
             double time = t[c0], h = dt[c0];
@@ -799,7 +801,7 @@ int ov_oracle_solve(const char* tag, int64_t ncells, int G, double rtol, double 
                     s[4] = o.newton;
                     s[5] = o.jacs;
                     s[6] = o.order;
-                    s[7] = 0;
+                    s[7] = o.ppass;
                 }
             }
         }
