@@ -76,6 +76,22 @@ typedef struct odevec_opts {
     int32_t group_size;       /* 1 or 32; 0: the variant's --nvector (1 if not 32) */
     int32_t precision;        /* OV_PREC_* */
     int32_t max_attempts;     /* cap on predictor attempts per cell or group; 0: 1000000 */
+    /* scheduling of per-cell control (group_size 1), no effect on results:
+       the Jacobian+LU and the step-size selection run for the waiting cells
+       of a warp together once jac_batch / ss_batch of its 32 cells wait, no
+       other cell can progress, or a cell has waited max_wait iterations.
+       0: defaults (12, 12, 4); 1, 1, 0 runs each cell's block at once. */
+    int32_t jac_batch;
+    int32_t ss_batch;
+    int32_t max_wait;
+    /* launch shape, no effect on results: staging 0 = automatic, 1 = per-cell
+       arrays in registers / local memory, 2 = in shared memory (per-cell
+       control, one 128-thread block per SM, where they fit); block_threads
+       (a multiple of 32 up to 128) and grid_blocks 0 = automatic (persistent
+       grid filling every SM) */
+    int32_t staging;
+    int32_t block_threads;
+    int32_t grid_blocks;
 } odevec_opts;
 
 typedef struct odevec_solver odevec_solver;

@@ -5,25 +5,34 @@
  * group of 32 cells that share them through max-norms over the warp
  * (G = 32: the reference's semantics with nvector = 32, reductions with
  * __shfl_xor_sync).  The grid is persistent: idle lanes take the next cells
- * from a global counter (warp-aggregated atomicAdd), so a warp keeps all 32
+ * from a global counter (warp-aggregated atomicAdd), so a warp keeps its
  * lanes busy while cells of very different stiffness finish at different
  * times.
  *
  * The reference's nested loops (src/odevec.F90: step loop :207, predictor
  * retry loop :259, corrector loop :321) are flattened into a per-lane state
- * machine.  Each trip of the kernel's main loop performs for every lane at
- * most one predictor (with its Jacobian and LU), one right-hand-side
- * evaluation and one Newton update, so lanes in different phases still
- * execute the expensive right-hand side, solve and factorisation code
- * together, and the cheap control code diverges.  The arithmetic per cell is
- * that of src/odevec.F90 operation by operation; with --fmad=false it is
- * bit-identical to the CPU oracle.
+ * machine.  Each trip of the main loop performs for every lane at most one
+ * predictor, one right-hand-side evaluation and one Newton update, so lanes
+ * in different phases still run the right-hand side and the solve together.
+ * The two expensive and rarely needed blocks -- Jacobian + LU factorisation
+ * and step-size/order selection -- exist once in the code; a lane that needs
+ * one waits until enough lanes of its warp need it (jac_batch / ss_batch),
+ * no lane can progress otherwise, or it has waited max_wait trips, and then
+ * all waiting lanes run it together.  Waiting changes only the interleaving
+ * across lanes, never a cell's own sequence of operations: the arithmetic
+ * per cell is that of src/odevec.F90 operation by operation, and with
+ * --fmad=false it is bit-identical to the CPU oracle.
+ *
+ * Species whose right-hand side is identically zero and on which nothing
+ * depends (the network header's frozen(); PRIMORDIAL's CR, g, Tgas, dummy)
+ * are not part of the solver state: their corrections are exact zeros in
+ * the reference, so leaving them out changes no result.  Norms still divide
+ * by the full neq.
  *
  * Per-cell state lives in thread-local arrays with compile-time indices
  * (Nordsieck history y_NS(0:5), en, en_old, error weights, packed LU);
  * loops over the runtime order are unrolled to the maximum order with
- * predicates so no array is indexed dynamically.  Small networks stay in
- * registers; larger ones spill to local memory (L1).
+ * predicates so no array is indexed dynamically.
  *
  * Every loop is bounded: at most max_attempts predictor attempts per cell
  * (status OV_ERR_MAX_STEPS), at most 4 Newton iterations per attempt and 10
@@ -45,18 +54,23 @@
 namespace ov {
 namespace OV_MODE_NS {
 
-constexpr int MAXQ = 5;           /* maxorder, pre_odevec.py:83 */
+constexpr int MAXQ = 5; /* maxorder, pre_odevec.py:83 */
 constexpr unsigned FULL = 0xffffffffu;
 
 enum Phase : int {
-    PH_IDLE = 0,     /* no cell */
-    PH_START = 1,    /* cell loaded: initial right-hand side pending */
-    PH_PRED = 2,     /* next: predictor attempt */
-    PH_NEWTON = 3,   /* next: right-hand side + Newton update */
-    PH_RESTART = 4,  /* next: right-hand side at the predicted state (3 error-test failures) */
-    PH_DONE = 5,     /* finished (status says how) */
-    PH_EXHAUSTED = 6 /* no cells left */
+    PH_IDLE = 0,      /* no cell */
+    PH_START = 1,     /* cell loaded: initial right-hand side pending */
+    PH_PRED = 2,      /* next: predictor attempt */
+    PH_JACWAIT = 3,   /* predicted; waits for the Jacobian + LU block */
+    PH_NEWTON = 4,    /* next: right-hand side + Newton update */
+    PH_RESTART = 5,   /* next: right-hand side at the predicted state (3 error-test failures) */
+    PH_SSWAIT = 6,    /* waits for the step-size/order selection block */
+    PH_DONE = 7,      /* finished (status says how) */
+    PH_EXHAUSTED = 8  /* no cells left */
 };
+
+/* why a lane waits for the step-size selection */
+enum SsMode : int { SS_REJECT = 1, SS_RESTART = 2, SS_ACCEPT = 3 };
 
 /* Nordsieck l-vectors l(q, 0:q), q = 1..6 (src/odevec.F90:127-134) */
 static __constant__ double c_lcoef[7][7] = {
@@ -69,6 +83,9 @@ static __constant__ double c_lcoef[7][7] = {
     {20.0 / 49.0, 1.0, 58.0 / 63.0, 5.0 / 12.0, 25.0 / 252.0, 1.0 / 84.0, 1.0 / 1764.0}};
 
 __device__ __forceinline__ double lcoef(int q, int k) { return c_lcoef[q][k]; }
+
+/* x^y out of line: the step-size selection calls it three times */
+static __device__ __noinline__ double pow_dev(double x, double y) { return ov_pow(x, y); }
 
 /* tau (src/odevec.F90:1034-1054) */
 __device__ __forceinline__ double tau(int order, int order2)
@@ -106,31 +123,74 @@ __device__ __forceinline__ bool group_any(bool b)
     return b;
 }
 
-template <class Net, int G, class LUT>
+/* Shared-memory staging: per-lane arrays laid out [entry][lane] with a
+   stride of the block size, so a warp's 32 lanes touch 32 consecutive
+   words (no bank conflicts). */
+constexpr int SHM_BLOCK = 128;
+
+template <class T>
+struct LaneCol {
+    T* base; /* &array[0][threadIdx.x] */
+    __device__ __forceinline__ T& operator[](int i) const { return base[i * SHM_BLOCK]; }
+};
+
+template <int ND>
+struct LaneHist {
+    double* base;
+    __device__ __forceinline__ LaneCol<double> operator[](int k) const
+    {
+        return LaneCol<double>{base + k * ND * SHM_BLOCK};
+    }
+};
+
+template <class Net, class LUT, bool SHM>
+struct Staging;
+
+template <class Net, class LUT>
+struct Staging<Net, LUT, false> { /* thread-local arrays (registers / local memory) */
+    using Hist = double (*)[Net::ND];
+    using LU = LUT*;
+    static constexpr size_t smem_bytes = 0;
+};
+
+template <class Net, class LUT>
+struct Staging<Net, LUT, true> { /* shared memory, [entry][lane] */
+    using Hist = LaneHist<Net::ND>;
+    using LU = LaneCol<LUT>;
+    static constexpr size_t hist_bytes = sizeof(double) * (MAXQ + 1) * Net::ND * SHM_BLOCK;
+    static constexpr size_t smem_bytes = hist_bytes + sizeof(LUT) * Net::NNZ * SHM_BLOCK;
+};
+
+template <class Net, int G, class LUT, bool SHM = false>
 struct Cell {
-    static constexpr int N = Net::NEQ;
+    static constexpr int N = Net::NEQ;  /* full state */
+    static constexpr int ND = Net::ND;  /* solver state */
+    static constexpr int NF = Net::NF;
     static constexpr int NNZ = Net::NNZ;
     static constexpr int NR = Net::NREA > 0 ? Net::NREA : 1;
     static constexpr bool SCALED = sizeof(LUT) == 4;
 
-    double yns[MAXQ + 1][N];
-    double en[N], eno[N], w2[N], y[N], f[N];
-    LUT a[NNZ];
+    typename Staging<Net, LUT, SHM>::Hist yns; /* Nordsieck history y_NS(0:5) */
+    double en[ND], eno[ND], w2[ND];
+    double y[N];
+    typename Staging<Net, LUT, SHM>::LU a;     /* packed LU of the iteration matrix */
     double rT[NR];
-    double sc[SCALED ? N : 1], isc[SCALED ? N : 1];
+    double sc[SCALED ? ND : 1], isc[SCALED ? ND : 1];
 
     double t, h, told, tstop, crate, jchg, cerr;
-    int q, swu, lju, fet, fc, it;
-    bool ujac, nuo, first, msk;
+    double fz_add; /* 0, or NaN when a frozen species has a non-finite error weight */
+    int q, swu, lju, fet, fc, it, ss_mode, wait;
+    bool ujac, nuo, first, msk, fz_neg;
     int status, attempts, steps, ltef, convf, newt, jacs, ppass;
 
-    /* WeightedNorm1 (src/odevec.F90:669-684) */
+    /* WeightedNorm1 (src/odevec.F90:669-684) over the solver state */
     __device__ __forceinline__ double wnorm(const double* e) const
     {
         double s = 0.0;
 #pragma unroll
-        for (int j = 0; j < N; ++j)
+        for (int j = 0; j < ND; ++j)
             s = s + e[j] * e[j] * w2[j];
+        s = s + fz_add;
         double v = msk ? sqrt(s / N) : -HUGE_VAL;
         return group_max<G>(v);
     }
@@ -140,14 +200,11 @@ struct Cell {
     {
         double s = 0.0;
 #pragma unroll
-        for (int j = 0; j < N; ++j) {
-            double e = 0.0;
-#pragma unroll
-            for (int k = 0; k <= MAXQ; ++k)
-                if (k == col)
-                    e = yns[k][j];
+        for (int j = 0; j < ND; ++j) {
+            const double e = yns[col][j];
             s = s + e * e * w2[j];
         }
+        s = s + fz_add;
         double v = msk ? sqrt(s / N) : -HUGE_VAL;
         return group_max<G>(v);
     }
@@ -156,27 +213,54 @@ struct Cell {
     __device__ __forceinline__ void weights(double rtol, double atol)
     {
 #pragma unroll
-        for (int j = 0; j < N; ++j) {
-            double w = 1.0 / (rtol * fabs(y[j]) + atol);
+        for (int j = 0; j < ND; ++j) {
+            double w = 1.0 / (rtol * fabs(y[Net::dyn(j)]) + atol);
             w2[j] = w * w;
         }
     }
 
-    /* PredictSolution (src/odevec.F90:769-793) */
+    /* frozen species: constant state, so their weights and signs are fixed */
+    __device__ __forceinline__ void frozen_flags(double rtol, double atol)
+    {
+        bool bad = false, neg = false;
+#pragma unroll
+        for (int j = 0; j < NF; ++j) {
+            const double v = y[Net::frozen(j)];
+            double w = 1.0 / (rtol * fabs(v) + atol);
+            w = w * w;
+            bad |= !(w - w == 0.0); /* inf or NaN */
+            neg |= v < 0.0;
+        }
+        fz_add = bad ? __longlong_as_double(0x7ff8000000000000LL) : 0.0;
+        fz_neg = neg;
+    }
+
+    /* PredictSolution (src/odevec.F90:769-793): per species, the Pascal
+       triangle y_NS(k-1) += y_NS(k) for l = 0..q-1, k = q..l+1, in the
+       reference's order, on register copies of the history.  The history is
+       indexed by runtime order only; species indices stay compile-time so
+       en, w2 and y remain in registers. */
     __device__ __forceinline__ void predict()
     {
         ppass += q * (q + 1) / 2;
+#pragma unroll 4
+        for (int j = 0; j < ND; ++j) {
+            double v[MAXQ + 1];
 #pragma unroll
-        for (int l = 0; l < MAXQ; ++l)
+            for (int k = 0; k <= MAXQ; ++k)
+                v[k] = yns[k][j];
 #pragma unroll
-            for (int k = MAXQ; k >= 1; --k)
-                if (l <= q - 1 && k <= q && k >= l + 1) {
+            for (int l = 0; l < MAXQ; ++l)
 #pragma unroll
-                    for (int j = 0; j < N; ++j)
-                        yns[k - 1][j] = yns[k][j] + yns[k - 1][j];
-                }
+                for (int k = MAXQ; k >= 1; --k)
+                    if (l <= q - 1 && k <= q && k >= l + 1)
+                        v[k - 1] = v[k] + v[k - 1];
 #pragma unroll
-        for (int j = 0; j < N; ++j)
+            for (int k = 0; k < MAXQ; ++k)
+                yns[k][j] = v[k];
+        }
+#pragma unroll
+        for (int j = 0; j < ND; ++j)
             en[j] = 0.0;
     }
 
@@ -184,29 +268,35 @@ struct Cell {
     __device__ __forceinline__ void reset()
     {
         ppass += q * (q + 1) / 2;
+#pragma unroll 4
+        for (int j = 0; j < ND; ++j) {
+            double v[MAXQ + 1];
 #pragma unroll
-        for (int k = 0; k < MAXQ; ++k)
+            for (int k = 0; k <= MAXQ; ++k)
+                v[k] = yns[k][j];
 #pragma unroll
-            for (int jj = MAXQ; jj >= 1; --jj)
-                if (k <= q - 1 && jj <= q && jj >= k + 1) {
+            for (int k = 0; k < MAXQ; ++k)
 #pragma unroll
-                    for (int j = 0; j < N; ++j)
-                        yns[jj - 1][j] = yns[jj - 1][j] - yns[jj][j];
-                }
+                for (int jj = MAXQ; jj >= 1; --jj)
+                    if (k <= q - 1 && jj <= q && jj >= k + 1)
+                        v[jj - 1] = v[jj - 1] - v[jj];
+#pragma unroll
+            for (int k = 0; k < MAXQ; ++k)
+                yns[k][j] = v[k];
+        }
     }
 
     /* SetStepSize (src/odevec.F90:720-743) */
     __device__ __forceinline__ void set_step(double dt_scale)
     {
         double dtt = 1.0;
+#pragma unroll 1
+        for (int k = 1; k <= q; ++k) {
+            dtt = dt_scale * dtt;
 #pragma unroll
-        for (int k = 1; k <= MAXQ; ++k)
-            if (k <= q) {
-                dtt = dt_scale * dtt;
-#pragma unroll
-                for (int j = 0; j < N; ++j)
-                    yns[k][j] = yns[k][j] * dtt;
-            }
+            for (int j = 0; j < ND; ++j)
+                yns[k][j] = yns[k][j] * dtt;
+        }
         h = h * dt_scale;
         jchg = jchg * dt_scale;
     }
@@ -214,14 +304,13 @@ struct Cell {
     /* UpdateNordsieck (src/odevec.F90:747-765) */
     __device__ __forceinline__ void update_nordsieck()
     {
+#pragma unroll 1
+        for (int k = 0; k <= q; ++k) {
+            const double c = lcoef(q, k);
 #pragma unroll
-        for (int k = 0; k <= MAXQ; ++k)
-            if (k <= q) {
-                const double c = lcoef(q, k);
-#pragma unroll
-                for (int j = 0; j < N; ++j)
-                    yns[k][j] = yns[k][j] + en[j] * c;
-            }
+            for (int j = 0; j < ND; ++j)
+                yns[k][j] = yns[k][j] + en[j] * c;
+        }
     }
 
     /* CalcStepSizeOrder (src/odevec.F90:547-618); returns dt_scale.  The
@@ -233,17 +322,17 @@ struct Cell {
         if (order == 1)
             down = 0.0;
         else
-            down = 1.0 / ((double)1.3f * ov_pow(wnorm_ns(order) / tau(order, order - 1), 1.0 / order)
+            down = 1.0 / ((double)1.3f * pow_dev(wnorm_ns(order) / tau(order, order - 1), 1.0 / order)
                           + 1e-6);
-        same = 1.0 / ((double)1.2f * ov_pow(wnorm(en) / tau(order, order), 1.0 / (order + 1.0)) + 1e-6);
+        same = 1.0 / ((double)1.2f * pow_dev(wnorm(en) / tau(order, order), 1.0 / (order + 1.0)) + 1e-6);
         if (order == MAXQ || nuo)
             up = 0.0;
         else {
-            double d[N];
+            double d[ND];
 #pragma unroll
-            for (int j = 0; j < N; ++j)
+            for (int j = 0; j < ND; ++j)
                 d[j] = en[j] - eno[j];
-            up = 1.0 / ((double)1.4f * ov_pow(wnorm(d) / tau(order, order + 1), 1.0 / (order + 2.0))
+            up = 1.0 / ((double)1.4f * pow_dev(wnorm(d) / tau(order, order + 1), 1.0 / (order + 2.0))
                         + 1e-6);
         }
         int loc = 1;
@@ -263,12 +352,8 @@ struct Cell {
                 if (order != MAXQ) {
                     const double c = lcoef(order, order);
 #pragma unroll
-                    for (int k = 2; k <= MAXQ; ++k)
-                        if (k == order + 1) {
-#pragma unroll
-                            for (int j = 0; j < N; ++j)
-                                yns[k][j] = c * en[j] / (order + 1.0);
-                        }
+                    for (int j = 0; j < ND; ++j)
+                        yns[order + 1][j] = c * en[j] / (order + 1.0);
                     q = order + 1;
                 } else
                     status = OV_ERR_ORDER;
@@ -300,9 +385,9 @@ struct Cell {
         }
         const double r15 = 1.5 * crate;
         const double crit = err * (1.0 < r15 ? 1.0 : r15) / (tau(q, q) / (2.0 * (q + 2.0)));
-        bool nan = false;
+        bool nan = fz_add != fz_add;
 #pragma unroll
-        for (int j = 0; j < N; ++j)
+        for (int j = 0; j < ND; ++j)
             nan |= (d[j] != d[j]) | (w2[j] != w2[j]);
         if (group_any<G>(nan)) {
             failed = true;
@@ -325,19 +410,19 @@ struct Cell {
 
     __device__ __forceinline__ bool any_negative_yns0() const
     {
-        bool neg = false;
+        bool neg = fz_neg;
 #pragma unroll
-        for (int j = 0; j < N; ++j)
+        for (int j = 0; j < ND; ++j)
             neg |= yns[0][j] < 0.0;
         return group_any<G>(msk && neg);
     }
 
     __device__ __forceinline__ bool any_negative_y() const
     {
-        bool neg = false;
+        bool neg = fz_neg;
 #pragma unroll
-        for (int j = 0; j < N; ++j)
-            neg |= y[j] < 0.0;
+        for (int j = 0; j < ND; ++j)
+            neg |= y[Net::dyn(j)] < 0.0;
         return group_any<G>(msk && neg);
     }
 
@@ -347,55 +432,56 @@ struct Cell {
         double k[NR];
         Net::rates_k(y, rT, k);
         if constexpr (!SCALED) {
-            Net::jac(y, k, lcoef(q, 0), h, a);
+            Net::template jac<LUT>(y, k, lcoef(q, 0), h, a);
         } else {
             /* scale by powers of two close to the error weights (exact in
                FP64), then round to FP32 */
 #pragma unroll
-            for (int j = 0; j < N; ++j) {
+            for (int j = 0; j < ND; ++j) {
                 int e = (int)((ov_d2bits(w2[j]) >> 52) & 0x7ff) - 1023;
                 int hexp = e >= 0 ? e / 2 : -((-e + 1) / 2);
                 hexp = hexp > 480 ? 480 : (hexp < -480 ? -480 : hexp);
                 sc[j] = ov_pow2i(hexp);
                 isc[j] = ov_pow2i(-hexp);
             }
-            double P[NNZ];
-            Net::jac(y, k, lcoef(q, 0), h, P);
-            Net::template store_scaled<LUT>(P, a, sc, isc);
+            Net::template jac_scaled<LUT>(y, k, lcoef(q, 0), h, a, sc, isc);
         }
         Net::template lu_factor<LUT>(a);
     }
 
     /* residual, solve, Newton update (src/odevec.F90:323-352) */
-    __device__ __forceinline__ void newton_update(double* den)
+    __device__ __forceinline__ void newton_update(const double* f, double* den)
     {
-        double res[N];
+        double res[ND];
 #pragma unroll
-        for (int j = 0; j < N; ++j)
-            res[j] = h * f[j] - (yns[1][j] + en[j]);
+        for (int j = 0; j < ND; ++j)
+            res[j] = h * f[Net::dyn(j)] - (yns[1][j] + en[j]);
         if constexpr (SCALED)
             Net::template lu_solve<LUT>(a, res, den, sc, isc);
         else
             Net::template lu_solve<LUT>(a, res, den, nullptr, nullptr);
         const double l0 = lcoef(q, 0);
 #pragma unroll
-        for (int j = 0; j < N; ++j) {
+        for (int j = 0; j < ND; ++j) {
             en[j] = en[j] + den[j];
             if (msk)
-                y[j] = yns[0][j] + l0 * en[j];
+                y[Net::dyn(j)] = yns[0][j] + l0 * en[j];
         }
     }
 
     /* CalcInitialStepSize (src/odevec.F90:216-238), f holds f(y) */
-    __device__ __forceinline__ double initial_step(double rtol, double atol)
+    __device__ __forceinline__ double initial_step(const double* f, double rtol, double atol)
     {
         weights(rtol, atol);
         const double tol = rtol;
         const double W0 = fabs(t) > fabs(tstop) ? fabs(t) : fabs(tstop);
         double s = 0.0;
 #pragma unroll
-        for (int j = 0; j < N; ++j)
-            s = s + f[j] * f[j] * (w2[j] * tol * tol);
+        for (int j = 0; j < ND; ++j) {
+            const double fj = f[Net::dyn(j)];
+            s = s + fj * fj * (w2[j] * tol * tol);
+        }
+        s = s + fz_add;
         const double mx = group_max<G>(msk ? s : -HUGE_VAL);
         const double d = sqrt(tol / (1.0 / (W0 * W0) + mx / N));
         const double span = fabs(tstop - t);
@@ -407,31 +493,64 @@ struct Cell {
     {
         const double rel_t = (tstop - t) / h;
 #pragma unroll
-        for (int j = 0; j < N; ++j) {
-            double acc = 0.0;
-#pragma unroll
-            for (int k = 0; k <= MAXQ; ++k)
-                if (k == q)
-                    acc = yns[k][j];
-#pragma unroll
-            for (int k = MAXQ - 1; k >= 0; --k)
-                if (k < q)
-                    acc = yns[k][j] + rel_t * acc;
+        for (int j = 0; j < ND; ++j) {
+            double acc = yns[q][j];
+#pragma unroll 1
+            for (int k = q - 1; k >= 0; --k)
+                acc = yns[k][j] + rel_t * acc;
             if (msk)
-                y[j] = acc;
+                y[Net::dyn(j)] = acc;
         }
+    }
+
+    /* end of an accepted step (src/odevec.F90:452-464, loop test :207) */
+    __device__ __forceinline__ int finish_step(bool& write_y)
+    {
+        fet = 0;
+        steps++;
+        if (lju >= 20)
+            ujac = true;
+        else if (fabs(jchg - (double)1.0f) > (double)0.3f) /* 1.0 and 0.3 are single precision */
+            ujac = true;
+#pragma unroll
+        for (int j = 0; j < ND; ++j)
+            eno[j] = en[j];
+        if (t < tstop) {
+            told = t;
+            return PH_PRED;
+        }
+        write_y = true;
+        interpolate();
+        t = tstop;
+        return PH_DONE;
     }
 };
 
-template <class Net, int G, class LUT>
-__global__ void __launch_bounds__(128) bdf_kernel(const LaunchArgs A)
+/* number of lanes of the warp for which b holds */
+__device__ __forceinline__ int warp_count(bool b) { return __popc(__ballot_sync(FULL, b)); }
+
+template <class Net, int G, class LUT, bool SHM>
+__global__ void __launch_bounds__(128, SHM ? 1 : 2) bdf_kernel(const LaunchArgs A)
 {
-    using C = Cell<Net, G, LUT>;
+    using C = Cell<Net, G, LUT, SHM>;
     constexpr int N = C::N;
+    constexpr int ND = C::ND;
     const int lane = threadIdx.x & 31;
     const int64_t ncells = A.ncells;
 
     C c;
+    if constexpr (SHM) {
+        extern __shared__ __align__(16) unsigned char ov_smem[];
+        c.yns = LaneHist<ND>{reinterpret_cast<double*>(ov_smem) + threadIdx.x};
+        c.a = LaneCol<LUT>{reinterpret_cast<LUT*>(ov_smem + Staging<Net, LUT, true>::hist_bytes)
+                           + threadIdx.x};
+    }
+    double history[SHM ? 1 : MAXQ + 1][ND];
+    LUT lu_local[SHM ? 1 : C::NNZ];
+    if constexpr (!SHM) {
+        c.yns = history;
+        c.a = lu_local;
+    }
     int ph = PH_IDLE;
     int64_t cell = -1;
     bool write_y = false;
@@ -489,13 +608,15 @@ __global__ void __launch_bounds__(128) bdf_kernel(const LaunchArgs A)
             c.lju = 0;
             c.cerr = 0.0;
             c.it = 0;
+            c.wait = 0;
+            c.ss_mode = 0;
 #pragma unroll
             for (int k = 0; k <= MAXQ; ++k)
 #pragma unroll
-                for (int j = 0; j < N; ++j)
+                for (int j = 0; j < ND; ++j)
                     c.yns[k][j] = 0.0;
 #pragma unroll
-            for (int j = 0; j < N; ++j)
+            for (int j = 0; j < ND; ++j)
                 c.eno[j] = 0.0;
             write_y = false;
             bool skip = !group_any<G>(c.msk);
@@ -509,6 +630,7 @@ __global__ void __launch_bounds__(128) bdf_kernel(const LaunchArgs A)
             }
             if (ph == PH_START) {
                 c.weights(A.rtol, A.atol);
+                c.frozen_flags(A.rtol, A.atol);
                 if (skip) {
                     c.t = c.tstop; /* src/odevec.F90:187-191 */
                     ph = PH_DONE;
@@ -516,13 +638,13 @@ __global__ void __launch_bounds__(128) bdf_kernel(const LaunchArgs A)
                     if (Net::NREA > 0)
                         Net::rates_T(c.y, c.rT);
 #pragma unroll
-                    for (int j = 0; j < N; ++j)
-                        c.yns[0][j] = c.y[j];
+                    for (int j = 0; j < ND; ++j)
+                        c.yns[0][j] = c.y[Net::dyn(j)];
                 }
             }
         }
 
-        /* ---- 2. predictor attempt (src/odevec.F90:259-315) ----------- */
+        /* ---- 2. predictor attempt (src/odevec.F90:259-299) ----------- */
         if (ph == PH_PRED) {
             if (++c.attempts > A.max_attempts) {
                 c.status = OV_ERR_MAX_STEPS;
@@ -542,37 +664,55 @@ __global__ void __launch_bounds__(128) bdf_kernel(const LaunchArgs A)
                 } else {
                     if (c.msk) {
 #pragma unroll
-                        for (int j = 0; j < N; ++j)
-                            c.y[j] = c.yns[0][j];
-                    }
-                    if (c.ujac) {
-                        c.jacobian_lu();
-                        c.jacs++;
-                        c.ujac = false;
-                        c.lju = 0;
-                        c.crate = 0.7;
-                        c.jchg = 1.0;
+                        for (int j = 0; j < ND; ++j)
+                            c.y[Net::dyn(j)] = c.yns[0][j];
                     }
                     c.it = 0;
-                    ph = PH_NEWTON;
+                    ph = c.ujac ? PH_JACWAIT : PH_NEWTON;
+                    c.wait = 0;
                 }
             }
         }
 
-        /* ---- 3. right-hand side ------------------------------------- */
+        /* ---- 3. Jacobian + LU for the waiting lanes (:301-315) ------- */
+        {
+            bool run;
+            if (G == 1) {
+                const int waiting = warp_count(ph == PH_JACWAIT);
+                const int moving = warp_count(ph == PH_NEWTON || ph == PH_START || ph == PH_RESTART);
+                const bool aged = __any_sync(FULL, ph == PH_JACWAIT && c.wait >= A.max_wait);
+                run = waiting > 0 && (waiting >= A.jac_batch || moving == 0 || aged);
+            } else {
+                run = ph == PH_JACWAIT;
+            }
+            if (run && ph == PH_JACWAIT) {
+                c.jacobian_lu();
+                c.jacs++;
+                c.ujac = false;
+                c.lju = 0;
+                c.crate = 0.7;
+                c.jchg = 1.0;
+                ph = PH_NEWTON;
+            } else if (ph == PH_JACWAIT) {
+                c.wait++;
+            }
+        }
+
+        /* ---- 4. right-hand side ------------------------------------- */
+        double f[N];
         if (ph == PH_START || ph == PH_NEWTON || ph == PH_RESTART) {
             double k[C::NR];
             Net::rates_k(c.y, c.rT, k);
-            Net::rhs(c.y, k, c.f);
+            Net::rhs(c.y, k, f);
         }
 
-        /* ---- 4. consume it ------------------------------------------ */
+        /* ---- 5. consume it ------------------------------------------ */
         if (ph == PH_START) {
             /* src/odevec.F90:201-210 */
 #pragma unroll
-            for (int j = 0; j < N; ++j)
-                c.yns[1][j] = c.h * c.f[j];
-            c.h = c.initial_step(A.rtol, A.atol);
+            for (int j = 0; j < ND; ++j)
+                c.yns[1][j] = c.h * f[Net::dyn(j)];
+            c.h = c.initial_step(f, A.rtol, A.atol);
             if (c.t < c.tstop) {
                 c.told = c.t;
                 ph = PH_PRED;
@@ -583,23 +723,18 @@ __global__ void __launch_bounds__(128) bdf_kernel(const LaunchArgs A)
                 ph = PH_DONE;
             }
         } else if (ph == PH_RESTART) {
-            /* src/odevec.F90:417-421, 434-439 */
+            /* src/odevec.F90:417-421 */
 #pragma unroll
-            for (int j = 0; j < N; ++j)
-                c.yns[1][j] = c.h * c.f[j];
+            for (int j = 0; j < ND; ++j)
+                c.yns[1][j] = c.h * f[Net::dyn(j)];
             c.ujac = true;
-            const double s = c.step_size_order();
-            if (c.status) {
-                ph = PH_DONE;
-            } else {
-                c.set_step(s);
-                c.fet++;
-                ph = PH_PRED;
-            }
+            c.ss_mode = SS_RESTART;
+            c.wait = 0;
+            ph = PH_SSWAIT;
         } else if (ph == PH_NEWTON) {
             c.newt++;
-            double den[N];
-            c.newton_update(den);
+            double den[ND];
+            c.newton_update(f, den);
             bool failed = false, converged = false;
             c.check_convergence(den, failed, converged);
             if (A.check_neg && c.any_negative_y()) {
@@ -633,76 +768,76 @@ __global__ void __launch_bounds__(128) bdf_kernel(const LaunchArgs A)
                 c.weights(A.rtol, A.atol);
                 if (error > 1.0) {
                     c.ltef++;
+                    c.t = c.told;
                     if (c.fet >= 3) {
-                        c.t = c.told;
                         c.q = 1;
                         if (c.msk) {
 #pragma unroll
-                            for (int j = 0; j < N; ++j)
-                                c.y[j] = c.yns[0][j];
+                            for (int j = 0; j < ND; ++j)
+                                c.y[Net::dyn(j)] = c.yns[0][j];
                         }
                         ph = PH_RESTART;
                     } else {
-                        c.t = c.told;
                         c.reset();
                         c.ujac = true;
                         c.swu = 0;
                         c.nuo = true;
-                        const double s = c.step_size_order();
-                        if (c.status) {
-                            ph = PH_DONE;
-                        } else {
-                            c.set_step(s);
-                            c.fet++;
-                            ph = PH_PRED;
-                        }
+                        c.ss_mode = SS_REJECT;
+                        c.wait = 0;
+                        ph = PH_SSWAIT;
                     }
                 } else {
                     c.swu++;
                     c.lju++;
                     c.update_nordsieck();
                     if (c.swu == c.q + 1) {
-                        const double s = c.step_size_order();
-                        if (!c.status)
-                            c.set_step(s);
-                    }
-                    if (c.status) {
-                        ph = PH_DONE;
+                        c.ss_mode = SS_ACCEPT;
+                        c.wait = 0;
+                        ph = PH_SSWAIT;
                     } else {
-                        c.fet = 0;
-                        c.steps++;
-                        /* src/odevec.F90:458-464; 1.0 and 0.3 are single precision */
-                        if (c.lju >= 20)
-                            c.ujac = true;
-                        else if (fabs(c.jchg - (double)1.0f) > (double)0.3f)
-                            c.ujac = true;
-#pragma unroll
-                        for (int j = 0; j < N; ++j)
-                            c.eno[j] = c.en[j];
-                        if (c.t < c.tstop) {
-                            c.told = c.t;
-                            ph = PH_PRED;
-                        } else {
-                            write_y = true;
-                            c.interpolate();
-                            c.t = c.tstop;
-                            ph = PH_DONE;
-                        }
+                        ph = c.finish_step(write_y);
                     }
                 }
             }
             /* else: next Newton iteration on the next trip */
         }
 
-        /* ---- 5. store finished cells -------------------------------- */
+        /* ---- 6. step-size / order selection for the waiting lanes --- */
+        {
+            bool run;
+            if (G == 1) {
+                const int waiting = warp_count(ph == PH_SSWAIT);
+                const int moving = warp_count(ph == PH_PRED || ph == PH_NEWTON || ph == PH_RESTART);
+                const bool aged = __any_sync(FULL, ph == PH_SSWAIT && c.wait >= A.max_wait);
+                run = waiting > 0 && (waiting >= A.ss_batch || moving == 0 || aged);
+            } else {
+                run = ph == PH_SSWAIT;
+            }
+            if (run && ph == PH_SSWAIT) {
+                const double s = c.step_size_order();
+                if (c.status) {
+                    ph = PH_DONE;
+                } else {
+                    c.set_step(s);
+                    if (c.ss_mode == SS_ACCEPT) {
+                        ph = c.finish_step(write_y);
+                    } else {
+                        c.fet++; /* src/odevec.F90:434-439 */
+                        ph = PH_PRED;
+                    }
+                }
+            } else if (ph == PH_SSWAIT) {
+                c.wait++;
+            }
+        }
+
+        /* ---- 7. store finished cells -------------------------------- */
         if (ph == PH_DONE) {
             const bool ok = c.status == OV_OK;
-            if (!ok || write_y) {
-                if (c.msk) {
+            if ((!ok || write_y) && c.msk) {
 #pragma unroll
-                    for (int j = 0; j < N; ++j)
-                        A.y[(int64_t)j * ncells + cell] = c.y[j];
-                }
+                for (int j = 0; j < ND; ++j)
+                    A.y[(int64_t)Net::dyn(j) * ncells + cell] = c.y[Net::dyn(j)];
             }
             A.t[cell] = c.t;
             if (c.status != OV_ERR_GROUP_MISMATCH)
@@ -726,23 +861,30 @@ __global__ void __launch_bounds__(128) bdf_kernel(const LaunchArgs A)
 }
 
 /* Launch helper: persistent grid of (SMs x resident blocks) unless given. */
-template <class Net, int G, class LUT>
+template <class Net, int G, class LUT, bool SHM>
 cudaError_t launch(const LaunchArgs& a, int block, int grid, cudaStream_t stream)
 {
-    auto kern = bdf_kernel<Net, G, LUT>;
-    if (block <= 0)
+    auto kern = bdf_kernel<Net, G, LUT, SHM>;
+    constexpr size_t smem = Staging<Net, LUT, SHM>::smem_bytes;
+    if (SHM)
+        block = SHM_BLOCK;
+    else if (block <= 0)
         block = 128;
-    if (grid <= 0) {
-        static int cached_grid[2] = {0, 0};
-        int dev = 0;
+    static int cached_grid[2] = {0, 0};
+    if (cached_grid[0] == 0 || cached_grid[1] != block) {
+        int dev = 0, sms = 0, per_sm = 0;
         cudaGetDevice(&dev);
-        if (cached_grid[0] == 0 || cached_grid[1] != block) {
-            int sms = 0, per_sm = 0;
-            cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, block, 0);
-            cached_grid[0] = sms * (per_sm > 0 ? per_sm : 1);
-            cached_grid[1] = block;
+        if (smem > 48 * 1024) {
+            cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+            if (e != cudaSuccess)
+                return e;
         }
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, block, smem);
+        cached_grid[0] = sms * (per_sm > 0 ? per_sm : 1);
+        cached_grid[1] = block;
+    }
+    if (grid <= 0) {
         grid = cached_grid[0];
         const int64_t warps_needed = (a.ncells + 31) / 32;
         const int64_t blocks_needed = (warps_needed * 32 + block - 1) / block;
@@ -751,28 +893,49 @@ cudaError_t launch(const LaunchArgs& a, int block, int grid, cudaStream_t stream
         if (grid < 1)
             grid = 1;
     }
-    kern<<<grid, block, 0, stream>>>(a);
+    kern<<<grid, block, smem, stream>>>(a);
     return cudaGetLastError();
+}
+
+/* shared-memory staging is compiled for per-cell control when the per-lane
+   arrays of a 128-thread block fit in 200 KB */
+template <class Net, class LUT>
+constexpr bool shm_fits()
+{
+    return Staging<Net, LUT, true>::smem_bytes <= 200 * 1024;
 }
 
 }  // namespace OV_MODE_NS
 }  // namespace ov
 
-/* Defines the launcher of one network variant in the current mode. */
+/* Defines the launcher of one network variant in the current mode.
+   stage: 1 = thread-local staging, 2 = shared-memory staging. */
 #define OV_DEFINE_LAUNCHER(cid, FP32)                                                            \
     namespace ov {                                                                               \
     namespace OV_MODE_NS {                                                                       \
-    cudaError_t launch_##cid(const LaunchArgs& a, int G, int lu, int block, int grid,             \
+    cudaError_t launch_##cid(const LaunchArgs& a, int G, int lu, int stage, int block, int grid,  \
                              cudaStream_t s)                                                     \
     {                                                                                            \
+        using NET = ov_net_##cid;                                                                \
+        if (stage == 2) {                                                                        \
+            if constexpr (shm_fits<NET, double>())                                               \
+                if (G == 1 && lu == 0)                                                           \
+                    return launch<NET, 1, double, true>(a, block, grid, s);                      \
+            if constexpr (FP32 && shm_fits<NET, float>())                                        \
+                if (G == 1 && lu == 1)                                                           \
+                    return launch<NET, 1, float, true>(a, block, grid, s);                       \
+            return cudaErrorNotSupported;                                                        \
+        }                                                                                        \
         if (G == 1 && lu == 0)                                                                   \
-            return launch<ov_net_##cid, 1, double>(a, block, grid, s);                           \
+            return launch<NET, 1, double, false>(a, block, grid, s);                             \
         if (G == 32 && lu == 0)                                                                  \
-            return launch<ov_net_##cid, 32, double>(a, block, grid, s);                          \
-        if (FP32 && G == 1 && lu == 1)                                                           \
-            return launch<ov_net_##cid, 1, float>(a, block, grid, s);                            \
-        if (FP32 && G == 32 && lu == 1)                                                          \
-            return launch<ov_net_##cid, 32, float>(a, block, grid, s);                           \
+            return launch<NET, 32, double, false>(a, block, grid, s);                            \
+        if constexpr (FP32) {                                                                    \
+            if (G == 1 && lu == 1)                                                               \
+                return launch<NET, 1, float, false>(a, block, grid, s);                          \
+            if (G == 32 && lu == 1)                                                              \
+                return launch<NET, 32, float, false>(a, block, grid, s);                         \
+        }                                                                                        \
         return cudaErrorNotSupported;                                                            \
     }                                                                                            \
     }                                                                                            \

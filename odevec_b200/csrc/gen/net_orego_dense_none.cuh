@@ -5,18 +5,34 @@
 #include "net_orego_dense_none.h"
 
 struct ov_net_orego_dense_none {
-  static constexpr int NEQ = 3;
-  static constexpr int NNZ = 8;
+  static constexpr int NEQ = 3;   /* all species (state vector) */
+  static constexpr int ND = 3;    /* species in the solver state */
+  static constexpr int NNZ = 8;   /* packed LU entries of the dynamic block */
   static constexpr int NREA = 0;
   static constexpr int IDX_TGAS = -1;
   static constexpr bool DENSE = true;
   static constexpr const char* TAG = "OREGO_DENSE_NONE";
+  /* dynamic species (solver state index -> species) and frozen ones */
+  OV_HD static constexpr int dyn(int i) { return i == 0 ? 0 : (i == 1 ? 1 : (2)); }
+  static constexpr int NF = 0;
+  OV_HD static constexpr int frozen(int i) { return 0; }
   OV_HD static OV_INLINE void rhs(const double* y, const double* k, double* f) { ov_orego_dense_none_rhs(y, k, f); }
-  OV_HD static OV_INLINE void jac(const double* y, const double* k, double beta, double dt, double* a) { ov_orego_dense_none_jac(y, k, beta, dt, a); }
-  OV_HD static OV_INLINE void rates_T(const double*, double*) {}
-  OV_HD static OV_INLINE void rates_k(const double*, const double*, double*) {}
-  /* a = D P D^-1 rounded to T, D = diag(sc) in species order (isc = 1/sc) */
-  template <class T> OV_HD static OV_INLINE void store_scaled(const double* OV_RESTRICT P, T* OV_RESTRICT a, const double* OV_RESTRICT sc, const double* OV_RESTRICT isc) {
+  static OV_INLINE __device__ void rates_k(const double*, const double*, double*) {}
+  static OV_INLINE __device__ void rates_T(const double*, double*) {}
+  /* P = I - dt*beta*J on the dynamic block, packed CSC order */
+  template <class T, class A> OV_HD static OV_INLINE void jac(const double* OV_RESTRICT y, const double* OV_RESTRICT k, double beta, double dt, A a) {
+    (void)y; (void)k; (void)beta; (void)dt;
+    a[0] = (T)(-beta*dt*(-0.0012942725*y[0] - 77.27*y[1] + 77.27) + 1.0);
+    a[1] = (T)(0.0129416332341141*beta*dt*y[1]);
+    a[2] = (T)(-0.161*beta*dt);
+    a[3] = (T)(-beta*dt*(77.27 - 77.27*y[0]));
+    a[4] = (T)(-beta*dt*(-0.0129416332341141*y[0] - 0.0129416332341141) + 1.0);
+    a[5] = (T)(0.0);
+    a[6] = (T)(-0.0129416332341141*beta*dt);
+    a[7] = (T)(0.161*beta*dt + 1.0);
+  }
+  /* a = D P D^-1 rounded to T, D = diag(sc) over solver-state indices */
+  template <class T, class A> OV_HD static OV_INLINE void store_scaled(const double* OV_RESTRICT P, A a, const double* OV_RESTRICT sc, const double* OV_RESTRICT isc) {
     a[0] = (T)(P[0]*sc[0]*isc[0]);
     a[1] = (T)(P[1]*sc[1]*isc[0]);
     a[2] = (T)(P[2]*sc[2]*isc[0]);
@@ -26,8 +42,22 @@ struct ov_net_orego_dense_none {
     a[6] = (T)(P[6]*sc[1]*isc[2]);
     a[7] = (T)(P[7]*sc[2]*isc[2]);
   }
-  /* in-place numeric LU of the packed matrix a[NNZ] */
-  template <class T> OV_HD static OV_INLINE void lu_factor(T* OV_RESTRICT a) {
+  /* the same, each entry evaluated in FP64, scaled by powers of two and
+     rounded to T on the fly */
+  template <class T, class A> OV_HD static OV_INLINE void jac_scaled(const double* OV_RESTRICT y, const double* OV_RESTRICT k, double beta, double dt, A a, const double* OV_RESTRICT sc, const double* OV_RESTRICT isc) {
+    (void)y; (void)k; (void)beta; (void)dt;
+    a[0] = (T)((-beta*dt*(-0.0012942725*y[0] - 77.27*y[1] + 77.27) + 1.0)*sc[0]*isc[0]);
+    a[1] = (T)((0.0129416332341141*beta*dt*y[1])*sc[1]*isc[0]);
+    a[2] = (T)((-0.161*beta*dt)*sc[2]*isc[0]);
+    a[3] = (T)((-beta*dt*(77.27 - 77.27*y[0]))*sc[0]*isc[1]);
+    a[4] = (T)((-beta*dt*(-0.0129416332341141*y[0] - 0.0129416332341141) + 1.0)*sc[1]*isc[1]);
+    a[5] = (T)((0.0)*sc[2]*isc[1]);
+    a[6] = (T)((-0.0129416332341141*beta*dt)*sc[1]*isc[2]);
+    a[7] = (T)((0.161*beta*dt + 1.0)*sc[2]*isc[2]);
+  }
+  /* in-place numeric LU of the packed dynamic block a[0..NNZ-1]; A is a
+     pointer or an accessor whose operator[] yields T& */
+  template <class T, class A> OV_HD static OV_INLINE void lu_factor(A a) {
     a[1] = a[1] / a[0];
     a[2] = a[2] / a[0];
     a[4] = a[4] - a[1]*a[3];
@@ -35,10 +65,10 @@ struct ov_net_orego_dense_none {
     a[5] = a[5] / a[4];
     a[7] = a[7] - a[5]*a[6];
   }
-  /* x = P^-1 r with P = LU in a[]; r and x in species order.  sc/isc scale
-     species i by sc[i] on the way in and isc[i] on the way out (pass
+  /* x = P^-1 r on the dynamic block; r, x over solver-state indices.  sc/isc
+     scale entry i by sc[i] on the way in and isc[i] on the way out (pass
      nullptr for none); T is the precision of the solve. */
-  template <class T> OV_HD static OV_INLINE void lu_solve(const T* OV_RESTRICT a, const double* OV_RESTRICT r, double* OV_RESTRICT x, const double* OV_RESTRICT sc, const double* OV_RESTRICT isc) {
+  template <class T, class A> OV_HD static OV_INLINE void lu_solve(A a, const double* OV_RESTRICT r, double* OV_RESTRICT x, const double* OV_RESTRICT sc, const double* OV_RESTRICT isc) {
 #define OV_SC(i) (sc ? sc[i] : 1.0)
 #define OV_ISC(i) (isc ? isc[i] : 1.0)
     T d0 = (T)(r[0]*OV_SC(0));
@@ -55,5 +85,4 @@ struct ov_net_orego_dense_none {
 #undef OV_SC
 #undef OV_ISC
   }
-  static constexpr int perm[3] = {0, 1, 2};
 };

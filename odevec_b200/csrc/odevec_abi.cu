@@ -23,10 +23,10 @@
 #define OV_NET(cid, TAG)                                                                       \
     namespace ov {                                                                             \
     namespace exact {                                                                          \
-    cudaError_t launch_##cid(const LaunchArgs&, int, int, int, int, cudaStream_t);             \
+    cudaError_t launch_##cid(const LaunchArgs&, int, int, int, int, int, cudaStream_t);        \
     }                                                                                          \
     namespace fma {                                                                            \
-    cudaError_t launch_##cid(const LaunchArgs&, int, int, int, int, cudaStream_t);             \
+    cudaError_t launch_##cid(const LaunchArgs&, int, int, int, int, int, cudaStream_t);        \
     }                                                                                          \
     }
 #include "gen/registry.inc"
@@ -108,6 +108,20 @@ static int32_t resolve_opts(const NetEntry& e, const odevec_opts* in, odevec_opt
         return fail(OV_API_EINVAL, "unknown precision %d", o.precision);
     if (o.max_attempts <= 0)
         o.max_attempts = 1000000;
+    if (o.jac_batch <= 0)
+        o.jac_batch = 12;
+    if (o.ss_batch <= 0)
+        o.ss_batch = 12;
+    if (o.max_wait <= 0)
+        o.max_wait = o.max_wait < 0 ? 0 : 4;
+    if (o.jac_batch > 32 || o.ss_batch > 32)
+        return fail(OV_API_EINVAL, "jac_batch and ss_batch must be <= 32");
+    if (o.staging < 0 || o.staging > 2)
+        return fail(OV_API_EINVAL, "staging must be 0, 1 or 2");
+    if (o.block_threads < 0 || o.block_threads > 128 || o.block_threads % 32)
+        return fail(OV_API_EINVAL, "block_threads must be 32, 64, 96 or 128 (0: automatic)");
+    if (o.grid_blocks < 0)
+        return fail(OV_API_EINVAL, "grid_blocks < 0");
     *out = o;
     return OV_API_OK;
 }
@@ -222,13 +236,23 @@ int32_t odevec_solve(odevec_solver* s, int64_t ncells, double* y, double* t, dou
     a.dt_min = o.dt_min;
     a.check_neg = o.check_negatives ? 1 : 0;
     a.max_attempts = o.max_attempts;
+    a.jac_batch = o.jac_batch;
+    a.ss_batch = o.ss_batch;
+    a.max_wait = o.max_wait;
     cudaStream_t st = (cudaStream_t)stream;
     cudaError_t err = cudaMemsetAsync(s->d_queue, 0, sizeof(unsigned long long), st);
     if (err != cudaSuccess)
         return fail(OV_API_ECUDA, "odevec_solve: %s", cudaGetErrorString(err));
     const int lu = o.precision == OV_PREC_FP32_LU ? 1 : 0;
     ov::launch_fn fn = o.precision == OV_PREC_FP64 ? e.exact : e.fma;
-    err = fn(a, o.group_size, lu, 0, 0, st);
+    int stage = o.staging;
+    if (stage == 0) /* automatic: shared memory where compiled, else thread-local */
+        stage = (o.group_size == 1) ? 2 : 1;
+    err = fn(a, o.group_size, lu, stage, o.block_threads, o.grid_blocks, st);
+    if (err == cudaErrorNotSupported && o.staging == 0 && stage == 2) {
+        (void)cudaGetLastError();
+        err = fn(a, o.group_size, lu, 1, o.block_threads, o.grid_blocks, st);
+    }
     if (err == cudaErrorNotSupported)
         return fail(OV_API_EUNSUPPORTED, "variant %s: group %d precision %d not compiled", e.tag,
                     o.group_size, o.precision);

@@ -18,12 +18,21 @@ struct LaunchArgs {
     double rtol, atol, dt_min;
     int32_t check_neg;
     int32_t max_attempts;
+    /* per-cell control (G = 1): the Jacobian+LU and the step-size selection
+       run for all waiting lanes of a warp at once when at least this many
+       lanes wait, when no lane of the warp can progress otherwise, or when a
+       lane has waited max_wait trips */
+    int32_t jac_batch;
+    int32_t ss_batch;
+    int32_t max_wait;
 };
 
 /* one launcher per network variant and arithmetic mode; returns the CUDA
-   error of the launch.  G: 1 or 32; lu: 0 = FP64 LU, 1 = FP32 LU.
+   error of the launch.  G: 1 or 32; lu: 0 = FP64 LU, 1 = FP32 LU;
+   stage: 1 = thread-local arrays, 2 = shared-memory arrays (per-cell
+   control only; cudaErrorNotSupported where the arrays do not fit).
    block/grid 0: default (persistent grid from the occupancy). */
-typedef cudaError_t (*launch_fn)(const LaunchArgs& a, int G, int lu, int block, int grid,
-                                 cudaStream_t stream);
+typedef cudaError_t (*launch_fn)(const LaunchArgs& a, int G, int lu, int stage, int block,
+                                 int grid, cudaStream_t stream);
 
 }  // namespace ov

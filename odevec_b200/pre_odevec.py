@@ -292,6 +292,14 @@ def _cexpr(expr, pr: NetPrinter) -> str:
     return pr.doprint(expr)
 
 
+def _cswitch(vals: Sequence[int]) -> str:
+    """constexpr table lookup as a nested conditional (usable on host and device)."""
+    expr = str(vals[-1])
+    for i in range(len(vals) - 2, -1, -1):
+        expr = "i == %d ? %d : (%s)" % (i, vals[i], expr)
+    return expr
+
+
 def _cid(tag: str) -> str:
     return re.sub(r"[^A-Za-z0-9_]", "_", tag).lower()
 
@@ -393,18 +401,22 @@ def _lu_factor_lines(sysm: System) -> List[str]:
     return out
 
 
-def _lu_solve_lines(sysm: System) -> List[str]:
+def _lu_solve_lines(sysm: System, dpos: Optional[Dict[int, int]] = None) -> List[str]:
     """Straight-line solve P_order x = r with the permutation folded in:
-    reads r[perm[i]] and writes x[perm[i]] (species order)."""
+    reads r[perm[i]] and writes x[perm[i]] (species order), or, with dpos,
+    the solver-state index dpos[perm[i]] of the dynamic species only."""
     n = sysm.neq
     pos = sysm.pos()
-    p = sysm.perm
+    p = list(sysm.perm)
+    if dpos is None:
+        dpos = {s_: s_ for s_ in range(n)}
+    live = [i for i in range(n) if p[i] in dpos]
     out = []
-    for i in range(n):
-        out.append("T d%d = (T)(r[%d]*OV_SC(%d));" % (i, p[i], p[i]))
+    for i in live:
+        out.append("T d%d = (T)(r[%d]*OV_SC(%d));" % (i, dpos[p[i]], dpos[p[i]]))
     if sysm.packaging == "DENSE":
         # forward, unit lower (src/odevec.F90:814-826): d_k = r_k - sum_{j<k} L_kj d_j
-        for k in range(n):
+        for k in live:
             terms = [j for j in range(k) if (k, j) in pos]
             if terms:
                 s = "a[%d]*d%d" % (pos[(k, terms[0])], terms[0])
@@ -412,7 +424,7 @@ def _lu_solve_lines(sysm: System) -> List[str]:
                     s = "(%s + a[%d]*d%d)" % (s, pos[(k, j)], j)
                 out.append("d%d = d%d - %s;" % (k, k, s))
         # backward (src/odevec.F90:835-847): x_k = (d_k - sum_{j>k} U_kj x_j) / U_kk
-        for k in range(n - 1, -1, -1):
+        for k in reversed(live):
             terms = [j for j in range(k + 1, n) if (k, j) in pos]
             if terms:
                 s = "a[%d]*d%d" % (pos[(k, terms[0])], terms[0])
@@ -424,17 +436,52 @@ def _lu_solve_lines(sysm: System) -> List[str]:
     else:
         ri, ucs, lcs = sysm.row_index, sysm.u_col_start, sysm.l_col_start
         # forward (src/odevec.F90:864-876)
-        for k in range(n):
+        for k in live:
             out.append("d%d = d%d / a[%d];" % (k, k, lcs[k]))
             for kk in range(lcs[k] + 1, ucs[k + 1]):
                 out.append("d%d = d%d - d%d*a[%d];" % (ri[kk], ri[kk], k, kk))
         # backward (src/odevec.F90:878-889)
-        for k in range(n - 1, -1, -1):
+        for k in reversed(live):
             for kk in range(ucs[k], lcs[k]):
                 out.append("d%d = d%d - d%d*a[%d];" % (ri[kk], ri[kk], k, kk))
-    for i in range(n):
-        out.append("x[%d] = (double)d%d*OV_ISC(%d);" % (p[i], i, p[i]))
+    for i in live:
+        out.append("x[%d] = (double)d%d*OV_ISC(%d);" % (dpos[p[i]], i, dpos[p[i]]))
     return out
+
+
+def frozen_species(sysm: System) -> List[int]:
+    """Species whose right-hand side is identically zero and that no other
+    right-hand side depends on.  Their Newton corrections are exact zeros,
+    their state never changes and their rows and columns of P are those of
+    the identity, so the CUDA kernel keeps them out of the solver state."""
+    net = sysm.net
+    n = net.neq
+    J = net.rhs.jacobian(net.y)
+    out = []
+    for i in range(n):
+        if sp.sympify(net.rhs[i]) == 0 and all(sp.sympify(J[r, i]) == 0 for r in range(n)):
+            out.append(i)
+    return out
+
+
+def _reduced(sysm: System):
+    """Dynamic species, their positions, and the packed-index map of the LU
+    pattern restricted to dynamic rows and columns."""
+    n = sysm.neq
+    fz = set(frozen_species(sysm))
+    dyn = [s for s in range(n) if s not in fz]
+    dpos = {s: i for i, s in enumerate(dyn)}
+    kmap = {}
+    for j in range(n):
+        for kk in range(sysm.u_col_start[j], sysm.u_col_start[j + 1]):
+            i = sysm.row_index[kk]
+            if sysm.perm[i] in dpos and sysm.perm[j] in dpos:
+                kmap[kk] = len(kmap)
+    return dyn, dpos, kmap
+
+
+def _remap_a(line: str, kmap: Dict[int, int]) -> str:
+    return re.sub(r"a\[(\d+)\]", lambda m: "a[%d]" % kmap[int(m.group(1))], line)
 
 
 def emit_cuda_header(sysm: System) -> str:
@@ -450,52 +497,81 @@ def emit_cuda_header(sysm: System) -> str:
     L.append("#pragma once")
     L.append('#include "net_%s.h"' % cid)
     L.append("")
+    dyn, dpos, kmap = _reduced(sysm)
+    nd = len(dyn)
+    pos = sysm.pos()
+    ymap = {sym: "y[%d]" % i for i, sym in enumerate(net.y)}
+    pr = NetPrinter(ymap)
     L.append("struct ov_net_%s {" % cid)
-    L.append("  static constexpr int NEQ = %d;" % n)
-    L.append("  static constexpr int NNZ = %d;" % sysm.nnz)
+    L.append("  static constexpr int NEQ = %d;   /* all species (state vector) */" % n)
+    L.append("  static constexpr int ND = %d;    /* species in the solver state */" % nd)
+    L.append("  static constexpr int NNZ = %d;   /* packed LU entries of the dynamic block */" % len(kmap))
     L.append("  static constexpr int NREA = %d;" % (net.nrea if net.rates else 0))
     L.append("  static constexpr int IDX_TGAS = %d;" % (net.idx_tgas if net.idx_tgas is not None else -1))
     L.append("  static constexpr bool DENSE = %s;" % ("true" if sysm.packaging == "DENSE" else "false"))
     L.append('  static constexpr const char* TAG = "%s";' % sysm.tag)
+    L.append("  /* dynamic species (solver state index -> species) and frozen ones */")
+    L.append("  OV_HD static constexpr int dyn(int i) { return %s; }"
+             % _cswitch(dyn))
+    fz = [s_ for s_ in range(n) if s_ not in dpos]
+    L.append("  static constexpr int NF = %d;" % len(fz))
+    L.append("  OV_HD static constexpr int frozen(int i) { return %s; }" % _cswitch(fz if fz else [0]))
     L.append("  OV_HD static OV_INLINE void rhs(const double* y, const double* k, double* f) "
              "{ ov_%s_rhs(y, k, f); }" % cid)
-    L.append("  OV_HD static OV_INLINE void jac(const double* y, const double* k, double beta, "
-             "double dt, double* a) { ov_%s_jac(y, k, beta, dt, a); }" % cid)
     if net.rates:
-        L.append("  OV_HD static OV_INLINE void rates_T(const double* y, double* r) "
-                 "{ ov_rates_%s_T(y[%d], r); }" % (net.rates, net.idx_tgas))
-        L.append("  OV_HD static OV_INLINE void rates_k(const double* y, const double* r, double* k) "
+        L.append("  static OV_INLINE __device__ void rates_k(const double* y, const double* r, double* k) "
                  "{ ov_rates_%s_k(y, %d, r, k); }" % (net.rates, n))
+        L.append("  static __device__ __noinline__ void rates_T(const double* y, double* r) "
+                 "{ ov_rates_%s_T(y[%d], r); }" % (net.rates, net.idx_tgas))
     else:
-        L.append("  OV_HD static OV_INLINE void rates_T(const double*, double*) {}")
-        L.append("  OV_HD static OV_INLINE void rates_k(const double*, const double*, double*) {}")
-    L.append("  /* a = D P D^-1 rounded to T, D = diag(sc) in species order (isc = 1/sc) */")
-    L.append("  template <class T> OV_HD static OV_INLINE void store_scaled(const double* OV_RESTRICT P, "
-             "T* OV_RESTRICT a, const double* OV_RESTRICT sc, const double* OV_RESTRICT isc) {")
-    for j in range(n):
-        for kk in range(sysm.u_col_start[j], sysm.u_col_start[j + 1]):
-            i = sysm.row_index[kk]
-            L.append("    a[%d] = (T)(P[%d]*sc[%d]*isc[%d]);" % (kk, kk, sysm.perm[i], sysm.perm[j]))
+        L.append("  static OV_INLINE __device__ void rates_k(const double*, const double*, double*) {}")
+        L.append("  static OV_INLINE __device__ void rates_T(const double*, double*) {}")
+    L.append("  /* P = I - dt*beta*J on the dynamic block, packed CSC order */")
+    L.append("  template <class T, class A> OV_HD static OV_INLINE void jac(const double* OV_RESTRICT y, "
+             "const double* OV_RESTRICT k, double beta, double dt, A a) {")
+    L.append("    (void)y; (void)k; (void)beta; (void)dt;")
+    for (i, j), kk in sorted(pos.items(), key=lambda t: t[1]):
+        if kk in kmap:
+            L.append("    a[%d] = (T)(%s);" % (kmap[kk], _cexpr(sysm.P_order[i, j], pr)))
     L.append("  }")
-    L.append("  /* in-place numeric LU of the packed matrix a[NNZ] */")
-    L.append("  template <class T> OV_HD static OV_INLINE void lu_factor(T* OV_RESTRICT a) {")
-    for s in _lu_factor_lines(sysm):
-        L.append("    " + s)
+    L.append("  /* a = D P D^-1 rounded to T, D = diag(sc) over solver-state indices */")
+    L.append("  template <class T, class A> OV_HD static OV_INLINE void store_scaled(const double* OV_RESTRICT P, "
+             "A a, const double* OV_RESTRICT sc, const double* OV_RESTRICT isc) {")
+    for (i, j), kk in sorted(pos.items(), key=lambda t: t[1]):
+        if kk in kmap:
+            L.append("    a[%d] = (T)(P[%d]*sc[%d]*isc[%d]);" % (kmap[kk], kmap[kk], dpos[sysm.perm[i]],
+                                                              dpos[sysm.perm[j]]))
     L.append("  }")
-    L.append("  /* x = P^-1 r with P = LU in a[]; r and x in species order.  sc/isc scale")
-    L.append("     species i by sc[i] on the way in and isc[i] on the way out (pass")
+    L.append("  /* the same, each entry evaluated in FP64, scaled by powers of two and")
+    L.append("     rounded to T on the fly */")
+    L.append("  template <class T, class A> OV_HD static OV_INLINE void jac_scaled(const double* OV_RESTRICT y, "
+             "const double* OV_RESTRICT k, double beta, double dt, A a, "
+             "const double* OV_RESTRICT sc, const double* OV_RESTRICT isc) {")
+    L.append("    (void)y; (void)k; (void)beta; (void)dt;")
+    for (i, j), kk in sorted(pos.items(), key=lambda t: t[1]):
+        if kk in kmap:
+            L.append("    a[%d] = (T)((%s)*sc[%d]*isc[%d]);" % (kmap[kk], _cexpr(sysm.P_order[i, j], pr),
+                                                             dpos[sysm.perm[i]], dpos[sysm.perm[j]]))
+    L.append("  }")
+    L.append("  /* in-place numeric LU of the packed dynamic block a[0..NNZ-1]; A is a")
+    L.append("     pointer or an accessor whose operator[] yields T& */")
+    L.append("  template <class T, class A> OV_HD static OV_INLINE void lu_factor(A a) {")
+    for ln in _lu_factor_lines(sysm):
+        L.append("    " + _remap_a(ln, kmap))
+    L.append("  }")
+    L.append("  /* x = P^-1 r on the dynamic block; r, x over solver-state indices.  sc/isc")
+    L.append("     scale entry i by sc[i] on the way in and isc[i] on the way out (pass")
     L.append("     nullptr for none); T is the precision of the solve. */")
-    L.append("  template <class T> OV_HD static OV_INLINE void lu_solve(const T* OV_RESTRICT a, "
+    L.append("  template <class T, class A> OV_HD static OV_INLINE void lu_solve(A a, "
              "const double* OV_RESTRICT r, double* OV_RESTRICT x, const double* OV_RESTRICT sc, "
              "const double* OV_RESTRICT isc) {")
     L.append("#define OV_SC(i) (sc ? sc[i] : 1.0)")
     L.append("#define OV_ISC(i) (isc ? isc[i] : 1.0)")
-    for s in _lu_solve_lines(sysm):
-        L.append("    " + s)
+    for ln in _lu_solve_lines(sysm, dpos=dpos):
+        L.append("    " + _remap_a(ln, kmap))
     L.append("#undef OV_SC")
     L.append("#undef OV_ISC")
     L.append("  }")
-    L.append("  static constexpr int perm[%d] = {%s};" % (n, ", ".join(map(str, sysm.perm))))
     L.append("};")
     return "\n".join(L) + "\n"
 

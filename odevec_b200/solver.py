@@ -59,7 +59,9 @@ class OdevecError(RuntimeError):
 class _Opts(ctypes.Structure):
     _fields_ = [("rtol", ctypes.c_double), ("atol", ctypes.c_double), ("dt_min", ctypes.c_double),
                 ("check_negatives", ctypes.c_int32), ("group_size", ctypes.c_int32),
-                ("precision", ctypes.c_int32), ("max_attempts", ctypes.c_int32)]
+                ("precision", ctypes.c_int32), ("max_attempts", ctypes.c_int32),
+                ("jac_batch", ctypes.c_int32), ("ss_batch", ctypes.c_int32), ("max_wait", ctypes.c_int32),
+                ("staging", ctypes.c_int32), ("block_threads", ctypes.c_int32), ("grid_blocks", ctypes.c_int32)]
 
 
 _lib = None
@@ -117,7 +119,9 @@ class Odevec:
     def __init__(self, network: str, max_cells: int = 0, RelativeTolerance: float = 1e-4,
                  AbsoluteTolerance: float = 1e-20, MinimalTimestep: Optional[float] = None,
                  CheckNegatives: bool = False, nvector: Optional[int] = None,
-                 precision: str = "fp64", max_attempts: int = 0, raise_on_failure: bool = True):
+                 precision: str = "fp64", max_attempts: int = 0, raise_on_failure: bool = True,
+                 jac_batch: int = 0, ss_batch: int = 0, max_wait: int = 0, staging: int = 0,
+                 block_threads: int = 0, grid_blocks: int = 0):
         info = network_info(network)
         self.network = network
         self.neq = info["neq"]
@@ -133,6 +137,12 @@ class Odevec:
         self.precision = precision
         self.max_attempts = max_attempts
         self.raise_on_failure = raise_on_failure
+        self.jac_batch = jac_batch
+        self.ss_batch = ss_batch
+        self.max_wait = max_wait
+        self.staging = staging
+        self.block_threads = block_threads
+        self.grid_blocks = grid_blocks
         self.status = None
         self.stats = None
         self._h = None
@@ -148,6 +158,12 @@ class Odevec:
             raise ValueError("precision must be one of %s" % list(PREC))
         o.precision = PREC[self.precision]
         o.max_attempts = int(self.max_attempts)
+        o.jac_batch = int(self.jac_batch)
+        o.ss_batch = int(self.ss_batch)
+        o.max_wait = int(self.max_wait)
+        o.staging = int(self.staging)
+        o.block_threads = int(self.block_threads)
+        o.grid_blocks = int(self.grid_blocks)
         return o
 
     @property
