@@ -92,6 +92,12 @@ typedef struct odevec_opts {
     int32_t staging;
     int32_t block_threads;
     int32_t grid_blocks;
+    /* 0: reproduce the reference exactly.  1: after three consecutive
+       error-test failures, undo the prediction (ResetSystem) before the
+       restart at order 1; the reference restarts from the predicted state
+       with the time reset (src/odevec.F90:404-421), which costs accuracy at
+       tight tolerances. */
+    int32_t fix_restart;
 } odevec_opts;
 
 typedef struct odevec_solver odevec_solver;

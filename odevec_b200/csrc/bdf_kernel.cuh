@@ -770,6 +770,8 @@ __global__ void __launch_bounds__(128, SHM ? 1 : 2) bdf_kernel(const LaunchArgs 
                     c.ltef++;
                     c.t = c.told;
                     if (c.fet >= 3) {
+                        if (A.fix_restart)
+                            c.reset();
                         c.q = 1;
                         if (c.msk) {
 #pragma unroll

@@ -239,6 +239,7 @@ int32_t odevec_solve(odevec_solver* s, int64_t ncells, double* y, double* t, dou
     a.jac_batch = o.jac_batch;
     a.ss_batch = o.ss_batch;
     a.max_wait = o.max_wait;
+    a.fix_restart = o.fix_restart ? 1 : 0;
     cudaStream_t st = (cudaStream_t)stream;
     cudaError_t err = cudaMemsetAsync(s->d_queue, 0, sizeof(unsigned long long), st);
     if (err != cudaSuccess)
@@ -324,3 +325,4 @@ int32_t odevec_close(odevec_solver* s)
 }
 
 }  // extern "C"
+

@@ -25,6 +25,7 @@ struct LaunchArgs {
     int32_t jac_batch;
     int32_t ss_batch;
     int32_t max_wait;
+    int32_t fix_restart; /* undo the prediction before an order-1 restart */
 };
 
 /* one launcher per network variant and arithmetic mode; returns the CUDA

@@ -61,7 +61,8 @@ class _Opts(ctypes.Structure):
                 ("check_negatives", ctypes.c_int32), ("group_size", ctypes.c_int32),
                 ("precision", ctypes.c_int32), ("max_attempts", ctypes.c_int32),
                 ("jac_batch", ctypes.c_int32), ("ss_batch", ctypes.c_int32), ("max_wait", ctypes.c_int32),
-                ("staging", ctypes.c_int32), ("block_threads", ctypes.c_int32), ("grid_blocks", ctypes.c_int32)]
+                ("staging", ctypes.c_int32), ("block_threads", ctypes.c_int32), ("grid_blocks", ctypes.c_int32),
+                ("fix_restart", ctypes.c_int32)]
 
 
 _lib = None
@@ -121,7 +122,7 @@ class Odevec:
                  CheckNegatives: bool = False, nvector: Optional[int] = None,
                  precision: str = "fp64", max_attempts: int = 0, raise_on_failure: bool = True,
                  jac_batch: int = 0, ss_batch: int = 0, max_wait: int = 0, staging: int = 0,
-                 block_threads: int = 0, grid_blocks: int = 0):
+                 block_threads: int = 0, grid_blocks: int = 0, fix_restart: bool = False):
         info = network_info(network)
         self.network = network
         self.neq = info["neq"]
@@ -143,6 +144,7 @@ class Odevec:
         self.staging = staging
         self.block_threads = block_threads
         self.grid_blocks = grid_blocks
+        self.fix_restart = fix_restart
         self.status = None
         self.stats = None
         self._h = None
@@ -164,6 +166,7 @@ class Odevec:
         o.staging = int(self.staging)
         o.block_threads = int(self.block_threads)
         o.grid_blocks = int(self.grid_blocks)
+        o.fix_restart = 1 if self.fix_restart else 0
         return o
 
     @property

@@ -95,7 +95,7 @@ typedef struct {
     const net_desc* net;
     int G, neq;
     double rtol, atol, dt_min;
-    int check_neg;
+    int check_neg, fix_restart;
     int64_t max_attempts;
     /* control, src/odevec.F90:39-56 */
     int order, SuccessesWithoutUpdate, LastJacobianUpdate, FailedErrorTests, FailedCorrections;
@@ -581,6 +581,8 @@ static void solve_linear_system(ode_t* o, double* t, double* dt, double* y)
             o->lte_fails++;
             if (o->FailedErrorTests >= 3) {
                 *t = told;
+                if (o->fix_restart) /* optional correction, not in the reference */
+                    reset_system(o);
                 o->order = 1;
                 masked_copy(o, y, NS(o, 0));
                 get_rhs(o, y, o->rhs);
@@ -709,7 +711,7 @@ static void solve_group(ode_t* o, double* time, double* dt, double t_stop, doubl
 
 /* --------------------------------------------------------------- C ABI */
 int ov_oracle_solve(const char* tag, int64_t ncells, int G, double rtol, double atol,
-                    double dt_min, int check_negatives, int64_t max_attempts, double* y, double* t,
+                    double dt_min, int check_negatives, int fix_restart, int64_t max_attempts, double* y, double* t,
                     double* dt, const double* t_stop, const uint8_t* mask, int32_t* status,
                     int32_t* stats, int nthreads)
 {
@@ -735,6 +737,7 @@ int ov_oracle_solve(const char* tag, int64_t ncells, int G, double rtol, double 
         o.atol = atol;
         o.dt_min = dt_min;
         o.check_neg = check_negatives;
+        o.fix_restart = fix_restart;
         o.max_attempts = max_attempts;
         init_coeff(&o);
         o.DoPermute = 0;

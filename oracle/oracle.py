@@ -21,8 +21,8 @@ def lib():
         L = ctypes.CDLL(path)
         d, i64, i32 = ctypes.c_double, ctypes.c_int64, ctypes.c_int
         P = ctypes.c_void_p
-        L.ov_oracle_solve.argtypes = [ctypes.c_char_p, i64, i32, d, d, d, i32, i64, P, P, P, P, P,
-                                      P, P, i32]
+        L.ov_oracle_solve.argtypes = [ctypes.c_char_p, i64, i32, d, d, d, i32, i32, i64, P, P, P, P,
+                                      P, P, P, i32]
         L.ov_oracle_solve.restype = i32
         L.ov_oracle_eval.argtypes = [ctypes.c_char_p, P, P, d, d, P, P]
         L.ov_oracle_rates.argtypes = [d, P]
@@ -65,7 +65,7 @@ def tags():
 
 
 def solve(tag, y, t, dt, t_stop, rtol, atol, dt_min, group=1, check_negatives=False,
-          mask=None, max_attempts=1000000, nthreads=0):
+          mask=None, max_attempts=1000000, nthreads=0, fix_restart=False):
     """SolveODE on all cells.  y: (neq, ncells) float64, modified copy returned
     with t, dt, status, stats."""
     y = np.ascontiguousarray(y, dtype=np.float64).copy()
@@ -77,7 +77,8 @@ def solve(tag, y, t, dt, t_stop, rtol, atol, dt_min, group=1, check_negatives=Fa
     status = np.zeros(ncells, np.int32)
     stats = np.zeros((ncells, OV_NSTATS), np.int32)
     rc = lib().ov_oracle_solve(tag.encode(), ncells, group, rtol, atol, dt_min,
-                               int(bool(check_negatives)), max_attempts, _p(y), _p(t), _p(dt),
+                               int(bool(check_negatives)), int(bool(fix_restart)), max_attempts,
+                               _p(y), _p(t), _p(dt),
                                _p(t_stop), _p(m), _p(status), _p(stats), nthreads)
     if rc != 0:
         raise ValueError("oracle solve failed rc=%d" % rc)

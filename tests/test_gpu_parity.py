@@ -156,12 +156,37 @@ def test_status_max_attempts(gpu_lib, oracle):
 
 
 def test_status_dt_min(gpu_lib, oracle):
-    # a minimal step far above the natural one: Newton failures shrink dt below it
-    wl = W.rober(ncells=64, network="ROBER_CSC_NONE")
-    wl.group = 1
-    g = run_gpu(gpu_lib, wl, "fp64", dt_min=1e3)
-    o = run_oracle(oracle, wl, dt_min=1e3)
+    # OREGO has occasional Newton failures, each dividing dt by 4; with a
+    # minimal step of 0.1 most cells end with OV_ERR_DTMIN_CONV
+    wl = W.orego(ncells=256)
+    g = run_gpu(gpu_lib, wl, "fp64", dt_min=0.1)
+    o = run_oracle(oracle, wl, dt_min=0.1)
+    assert np.sum(o[3] == 3) > 50
     assert_bitwise(g, o, "dt_min")
+
+
+@pytest.mark.parametrize("network", ["ROBER_CSC_NONE", "PRIMORDIAL_CSC_FF"])
+def test_fix_restart_matches_oracle(gpu_lib, oracle, network):
+    # the optional correction of the order-1 restart, at a tight tolerance
+    # where the restart happens often
+    wl = W.rober(ncells=128, network=network) if network.startswith("ROBER") else \
+        W.primordial(ncells=256, network=network)
+    wl.group = 1
+    wl.rtol = 1e-10
+    wl.atol = 1e-16 if network.startswith("ROBER") else 1e-24
+    import torch
+    ode = gpu_lib.Odevec(wl.network, RelativeTolerance=wl.rtol, AbsoluteTolerance=wl.atol,
+                         MinimalTimestep=wl.dt_min, nvector=1, precision="fp64", fix_restart=True,
+                         raise_on_failure=False)
+    gpu_lib.InitOdevec(ode)
+    y = torch.tensor(wl.y, device="cuda")
+    t, dt = gpu_lib.SolveODE(ode, torch.tensor(wl.t0, device="cuda"), torch.tensor(wl.dt0, device="cuda"),
+                             torch.tensor(wl.t_stop, device="cuda"), y)
+    g = (y.cpu().numpy(), t.cpu().numpy(), dt.cpu().numpy(), ode.status.cpu().numpy(), ode.stats.cpu().numpy())
+    gpu_lib.CloseOdevec(ode)
+    o = oracle.solve(wl.network, wl.y, wl.t0, wl.dt0, wl.t_stop, wl.rtol, wl.atol, wl.dt_min, group=1,
+                     fix_restart=True)
+    assert_bitwise(g, o, "fix_restart")
 
 
 def test_group_mismatch(gpu_lib, oracle):

@@ -1,0 +1,54 @@
+"""The shared elementary functions (odevec_b200/csrc/ov_common.h) against the
+C library, through the oracle build (same source as the device code)."""
+import numpy as np
+import pytest
+
+
+def ulps(a, b):
+    a = np.asarray(a, np.float64)
+    b = np.asarray(b, np.float64)
+    return np.abs(a - b) / np.spacing(np.abs(b))
+
+
+@pytest.fixture(scope="module")
+def lib(oracle):
+    return oracle.lib()
+
+
+def test_exp(lib):
+    rng = np.random.default_rng(0)
+    xs = np.concatenate([rng.uniform(-745, 709.7, 20000), rng.uniform(-1, 1, 20000),
+                         [0.0, -0.0, 1.0, -1.0, 700.0, -700.0, -740.0]])
+    got = np.array([lib.ov_oracle_exp(float(x)) for x in xs])
+    ref = np.exp(xs)
+    normal = ref > 2.3e-308
+    assert np.max(ulps(got[normal], ref[normal])) <= 2.0
+    sub = (ref > 0) & ~normal
+    assert np.all(np.abs(got[sub] - ref[sub]) <= 2 * 4.9e-324 * 4)
+    assert lib.ov_oracle_exp(1000.0) == np.inf and lib.ov_oracle_exp(-1000.0) == 0.0
+    assert np.isnan(lib.ov_oracle_exp(float("nan")))
+
+
+def test_log(lib):
+    rng = np.random.default_rng(1)
+    xs = np.concatenate([10.0 ** rng.uniform(-300, 300, 20000), rng.uniform(0.5, 2.0, 20000),
+                         [1.0, 2.0, 0.5, 1e-310, 5e-324, 1.7e308]])
+    got = np.array([lib.ov_oracle_log(float(x)) for x in xs])
+    ref = np.log(xs)
+    nz = ref != 0
+    assert np.max(ulps(got[nz], ref[nz])) <= 2.0
+    assert lib.ov_oracle_log(1.0) == 0.0
+    assert lib.ov_oracle_log(0.0) == -np.inf and np.isnan(lib.ov_oracle_log(-1.0))
+
+
+def test_pow(lib):
+    rng = np.random.default_rng(2)
+    x = 10.0 ** rng.uniform(-10, 10, 20000)
+    y = rng.uniform(-3, 3, 20000)
+    got = np.array([lib.ov_oracle_pow(float(a), float(b)) for a, b in zip(x, y)])
+    ref = np.power(x, y)
+    # exp(y log x): relative error grows with |y log x| (<= 70 here)
+    rel = np.abs(got - ref) / ref
+    assert np.max(rel / (1.0 + np.abs(y * np.log(x)))) < 4e-16
+    assert lib.ov_oracle_pow(0.0, 0.5) == 0.0 and lib.ov_oracle_pow(7.0, 0.0) == 1.0
+    assert abs(lib.ov_oracle_pow(-2.0, 3.0) + 8.0) < 1e-14 and np.isnan(lib.ov_oracle_pow(-2.0, 0.5))
