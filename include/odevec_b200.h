@@ -137,6 +137,28 @@ int32_t odevec_close(odevec_solver* s);
 /* message of the last failed call on this thread */
 const char* odevec_last_error(void);
 
+/* SolveODE on device arrays without allocating anything.  No counterpart in
+   the reference.  For callers that cannot call cudaMalloc -- a host code
+   that passes its own device arrays from a region where device allocation
+   is forbidden or would break its memory-pool budget.  Same arguments as
+   odevec_solve, with the network and options given directly instead of a
+   solver created by odevec_init.  The solve kernel's scratch (the counter
+   that hands out cells) lives in a static device array of
+   OV_NOALLOC_SCRATCH_BYTES, which every GPU that loads the library holds
+   until the process exits; at most OV_NOALLOC_MAX_CELLS cells per call
+   (larger calls fail with OV_API_ETOOBIG).  The first call on a device looks
+   up that array's device address (cudaGetSymbolAddress) and caches it, so
+   make the first call on each device before any stream capture.  Every
+   call resets the counter to zero on `stream` before the launch; all calls
+   share the one counter, so calls that overlap on the GPU (different
+   streams, or different host threads) race and must be serialised by the
+   caller. */
+#define OV_NOALLOC_SCRATCH_BYTES 256
+#define OV_NOALLOC_MAX_CELLS (1LL << 40)
+int32_t odevec_solve_noalloc(const char* network, const odevec_opts* opts, int64_t ncells,
+                             double* y, double* t, double* dt, const double* t_stop,
+                             const uint8_t* mask, int32_t* status, int32_t* stats, void* stream);
+
 /* Measurement utility, no counterpart in the reference: times `blocks` x
    `threads` threads each running 8 independent FMA chains of `iters` steps
    (FP64 if fp64 != 0, else FP32) on `stream`; scratch: >= blocks*8 bytes of

@@ -13,6 +13,7 @@
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 #include <new>
 
 #include "../../include/odevec_b200.h"
@@ -326,3 +327,122 @@ int32_t odevec_close(odevec_solver* s)
 
 }  // extern "C"
 
+/* ------------------------------------------------------------------------
+ * Solve without any device allocation.
+ *
+ * odevec_init allocates a small device work counter (and, for host arrays,
+ * staging buffers) with cudaMalloc.  Some callers cannot do that: a host
+ * code that hands the solver its own device arrays from inside a region
+ * where device allocation is forbidden or would break its memory-pool
+ * discipline (an operator-split hydro step running under a fixed memory
+ * budget, or an application that owns every byte of the GPU through its own
+ * allocator).  odevec_solve_noalloc serves them: it launches the same solve
+ * kernel on the caller's device arrays, and takes the kernel's only scratch
+ * -- the 64-bit counter from which the persistent grid hands out cells --
+ * from a file-scope device array that the library image carries on every
+ * GPU that loads it, until the process exits.
+ * ------------------------------------------------------------------------ */
+namespace {
+
+/* OV_NOALLOC_SCRATCH_BYTES of static device memory: word 0 is the cell
+   counter, the rest keeps the array on its own 256-byte line. */
+static __device__ __align__(256) unsigned long long ov_noalloc_scratch[OV_NOALLOC_SCRATCH_BYTES / 8];
+
+constexpr int kMaxDevices = 64;
+std::mutex g_noalloc_mutex;
+unsigned long long* g_noalloc_ptr[kMaxDevices] = {};
+
+/* Device address of the static scratch on the current device.  In host code
+   the name ov_noalloc_scratch is only a handle, so the address is looked up
+   once per device with that device current, and cached. */
+int32_t noalloc_scratch(int dev, unsigned long long** out)
+{
+    if (dev < 0 || dev >= kMaxDevices)
+        return fail(OV_API_EINVAL, "odevec_solve_noalloc: device ordinal %d out of range", dev);
+    std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+    if (!g_noalloc_ptr[dev]) {
+        void* p = nullptr;
+        cudaError_t e = cudaGetSymbolAddress(&p, ov_noalloc_scratch);
+        if (e != cudaSuccess || !p)
+            return fail(OV_API_ECUDA, "odevec_solve_noalloc: cudaGetSymbolAddress: %s",
+                        cudaGetErrorString(e));
+        g_noalloc_ptr[dev] = static_cast<unsigned long long*>(p);
+    }
+    *out = g_noalloc_ptr[dev];
+    return OV_API_OK;
+}
+
+}  // namespace
+
+extern "C" int32_t odevec_solve_noalloc(const char* network, const odevec_opts* opts, int64_t ncells,
+                                        double* y, double* t, double* dt, const double* t_stop,
+                                        const uint8_t* mask, int32_t* status, int32_t* stats,
+                                        void* stream)
+{
+    const int ni = find_net(network);
+    if (ni < 0)
+        return fail(OV_API_ENONET, "unknown network variant '%s'", network ? network : "(null)");
+    if (ncells < 0)
+        return fail(OV_API_EINVAL, "ncells < 0");
+    if (ncells > OV_NOALLOC_MAX_CELLS)
+        return fail(OV_API_ETOOBIG, "odevec_solve_noalloc: %lld cells exceed the maximum of %lld",
+                    (long long)ncells, (long long)OV_NOALLOC_MAX_CELLS);
+    if (ncells == 0)
+        return OV_API_OK;
+    if (!y || !t || !dt || !t_stop)
+        return fail(OV_API_EINVAL, "y, t, dt and t_stop are required");
+    odevec_opts o;
+    int32_t rc = resolve_opts(g_nets[ni], opts, &o);
+    if (rc)
+        return rc;
+    if (o.group_size == 32 && ncells % 32)
+        return fail(OV_API_EINVAL, "group_size 32 needs ncells divisible by 32 (got %lld)",
+                    (long long)ncells);
+    int dev = 0;
+    cudaError_t err = cudaGetDevice(&dev);
+    if (err != cudaSuccess)
+        return fail(OV_API_ECUDA, "odevec_solve_noalloc: %s", cudaGetErrorString(err));
+    unsigned long long* counter = nullptr;
+    rc = noalloc_scratch(dev, &counter);
+    if (rc)
+        return rc;
+    cudaStream_t st = (cudaStream_t)stream;
+    /* the scratch keeps the previous call's count: the counter must start at 0 */
+    err = cudaMemsetAsync(counter, 0, sizeof(unsigned long long), st);
+    if (err != cudaSuccess)
+        return fail(OV_API_ECUDA, "odevec_solve_noalloc: %s", cudaGetErrorString(err));
+    ov::LaunchArgs a;
+    a.ncells = ncells;
+    a.y = y;
+    a.t = t;
+    a.dt = dt;
+    a.t_stop = t_stop;
+    a.mask = mask;
+    a.status = status;
+    a.stats = stats;
+    a.queue = counter;
+    a.rtol = o.rtol;
+    a.atol = o.atol;
+    a.dt_min = o.dt_min;
+    a.check_neg = o.check_negatives ? 1 : 0;
+    a.max_attempts = o.max_attempts;
+    a.jac_batch = o.jac_batch;
+    a.ss_batch = o.ss_batch;
+    a.max_wait = o.max_wait;
+    a.fix_restart = o.fix_restart ? 1 : 0;
+    const NetEntry& e = g_nets[ni];
+    const int lu = o.precision == OV_PREC_FP32_LU ? 1 : 0;
+    ov::launch_fn fn = o.precision == OV_PREC_FP64 ? e.exact : e.fma;
+    int stage = o.staging ? o.staging : (o.group_size == 1 ? 2 : 1);
+    err = fn(a, o.group_size, lu, stage, o.block_threads, o.grid_blocks, st);
+    if (err == cudaErrorNotSupported && o.staging == 0 && stage == 2) {
+        (void)cudaGetLastError();
+        err = fn(a, o.group_size, lu, 1, o.block_threads, o.grid_blocks, st);
+    }
+    if (err == cudaErrorNotSupported)
+        return fail(OV_API_EUNSUPPORTED, "variant %s: group %d precision %d not compiled", e.tag,
+                    o.group_size, o.precision);
+    if (err != cudaSuccess)
+        return fail(OV_API_ECUDA, "odevec_solve_noalloc launch: %s", cudaGetErrorString(err));
+    return OV_API_OK;
+}

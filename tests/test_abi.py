@@ -27,7 +27,7 @@ def declared():
 
 def test_exports_every_declared_function(L):
     names = declared()
-    assert "odevec_solve" in names and len(names) >= 10
+    assert "odevec_solve" in names and "odevec_solve_noalloc" in names and len(names) >= 11
     for n in names:
         assert hasattr(L, n), n
 
@@ -71,6 +71,21 @@ def test_solve_argument_errors(L):
     assert L.odevec_solve(None, 10, None, None, None, None, None, None, None, None) == -1
     assert L.odevec_solve_host(None, 10, None, None, None, None, None, None, None) == -1
     assert L.odevec_close(None) == 0
+
+
+def test_noalloc_argument_errors(L):
+    f = L.odevec_solve_noalloc
+    from odevec_b200 import solver
+    f.argtypes = [ctypes.c_char_p, ctypes.POINTER(solver._Opts), ctypes.c_int64] + [ctypes.c_void_p] * 8
+    P = ctypes.c_void_p(16)
+    o = _opts()
+    assert f(b"NOPE", ctypes.byref(o), 10, P, P, P, P, None, None, None, None) == -2
+    assert f(b"ROBER_DENSE_NONE", ctypes.byref(o), -1, P, P, P, P, None, None, None, None) == -1
+    assert f(b"ROBER_DENSE_NONE", ctypes.byref(o), (1 << 40) + 1, P, P, P, P, None, None, None, None) == -6
+    assert f(b"ROBER_DENSE_NONE", ctypes.byref(o), 0, P, P, P, P, None, None, None, None) == 0
+    assert f(b"ROBER_DENSE_NONE", ctypes.byref(o), 64, None, P, P, P, None, None, None, None) == -1
+    bad = _opts(rtol=-1.0)
+    assert f(b"ROBER_DENSE_NONE", ctypes.byref(bad), 64, P, P, P, P, None, None, None, None) == -1
 
 
 def test_probe_argument_errors(L):
