@@ -68,6 +68,7 @@ CASES = [
     ("PRIMORDIAL", dict(ncells=256), "PRIMORDIAL_CSC_CMK", 1),
     ("PRIMORDIAL", dict(ncells=256), "PRIMORDIAL_DENSE_NONE", 1),
     ("PRIMORDIAL", dict(ncells=256), "PRIMORDIAL_DENSE_NONE", 32),
+    ("SYN64", dict(ncells=128), "SYN64_CSC_CMK", 1),
 ]
 
 
@@ -76,6 +77,7 @@ def test_fp64_bit_exact_vs_oracle(gpu_lib, oracle, name, kw, network, group):
     wl = W.BUILDERS[name](network=network, **kw)
     if group == 32 and name == "PRIMORDIAL":
         wl.t_stop[:] = 1e10  # lockstep groups need a common t_stop
+    wl.group = group
     g = run_gpu(gpu_lib, wl, "fp64", group=group)
     o = run_oracle(oracle, wl, group=group)
     assert np.all(o[3] == 0), "oracle failures: %s" % np.unique(o[3])
@@ -212,3 +214,12 @@ def test_primordial_conservation_large_sample(gpu_lib, precision, tol):
     for k in range(3):
         assert np.max(np.abs(b[k] - a[k]) / a[k]) < tol
     assert np.max(np.abs(b[3]) / a[0]) < tol
+
+
+def test_syn64_mass_conservation(gpu_lib):
+    from odevec_b200 import syn64
+    wl = W.syn64(ncells=1024)
+    g = run_gpu(gpu_lib, wl, "fp32_lu")
+    assert np.all(g[3] == 0)
+    m = syn64.masses()
+    assert np.max(np.abs(m @ g[0] - m @ wl.y) / (m @ wl.y)) < 1e-4

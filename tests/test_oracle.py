@@ -144,3 +144,13 @@ def test_status_codes(oracle):
     ts[3] = 2e5
     y, t, dt, st, _ = oracle.solve("ROBER_DENSE_NONE", wl.y, 0.0, 1e-10, ts, 1e-4, 1e-10, 1e-20, group=32)
     assert np.all(st == 6) and np.array_equal(y, wl.y) and np.all(t == 0.0)
+
+
+def test_syn64_mass_conservation(oracle):
+    from odevec_b200 import syn64
+    wl = W.syn64(ncells=32)
+    y, t, dt, st, stats = oracle.solve(wl.network, wl.y, wl.t0, wl.dt0, wl.t_stop, wl.rtol, wl.atol,
+                                       wl.dt_min)
+    assert np.all(st == 0) and np.all(t == 1e10)
+    m = syn64.masses()
+    assert np.max(np.abs(m @ y - m @ wl.y) / (m @ wl.y)) < 1e-12
