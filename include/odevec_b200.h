@@ -80,15 +80,18 @@ typedef struct odevec_opts {
        the Jacobian+LU and the step-size selection run for the waiting cells
        of a warp together once jac_batch / ss_batch of its 32 cells wait, no
        other cell can progress, or a cell has waited max_wait iterations.
-       0: defaults (12, 12, 4); 1, 1, 0 runs each cell's block at once. */
+       0: defaults (24, 24, 8); 1, 1, -1 runs each cell's block at once. */
     int32_t jac_batch;
     int32_t ss_batch;
     int32_t max_wait;
-    /* launch shape, no effect on results: staging 0 = automatic, 1 = per-cell
-       arrays in registers / local memory, 2 = in shared memory (per-cell
-       control, one 128-thread block per SM, where they fit); block_threads
-       (a multiple of 32 up to 128) and grid_blocks 0 = automatic (persistent
-       grid filling every SM) */
+    /* launch shape, no effect on results.  staging: 0 = automatic (3 for
+       per-cell control, 1 for lockstep); 1 = per-cell arrays in registers /
+       local memory, 2 blocks of 128 threads per SM; 2 = history and LU in
+       shared memory, 1 block of 128 (where they fit); 3, 4 = as 1 with 3 or 4
+       blocks per SM (fewer registers, more warps); 5 = as 2 with 192-thread
+       blocks (FP32 LU).  block_threads (a multiple of 32 up to the block of
+       the staging) and grid_blocks: 0 = automatic (persistent grid filling
+       every SM) */
     int32_t staging;
     int32_t block_threads;
     int32_t grid_blocks;
@@ -98,6 +101,12 @@ typedef struct odevec_opts {
        with the time reset (src/odevec.F90:404-421), which costs accuracy at
        tight tolerances. */
     int32_t fix_restart;
+    /* OV_PREC_FP32_LU only: cells whose solve fails with FP32 factors (a
+       badly conditioned iteration matrix) are solved again from their inputs
+       with FP64 factors, in a second launch on the same stream that exits at
+       once when no cell failed.  1 disables this escalation.  Their
+       statistics are those of the FP32 attempt. */
+    int32_t no_escalation;
 } odevec_opts;
 
 typedef struct odevec_solver odevec_solver;
@@ -131,6 +140,21 @@ int32_t odevec_solve_host(odevec_solver* s, int64_t ncells, double* y, double* t
                           const double* t_stop, const uint8_t* mask, int32_t* status,
                           int32_t* stats);
 
+/* Continuation across calls (no counterpart in the reference, which
+   restarts from y at order 1 on every SolveODE): the integrator state of
+   every cell -- Nordsieck history, order, step size, error weights and
+   control counters -- stays in a device workspace owned by the caller.
+   odevec_workspace_doubles gives its size in doubles per cell.  A call with
+   resume = 0 starts fresh (exactly as odevec_solve) and saves the state of
+   every successfully finished cell; resume = 1 continues each cell from its
+   saved state to the new t_stop (the Jacobian and rate coefficients are
+   recomputed, so the caller may change the temperature between calls; it
+   must not change the dynamic species).  Other arguments as odevec_solve. */
+int32_t odevec_workspace_doubles(const char* network, int64_t* per_cell);
+int32_t odevec_solve_resident(odevec_solver* s, int64_t ncells, double* y, double* t, double* dt,
+                              const double* t_stop, const uint8_t* mask, int32_t* status,
+                              int32_t* stats, double* workspace, int32_t resume, void* stream);
+
 /* CloseOdevec */
 int32_t odevec_close(odevec_solver* s);
 
@@ -152,7 +176,8 @@ const char* odevec_last_error(void);
    call resets the counter to zero on `stream` before the launch; all calls
    share the one counter, so calls that overlap on the GPU (different
    streams, or different host threads) race and must be serialised by the
-   caller. */
+   caller.  The FP32-LU escalation of odevec_solve (see no_escalation) needs
+   buffers and is not done here. */
 #define OV_NOALLOC_SCRATCH_BYTES 256
 #define OV_NOALLOC_MAX_CELLS (1LL << 40)
 int32_t odevec_solve_noalloc(const char* network, const odevec_opts* opts, int64_t ncells,

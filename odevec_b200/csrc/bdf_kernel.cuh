@@ -87,18 +87,28 @@ __device__ __forceinline__ double lcoef(int q, int k) { return c_lcoef[q][k]; }
 /* x^y out of line: the step-size selection calls it three times */
 static __device__ __noinline__ double pow_dev(double x, double y) { return ov_pow(x, y); }
 
-/* tau (src/odevec.F90:1034-1054) */
-__device__ __forceinline__ double tau(int order, int order2)
+/* tau (src/odevec.F90:1034-1054), evaluated at compile time with the same
+   IEEE operations: q! by repeated multiplication, then one division */
+constexpr double kL[7] = {0.0, 1.0, 1.0 / 3.0, 1.0 / 11.0, 1.0 / 50.0, 1.0 / 274.0, 1.0 / 1764.0};
+constexpr double tau_c(int order, int order2)
 {
     double faculty = 1.0;
-#pragma unroll
-    for (int i = 1; i <= MAXQ + 1; ++i)
-        if (i <= order)
-            faculty = faculty * i;
+    for (int i = 1; i <= order; ++i)
+        faculty = faculty * i;
     if (order - 1 == order2)
         return (order2 + 1.0) / faculty;
-    return (order2 + 1.0) / (faculty * lcoef(order, order));
+    return (order2 + 1.0) / (faculty * kL[order]);
 }
+/* per order q = 1..5: tau(q,q-1), tau(q,q), tau(q,q+1) and the
+   convergence-test divisor tau(q,q) / (2 (q+2)) (src/odevec.F90:640-641) */
+static __constant__ double c_tau[6][4] = {
+    {0, 0, 0, 0},
+#define OV_TAU_ROW(q) {tau_c(q, q - 1), tau_c(q, q), tau_c(q, q + 1), tau_c(q, q) / (2.0 * (q + 2.0))}
+    OV_TAU_ROW(1), OV_TAU_ROW(2), OV_TAU_ROW(3), OV_TAU_ROW(4), OV_TAU_ROW(5)
+#undef OV_TAU_ROW
+};
+__device__ __forceinline__ double tau(int order, int order2) { return c_tau[order][order2 - order + 1]; }
+__device__ __forceinline__ double conv_divisor(int order) { return c_tau[order][3]; }
 
 /* NaN and masked-out values never win a max (as the oracle's comparison loop) */
 __device__ __forceinline__ double max_operand(double v) { return v > -HUGE_VAL ? v : -HUGE_VAL; }
@@ -126,42 +136,51 @@ __device__ __forceinline__ bool group_any(bool b)
 /* Shared-memory staging: per-lane arrays laid out [entry][lane] with a
    stride of the block size, so a warp's 32 lanes touch 32 consecutive
    words (no bank conflicts). */
-constexpr int SHM_BLOCK = 128;
-
-template <class T>
+template <class T, int BS>
 struct LaneCol {
     T* base; /* &array[0][threadIdx.x] */
-    __device__ __forceinline__ T& operator[](int i) const { return base[i * SHM_BLOCK]; }
+    __device__ __forceinline__ T& operator[](int i) const { return base[i * BS]; }
 };
 
-template <int ND>
+template <int ND, int BS>
 struct LaneHist {
     double* base;
-    __device__ __forceinline__ LaneCol<double> operator[](int k) const
+    __device__ __forceinline__ LaneCol<double, BS> operator[](int k) const
     {
-        return LaneCol<double>{base + k * ND * SHM_BLOCK};
+        return LaneCol<double, BS>{base + k * ND * BS};
     }
 };
 
-template <class Net, class LUT, bool SHM>
+/* Kernel configurations ("stagings"): where the per-cell arrays live and the
+   launch shape.  BS threads per block, MINB blocks per SM for the register
+   budget; SHM places the Nordsieck history and the LU in shared memory. */
+template <int STAGE>
+struct StageCfg;
+template <> struct StageCfg<1> { static constexpr bool SHM = false; static constexpr int BS = 128, MINB = 2; };
+template <> struct StageCfg<2> { static constexpr bool SHM = true;  static constexpr int BS = 128, MINB = 1; };
+template <> struct StageCfg<3> { static constexpr bool SHM = false; static constexpr int BS = 128, MINB = 3; };
+template <> struct StageCfg<4> { static constexpr bool SHM = false; static constexpr int BS = 128, MINB = 4; };
+template <> struct StageCfg<5> { static constexpr bool SHM = true;  static constexpr int BS = 192, MINB = 1; };
+
+template <class Net, class LUT, bool SHM, int BS>
 struct Staging;
 
-template <class Net, class LUT>
-struct Staging<Net, LUT, false> { /* thread-local arrays (registers / local memory) */
+template <class Net, class LUT, int BS>
+struct Staging<Net, LUT, false, BS> { /* thread-local arrays (registers / local memory) */
     using Hist = double (*)[Net::ND];
     using LU = LUT*;
     static constexpr size_t smem_bytes = 0;
 };
 
-template <class Net, class LUT>
-struct Staging<Net, LUT, true> { /* shared memory, [entry][lane] */
-    using Hist = LaneHist<Net::ND>;
-    using LU = LaneCol<LUT>;
-    static constexpr size_t hist_bytes = sizeof(double) * (MAXQ + 1) * Net::ND * SHM_BLOCK;
-    static constexpr size_t smem_bytes = hist_bytes + sizeof(LUT) * Net::NNZ * SHM_BLOCK;
+template <class Net, class LUT, int BS>
+struct Staging<Net, LUT, true, BS> { /* shared memory, [entry][lane] */
+    using Hist = LaneHist<Net::ND, BS>;
+    using LU = LaneCol<LUT, BS>;
+    static constexpr size_t hist_bytes = sizeof(double) * (MAXQ + 1) * Net::ND * BS;
+    static constexpr size_t smem_bytes = hist_bytes + sizeof(LUT) * Net::NNZ * BS;
 };
 
-template <class Net, int G, class LUT, bool SHM = false>
+template <class Net, int G, class LUT, bool SHM = false, int BS = 128>
 struct Cell {
     static constexpr int N = Net::NEQ;  /* full state */
     static constexpr int ND = Net::ND;  /* solver state */
@@ -170,14 +189,14 @@ struct Cell {
     static constexpr int NR = Net::NREA > 0 ? Net::NREA : 1;
     static constexpr bool SCALED = sizeof(LUT) == 4;
 
-    typename Staging<Net, LUT, SHM>::Hist yns; /* Nordsieck history y_NS(0:5) */
+    typename Staging<Net, LUT, SHM, BS>::Hist yns; /* Nordsieck history y_NS(0:5) */
     double en[ND], eno[ND], w2[ND];
     double y[N];
-    typename Staging<Net, LUT, SHM>::LU a;     /* packed LU of the iteration matrix */
+    typename Staging<Net, LUT, SHM, BS>::LU a; /* packed LU of the iteration matrix */
     double rT[NR];
     double sc[SCALED ? ND : 1], isc[SCALED ? ND : 1];
 
-    double t, h, told, tstop, crate, jchg, cerr;
+    double t, h, told, tstop, crate, jchg, cerr, tint;
     double fz_add; /* 0, or NaN when a frozen species has a non-finite error weight */
     int q, swu, lju, fet, fc, it, ss_mode, wait;
     bool ujac, nuo, first, msk, fz_neg;
@@ -214,7 +233,8 @@ struct Cell {
     {
 #pragma unroll
         for (int j = 0; j < ND; ++j) {
-            double w = 1.0 / (rtol * fabs(y[Net::dyn(j)]) + atol);
+            /* correctly rounded reciprocal: the same bits as 1.0 / x */
+            double w = __drcp_rn(rtol * fabs(y[Net::dyn(j)]) + atol);
             w2[j] = w * w;
         }
     }
@@ -384,7 +404,7 @@ struct Cell {
             crate = fmax(0.2 * crate, rate_tmp);
         }
         const double r15 = 1.5 * crate;
-        const double crit = err * (1.0 < r15 ? 1.0 : r15) / (tau(q, q) / (2.0 * (q + 2.0)));
+        const double crit = err * (1.0 < r15 ? 1.0 : r15) / conv_divisor(q);
         bool nan = fz_add != fz_add;
 #pragma unroll
         for (int j = 0; j < ND; ++j)
@@ -521,29 +541,86 @@ struct Cell {
         }
         write_y = true;
         interpolate();
+        tint = t;
         t = tstop;
         return PH_DONE;
+    }
+
+    /* resident workspace: [field][cell] with stride ncells */
+    __device__ __forceinline__ void save_state(double* ws, int64_t n, int64_t cell) const
+    {
+        int f = 0;
+#pragma unroll 1
+        for (int k = 0; k <= MAXQ; ++k)
+#pragma unroll
+            for (int j = 0; j < ND; ++j)
+                ws[(f + k * ND + j) * n + cell] = yns[k][j];
+        f += (MAXQ + 1) * ND;
+#pragma unroll
+        for (int j = 0; j < ND; ++j) {
+            ws[(f + j) * n + cell] = eno[j];
+            ws[(f + ND + j) * n + cell] = w2[j];
+        }
+        f += 2 * ND;
+        const double sc[12] = {tint, h, crate, jchg, (double)q, (double)swu, (double)lju, (double)fet,
+                               (double)fc, ujac ? 1.0 : 0.0, nuo ? 1.0 : 0.0, first ? 1.0 : 0.0};
+#pragma unroll
+        for (int i = 0; i < 12; ++i)
+            ws[(f + i) * n + cell] = sc[i];
+    }
+
+    __device__ __forceinline__ void load_state(const double* ws, int64_t n, int64_t cell)
+    {
+        int f = 0;
+#pragma unroll 1
+        for (int k = 0; k <= MAXQ; ++k)
+#pragma unroll
+            for (int j = 0; j < ND; ++j)
+                yns[k][j] = ws[(f + k * ND + j) * n + cell];
+        f += (MAXQ + 1) * ND;
+#pragma unroll
+        for (int j = 0; j < ND; ++j) {
+            eno[j] = ws[(f + j) * n + cell];
+            w2[j] = ws[(f + ND + j) * n + cell];
+        }
+        f += 2 * ND;
+        t = ws[(f + 0) * n + cell];
+        h = ws[(f + 1) * n + cell];
+        crate = ws[(f + 2) * n + cell];
+        jchg = ws[(f + 3) * n + cell];
+        q = (int)ws[(f + 4) * n + cell];
+        swu = (int)ws[(f + 5) * n + cell];
+        lju = (int)ws[(f + 6) * n + cell];
+        fet = (int)ws[(f + 7) * n + cell];
+        fc = (int)ws[(f + 8) * n + cell];
+        ujac = ws[(f + 9) * n + cell] != 0.0;
+        nuo = ws[(f + 10) * n + cell] != 0.0;
+        first = ws[(f + 11) * n + cell] != 0.0;
     }
 };
 
 /* number of lanes of the warp for which b holds */
 __device__ __forceinline__ int warp_count(bool b) { return __popc(__ballot_sync(FULL, b)); }
 
-template <class Net, int G, class LUT, bool SHM>
-__global__ void __launch_bounds__(128, SHM ? 1 : 2) bdf_kernel(const LaunchArgs A)
+template <class Net, int G, class LUT, int STAGE>
+__global__ void __launch_bounds__(StageCfg<STAGE>::BS, StageCfg<STAGE>::MINB) bdf_kernel(const LaunchArgs A)
 {
-    using C = Cell<Net, G, LUT, SHM>;
+    constexpr bool SHM = StageCfg<STAGE>::SHM;
+    constexpr int BS = StageCfg<STAGE>::BS;
+    using C = Cell<Net, G, LUT, SHM, BS>;
     constexpr int N = C::N;
     constexpr int ND = C::ND;
     const int lane = threadIdx.x & 31;
     const int64_t ncells = A.ncells;
+    if (A.run_if && *A.run_if == 0)
+        return;
 
     C c;
     if constexpr (SHM) {
         extern __shared__ __align__(16) unsigned char ov_smem[];
-        c.yns = LaneHist<ND>{reinterpret_cast<double*>(ov_smem) + threadIdx.x};
-        c.a = LaneCol<LUT>{reinterpret_cast<LUT*>(ov_smem + Staging<Net, LUT, true>::hist_bytes)
-                           + threadIdx.x};
+        c.yns = LaneHist<ND, BS>{reinterpret_cast<double*>(ov_smem) + threadIdx.x};
+        c.a = LaneCol<LUT, BS>{reinterpret_cast<LUT*>(ov_smem + Staging<Net, LUT, true, BS>::hist_bytes)
+                               + threadIdx.x};
     }
     double history[SHM ? 1 : MAXQ + 1][ND];
     LUT lu_local[SHM ? 1 : C::NNZ];
@@ -634,6 +711,29 @@ __global__ void __launch_bounds__(128, SHM ? 1 : 2) bdf_kernel(const LaunchArgs 
                 if (skip) {
                     c.t = c.tstop; /* src/odevec.F90:187-191 */
                     ph = PH_DONE;
+                } else if (A.resume) {
+                    /* continuation: the saved history, step, order and
+                       weights; the state is the saved y_NS(0); rates and
+                       Jacobian are recomputed (the caller may have changed
+                       the temperature) */
+                    c.load_state(A.ws, ncells, cell);
+#pragma unroll
+                    for (int j = 0; j < ND; ++j)
+                        if (c.msk)
+                            c.y[Net::dyn(j)] = c.yns[0][j];
+                    if (Net::NREA > 0)
+                        Net::rates_T(c.y, c.rT);
+                    c.ujac = true;
+                    if (c.t < c.tstop) {
+                        c.told = c.t;
+                        ph = PH_PRED;
+                    } else {
+                        write_y = true;
+                        c.interpolate();
+                        c.tint = c.t;
+                        c.t = c.tstop;
+                        ph = PH_DONE;
+                    }
                 } else {
                     if (Net::NREA > 0)
                         Net::rates_T(c.y, c.rT);
@@ -719,6 +819,7 @@ __global__ void __launch_bounds__(128, SHM ? 1 : 2) bdf_kernel(const LaunchArgs 
             } else {
                 write_y = true;
                 c.interpolate();
+                c.tint = c.t;
                 c.t = c.tstop;
                 ph = PH_DONE;
             }
@@ -836,6 +937,8 @@ __global__ void __launch_bounds__(128, SHM ? 1 : 2) bdf_kernel(const LaunchArgs 
         /* ---- 7. store finished cells -------------------------------- */
         if (ph == PH_DONE) {
             const bool ok = c.status == OV_OK;
+            if (A.ws && ok && write_y)
+                c.save_state(A.ws, ncells, cell);
             if ((!ok || write_y) && c.msk) {
 #pragma unroll
                 for (int j = 0; j < ND; ++j)
@@ -863,15 +966,14 @@ __global__ void __launch_bounds__(128, SHM ? 1 : 2) bdf_kernel(const LaunchArgs 
 }
 
 /* Launch helper: persistent grid of (SMs x resident blocks) unless given. */
-template <class Net, int G, class LUT, bool SHM>
+template <class Net, int G, class LUT, int STAGE>
 cudaError_t launch(const LaunchArgs& a, int block, int grid, cudaStream_t stream)
 {
-    auto kern = bdf_kernel<Net, G, LUT, SHM>;
-    constexpr size_t smem = Staging<Net, LUT, SHM>::smem_bytes;
-    if (SHM)
-        block = SHM_BLOCK;
-    else if (block <= 0)
-        block = 128;
+    using Cfg = StageCfg<STAGE>;
+    auto kern = bdf_kernel<Net, G, LUT, STAGE>;
+    constexpr size_t smem = Staging<Net, LUT, Cfg::SHM, Cfg::BS>::smem_bytes;
+    if (Cfg::SHM || block <= 0 || block > Cfg::BS)
+        block = Cfg::BS;
     static int cached_grid[2] = {0, 0};
     if (cached_grid[0] == 0 || cached_grid[1] != block) {
         int dev = 0, sms = 0, per_sm = 0;
@@ -900,18 +1002,25 @@ cudaError_t launch(const LaunchArgs& a, int block, int grid, cudaStream_t stream
 }
 
 /* shared-memory staging is compiled for per-cell control when the per-lane
-   arrays of a 128-thread block fit in 200 KB */
-template <class Net, class LUT>
+   arrays of a block fit in 200 KB */
+template <class Net, class LUT, int BS>
 constexpr bool shm_fits()
 {
-    return Staging<Net, LUT, true>::smem_bytes <= 200 * 1024;
+    return Staging<Net, LUT, true, BS>::smem_bytes <= 200 * 1024;
 }
 
 }  // namespace OV_MODE_NS
 }  // namespace ov
 
 /* Defines the launcher of one network variant in the current mode.
-   stage: 1 = thread-local staging, 2 = shared-memory staging. */
+   stage: 1 = thread-local arrays, 2 blocks of 128 per SM; 2 = history and
+   LU in shared memory, 1 block of 128; 3, 4 = thread-local, 3 or 4 blocks of
+   128 (fewer registers, more warps); 5 = shared memory, 1 block of 192.
+   Stages 2-5 exist for per-cell control (G = 1). */
+#define OV_STAGE_CASE(NET, LU, ST)                                                               \
+    if (stage == ST)                                                                             \
+        return launch<NET, 1, LU, ST>(a, block, grid, s);
+
 #define OV_DEFINE_LAUNCHER(cid, FP32)                                                            \
     namespace ov {                                                                               \
     namespace OV_MODE_NS {                                                                       \
@@ -919,25 +1028,33 @@ constexpr bool shm_fits()
                              cudaStream_t s)                                                     \
     {                                                                                            \
         using NET = ov_net_##cid;                                                                \
-        if (stage == 2) {                                                                        \
-            if constexpr (shm_fits<NET, double>())                                               \
-                if (G == 1 && lu == 0)                                                           \
-                    return launch<NET, 1, double, true>(a, block, grid, s);                      \
-            if constexpr (FP32 && shm_fits<NET, float>())                                        \
-                if (G == 1 && lu == 1)                                                           \
-                    return launch<NET, 1, float, true>(a, block, grid, s);                       \
+        if (G == 1 && lu == 0) {                                                                 \
+            OV_STAGE_CASE(NET, double, 1)                                                        \
+            OV_STAGE_CASE(NET, double, 3)                                                        \
+            OV_STAGE_CASE(NET, double, 4)                                                        \
+            if constexpr (shm_fits<NET, double, 128>()) {                                        \
+                OV_STAGE_CASE(NET, double, 2)                                                    \
+            }                                                                                    \
             return cudaErrorNotSupported;                                                        \
         }                                                                                        \
-        if (G == 1 && lu == 0)                                                                   \
-            return launch<NET, 1, double, false>(a, block, grid, s);                             \
-        if (G == 32 && lu == 0)                                                                  \
-            return launch<NET, 32, double, false>(a, block, grid, s);                            \
         if constexpr (FP32) {                                                                    \
-            if (G == 1 && lu == 1)                                                               \
-                return launch<NET, 1, float, false>(a, block, grid, s);                          \
+            if (G == 1 && lu == 1) {                                                             \
+                OV_STAGE_CASE(NET, float, 1)                                                     \
+                OV_STAGE_CASE(NET, float, 3)                                                     \
+                OV_STAGE_CASE(NET, float, 4)                                                     \
+                if constexpr (shm_fits<NET, float, 128>()) {                                     \
+                    OV_STAGE_CASE(NET, float, 2)                                                 \
+                }                                                                                \
+                if constexpr (shm_fits<NET, float, 192>()) {                                     \
+                    OV_STAGE_CASE(NET, float, 5)                                                 \
+                }                                                                                \
+                return cudaErrorNotSupported;                                                    \
+            }                                                                                    \
             if (G == 32 && lu == 1)                                                              \
-                return launch<NET, 32, float, false>(a, block, grid, s);                         \
+                return launch<NET, 32, float, 1>(a, block, grid, s);                             \
         }                                                                                        \
+        if (G == 32 && lu == 0)                                                                  \
+            return launch<NET, 32, double, 1>(a, block, grid, s);                                \
         return cudaErrorNotSupported;                                                            \
     }                                                                                            \
     }                                                                                            \

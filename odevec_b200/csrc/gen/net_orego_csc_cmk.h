@@ -14,7 +14,7 @@
 #define OV_OREGO_CSC_CMK_NVECTOR 1
 #define OV_OREGO_CSC_CMK_DT_MIN 1e-10
 #define OV_OREGO_CSC_CMK_IDX_TGAS -1
-static const int ov_orego_csc_cmk_sizes[5] = {3, 7, 0, 0, -1};
+static const int ov_orego_csc_cmk_sizes[6] = {3, 7, 0, 0, -1, 3};
 static const double ov_orego_csc_cmk_defaults[2] = {1.0, 1e-10}; /* nvector, dt_min */
 static const int ov_orego_csc_cmk_perm[3] = {2, 1, 0};
 static const int ov_orego_csc_cmk_row_index[7] = {0, 1, 1, 2, 0, 1, 2};

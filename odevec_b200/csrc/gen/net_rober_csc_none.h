@@ -14,7 +14,7 @@
 #define OV_ROBER_CSC_NONE_NVECTOR 32
 #define OV_ROBER_CSC_NONE_DT_MIN 1e-20
 #define OV_ROBER_CSC_NONE_IDX_TGAS -1
-static const int ov_rober_csc_none_sizes[5] = {3, 8, 0, 0, -1};
+static const int ov_rober_csc_none_sizes[6] = {3, 8, 0, 0, -1, 3};
 static const double ov_rober_csc_none_defaults[2] = {32.0, 1e-20}; /* nvector, dt_min */
 static const int ov_rober_csc_none_perm[3] = {0, 1, 2};
 static const int ov_rober_csc_none_row_index[8] = {0, 1, 0, 1, 2, 0, 1, 2};

@@ -84,7 +84,35 @@ struct odevec_solver {
     uint8_t* d_mask;
     int32_t *d_status, *d_stats;
     cudaStream_t stream;
+    /* FP32-LU escalation: input copies, per-cell status and retry mask */
+    int64_t fb_cells;
+    double *fb_y, *fb_t, *fb_dt;
+    int32_t* fb_status;
+    uint8_t* fb_mask;
 };
+
+namespace {
+/* cells whose FP32-LU solve failed get their inputs back and a retry mask;
+   *nfail counts them */
+__global__ void ov_escalate(int64_t ncells, int neq, double* y, double* t, double* dt,
+                            const double* y_in, const double* t_in, const double* dt_in,
+                            const int32_t* status, const uint8_t* mask, uint8_t* retry,
+                            unsigned long long* nfail)
+{
+    for (int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; c < ncells;
+         c += (int64_t)gridDim.x * blockDim.x) {
+        const bool bad = status[c] != OV_OK && (!mask || mask[c]);
+        retry[c] = bad ? 1 : 0;
+        if (bad) {
+            for (int s = 0; s < neq; ++s)
+                y[(int64_t)s * ncells + c] = y_in[(int64_t)s * ncells + c];
+            t[c] = t_in[c];
+            dt[c] = dt_in[c];
+            atomicAdd(nfail, 1ull);
+        }
+    }
+}
+}  // namespace
 
 static int32_t resolve_opts(const NetEntry& e, const odevec_opts* in, odevec_opts* out)
 {
@@ -110,15 +138,15 @@ static int32_t resolve_opts(const NetEntry& e, const odevec_opts* in, odevec_opt
     if (o.max_attempts <= 0)
         o.max_attempts = 1000000;
     if (o.jac_batch <= 0)
-        o.jac_batch = 12;
+        o.jac_batch = 24;
     if (o.ss_batch <= 0)
-        o.ss_batch = 12;
+        o.ss_batch = 24;
     if (o.max_wait <= 0)
-        o.max_wait = o.max_wait < 0 ? 0 : 4;
+        o.max_wait = o.max_wait < 0 ? 0 : 8;
     if (o.jac_batch > 32 || o.ss_batch > 32)
         return fail(OV_API_EINVAL, "jac_batch and ss_batch must be <= 32");
-    if (o.staging < 0 || o.staging > 2)
-        return fail(OV_API_EINVAL, "staging must be 0, 1 or 2");
+    if (o.staging < 0 || o.staging > 5)
+        return fail(OV_API_EINVAL, "staging must be 0..5");
     if (o.block_threads < 0 || o.block_threads > 128 || o.block_threads % 32)
         return fail(OV_API_EINVAL, "block_threads must be 32, 64, 96 or 128 (0: automatic)");
     if (o.grid_blocks < 0)
@@ -205,9 +233,41 @@ int32_t odevec_set_options(odevec_solver* s, const odevec_opts* opts)
     return OV_API_OK;
 }
 
+static int32_t solve_impl(odevec_solver* s, int64_t ncells, double* y, double* t, double* dt,
+                          const double* t_stop, const uint8_t* mask, int32_t* status, int32_t* stats,
+                          double* ws, int32_t resume, void* stream);
+
 int32_t odevec_solve(odevec_solver* s, int64_t ncells, double* y, double* t, double* dt,
                      const double* t_stop, const uint8_t* mask, int32_t* status, int32_t* stats,
                      void* stream)
+{
+    return solve_impl(s, ncells, y, t, dt, t_stop, mask, status, stats, nullptr, 0, stream);
+}
+
+int32_t odevec_workspace_doubles(const char* network, int64_t* per_cell)
+{
+    const int i = find_net(network);
+    if (i < 0)
+        return fail(OV_API_ENONET, "unknown network variant '%s'", network ? network : "(null)");
+    if (!per_cell)
+        return fail(OV_API_EINVAL, "per_cell is null");
+    *per_cell = ov::ws_doubles(g_nets[i].sizes[5]);
+    return OV_API_OK;
+}
+
+int32_t odevec_solve_resident(odevec_solver* s, int64_t ncells, double* y, double* t, double* dt,
+                              const double* t_stop, const uint8_t* mask, int32_t* status,
+                              int32_t* stats, double* workspace, int32_t resume, void* stream)
+{
+    if (!workspace)
+        return fail(OV_API_EINVAL, "odevec_solve_resident: workspace is null");
+    return solve_impl(s, ncells, y, t, dt, t_stop, mask, status, stats, workspace, resume ? 1 : 0,
+                      stream);
+}
+
+static int32_t solve_impl(odevec_solver* s, int64_t ncells, double* y, double* t, double* dt,
+                          const double* t_stop, const uint8_t* mask, int32_t* status, int32_t* stats,
+                          double* ws, int32_t resume, void* stream)
 {
     if (!s)
         return fail(OV_API_EINVAL, "solver is null");
@@ -241,19 +301,64 @@ int32_t odevec_solve(odevec_solver* s, int64_t ncells, double* y, double* t, dou
     a.ss_batch = o.ss_batch;
     a.max_wait = o.max_wait;
     a.fix_restart = o.fix_restart ? 1 : 0;
+    a.ws = ws;
+    a.resume = resume;
+    a.run_if = nullptr;
     cudaStream_t st = (cudaStream_t)stream;
     cudaError_t err = cudaMemsetAsync(s->d_queue, 0, sizeof(unsigned long long), st);
     if (err != cudaSuccess)
         return fail(OV_API_ECUDA, "odevec_solve: %s", cudaGetErrorString(err));
     const int lu = o.precision == OV_PREC_FP32_LU ? 1 : 0;
     ov::launch_fn fn = o.precision == OV_PREC_FP64 ? e.exact : e.fma;
-    int stage = o.staging;
-    if (stage == 0) /* automatic: shared memory where compiled, else thread-local */
-        stage = (o.group_size == 1) ? 2 : 1;
+    /* automatic: thread-local arrays with 3 blocks of 128 per SM for per-cell
+       control (the fastest measured configuration), 2 blocks for lockstep */
+    const int stage = o.staging ? o.staging : (o.group_size == 1 ? 3 : 1);
+    const bool escalate = lu && !o.no_escalation;
+    const int neq = e.sizes[0];
+    if (escalate) {
+        /* FP32 factors can be too inaccurate for a badly conditioned cell
+           (Newton then fails until dt < dt_min): such cells are solved again
+           from their inputs with FP64 factors */
+        if (s->fb_cells < ncells) {
+            cudaFree(s->fb_y); cudaFree(s->fb_t); cudaFree(s->fb_dt); cudaFree(s->fb_status); cudaFree(s->fb_mask);
+            s->fb_y = nullptr; s->fb_t = nullptr; s->fb_dt = nullptr; s->fb_status = nullptr; s->fb_mask = nullptr;
+            s->fb_cells = 0;
+            const size_t n = (size_t)ncells;
+            err = cudaMalloc(&s->fb_y, sizeof(double) * n * neq);
+            if (err == cudaSuccess) err = cudaMalloc(&s->fb_t, sizeof(double) * n);
+            if (err == cudaSuccess) err = cudaMalloc(&s->fb_dt, sizeof(double) * n);
+            if (err == cudaSuccess) err = cudaMalloc(&s->fb_status, sizeof(int32_t) * n);
+            if (err == cudaSuccess) err = cudaMalloc(&s->fb_mask, n);
+            if (err != cudaSuccess)
+                return fail(OV_API_ENOMEM, "odevec_solve: escalation buffers: %s", cudaGetErrorString(err));
+            s->fb_cells = ncells;
+        }
+        const size_t n = (size_t)ncells;
+        err = cudaMemcpyAsync(s->fb_y, y, sizeof(double) * n * neq, cudaMemcpyDeviceToDevice, st);
+        if (err == cudaSuccess) err = cudaMemcpyAsync(s->fb_t, t, sizeof(double) * n, cudaMemcpyDeviceToDevice, st);
+        if (err == cudaSuccess) err = cudaMemcpyAsync(s->fb_dt, dt, sizeof(double) * n, cudaMemcpyDeviceToDevice, st);
+        if (err == cudaSuccess) err = cudaMemsetAsync(s->d_queue + 1, 0, sizeof(unsigned long long), st);
+        if (err != cudaSuccess)
+            return fail(OV_API_ECUDA, "odevec_solve: %s", cudaGetErrorString(err));
+        if (!a.status)
+            a.status = s->fb_status;
+    }
     err = fn(a, o.group_size, lu, stage, o.block_threads, o.grid_blocks, st);
-    if (err == cudaErrorNotSupported && o.staging == 0 && stage == 2) {
-        (void)cudaGetLastError();
-        err = fn(a, o.group_size, lu, 1, o.block_threads, o.grid_blocks, st);
+    if (escalate && err == cudaSuccess) {
+        int blocks = 0;
+        cudaDeviceGetAttribute(&blocks, cudaDevAttrMultiProcessorCount, s->device);
+        ov_escalate<<<blocks * 4, 256, 0, st>>>(ncells, neq, y, t, dt, s->fb_y, s->fb_t, s->fb_dt,
+                                                a.status, mask, s->fb_mask, s->d_queue + 1);
+        err = cudaGetLastError();
+        if (err == cudaSuccess) {
+            ov::LaunchArgs b = a;
+            b.mask = s->fb_mask;
+            b.stats = nullptr;
+            b.run_if = s->d_queue + 1;
+            err = cudaMemsetAsync(s->d_queue, 0, sizeof(unsigned long long), st);
+            if (err == cudaSuccess)
+                err = e.fma(b, o.group_size, 0, stage, o.block_threads, o.grid_blocks, st);
+        }
     }
     if (err == cudaErrorNotSupported)
         return fail(OV_API_EUNSUPPORTED, "variant %s: group %d precision %d not compiled", e.tag,
@@ -319,6 +424,11 @@ int32_t odevec_close(odevec_solver* s)
     cudaFree(s->d_mask);
     cudaFree(s->d_status);
     cudaFree(s->d_stats);
+    cudaFree(s->fb_y);
+    cudaFree(s->fb_t);
+    cudaFree(s->fb_dt);
+    cudaFree(s->fb_status);
+    cudaFree(s->fb_mask);
     if (s->stream)
         cudaStreamDestroy(s->stream);
     delete s;
@@ -430,15 +540,14 @@ extern "C" int32_t odevec_solve_noalloc(const char* network, const odevec_opts* 
     a.ss_batch = o.ss_batch;
     a.max_wait = o.max_wait;
     a.fix_restart = o.fix_restart ? 1 : 0;
+    a.ws = nullptr;
+    a.resume = 0;
+    a.run_if = nullptr;
     const NetEntry& e = g_nets[ni];
     const int lu = o.precision == OV_PREC_FP32_LU ? 1 : 0;
     ov::launch_fn fn = o.precision == OV_PREC_FP64 ? e.exact : e.fma;
-    int stage = o.staging ? o.staging : (o.group_size == 1 ? 2 : 1);
+    const int stage = o.staging ? o.staging : (o.group_size == 1 ? 3 : 1);
     err = fn(a, o.group_size, lu, stage, o.block_threads, o.grid_blocks, st);
-    if (err == cudaErrorNotSupported && o.staging == 0 && stage == 2) {
-        (void)cudaGetLastError();
-        err = fn(a, o.group_size, lu, 1, o.block_threads, o.grid_blocks, st);
-    }
     if (err == cudaErrorNotSupported)
         return fail(OV_API_EUNSUPPORTED, "variant %s: group %d precision %d not compiled", e.tag,
                     o.group_size, o.precision);

@@ -26,7 +26,20 @@ struct LaunchArgs {
     int32_t ss_batch;
     int32_t max_wait;
     int32_t fix_restart; /* undo the prediction before an order-1 restart */
+    /* resident integrator state (continuation across calls): ws = null for
+       none; otherwise ws holds ws_doubles(ND) doubles per cell, [field][cell],
+       written at the end of every successful solve and, with resume = 1,
+       read at the start instead of a fresh start */
+    double* ws;
+    int32_t resume;
+    /* if non-null, the kernel returns at once unless *run_if != 0 (a count
+       written by an earlier kernel on the same stream) */
+    const unsigned long long* run_if;
 };
+
+/* doubles per cell of the resident workspace: history y_NS(0:5), en_old,
+   error weights, and 12 scalars (internal time, step, control state) */
+__host__ __device__ constexpr int ws_doubles(int nd) { return 6 * nd + 2 * nd + 12; }
 
 /* one launcher per network variant and arithmetic mode; returns the CUDA
    error of the launch.  G: 1 or 32; lu: 0 = FP64 LU, 1 = FP32 LU;

@@ -338,7 +338,7 @@ def emit_c_header(sysm: System) -> str:
         L.append("static const int ov_%s_%s[%d] = {%s};" % (cid, name, len(vals),
                                                           ", ".join(str(v) for v in vals)))
     arr("sizes", [n, nnz, net.nrea if net.rates else 0, 1 if sysm.packaging == "DENSE" else 0,
-                  net.idx_tgas if net.idx_tgas is not None else -1])
+                  net.idx_tgas if net.idx_tgas is not None else -1, n - len(frozen_species(sysm))])
     L.append("static const double ov_%s_defaults[2] = {%d.0, %r}; /* nvector, dt_min */"
              % (cid, sysm.nvector, float(sysm.dt_min)))
     arr("perm", sysm.perm)

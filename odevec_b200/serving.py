@@ -1,0 +1,343 @@
+"""Serving loop: continuous batching of solve requests on one GPU.
+
+A request is a set of cells of one network, as an operator-split hydro code
+hands them over: it is advanced through `steps` successive hydro steps
+(t_stop = t0 + k * dt_hydro), and between steps its integrator state --
+Nordsieck history, order, step size, error weights -- stays resident on the
+device (odevec_solve_resident), so a hydro step costs only the integration
+steps it needs.
+
+Continuous batching: requests arrive over time; a request is admitted as
+soon as its device memory fits in the HBM budget and an execution slot (a
+CUDA stream) is free, not when the previous batch ends.  Every admitted
+request advances on its own stream, so the steps of different requests and
+networks overlap on the device; a finished step immediately queues the
+request's next step.  Cells are independent and every launch is
+deterministic, so a request's results are the same alone and in any mix
+(tests/test_serving.py).
+
+Latency of a request step = completion time - the time the step became
+ready (its arrival for step 0, the previous step's completion after that),
+so it includes any wait for admission.
+
+Failures: where the reference stops the program (src/odevec.F90:272-275,
+380-390), a cell here gets a nonzero status.  A failed cell keeps its
+first nonzero status and is masked out of the request's later hydro steps
+(its state stays at the failure); the request still completes, and its
+result carries the per-cell status next to the state.
+
+The scheduler is backend-agnostic: GpuBackend drives the CUDA library;
+tests drive the same scheduler with a CPU backend built on the oracle.
+"""
+from __future__ import annotations
+
+import dataclasses
+import time
+from typing import Dict, List, Optional
+
+import numpy as np
+
+
+@dataclasses.dataclass
+class Request:
+    rid: int
+    network: str
+    y0: np.ndarray            # (neq, ncells)
+    dt_hydro: float
+    steps: int
+    arrival: float            # seconds after the stream starts
+    rtol: float
+    atol: float
+    dt_min: float
+    dt_in: float = 1e-10
+
+    @property
+    def ncells(self) -> int:
+        return self.y0.shape[1]
+
+
+@dataclasses.dataclass
+class StepRecord:
+    rid: int
+    step: int
+    ncells: int
+    network: str
+    ready: float
+    done: float
+
+    @property
+    def latency(self) -> float:
+        return self.done - self.ready
+
+
+@dataclasses.dataclass
+class Result:
+    y: np.ndarray             # (neq, ncells) state after the last hydro step
+    status: np.ndarray        # (ncells,) first nonzero status of each cell, 0 = OK
+
+    @property
+    def failed(self) -> int:
+        return int(np.count_nonzero(self.status))
+
+
+class Scheduler:
+    """Admission by memory budget and slot count, FIFO by readiness."""
+
+    def __init__(self, backend, hbm_budget: float, slots: int):
+        self.backend = backend
+        self.budget = float(hbm_budget)
+        self.slots = int(slots)
+
+    def run(self, requests: List[Request], realtime: bool = True, poll_s: float = 2e-4):
+        pending = sorted(requests, key=lambda r: (r.arrival, r.rid))
+        waiting: List[Request] = []            # arrived, not admitted
+        active: Dict[int, dict] = {}           # rid -> state
+        used = 0.0
+        records: List[StepRecord] = []
+        results: Dict[int, Result] = {}
+        t_start = time.perf_counter()
+        now = lambda: time.perf_counter() - t_start
+        i = 0
+        while i < len(pending) or waiting or active:
+            t = now()
+            if not realtime and not waiting and not active and i < len(pending):
+                t = pending[i].arrival  # jump to the next arrival when idle
+                t_start -= max(0.0, t - now())
+            while i < len(pending) and pending[i].arrival <= now():
+                waiting.append(pending[i])
+                i += 1
+            # admit in arrival order while memory and slots allow
+            while waiting and len(active) < self.slots:
+                r = waiting[0]
+                need = self.backend.bytes_needed(r)
+                if need > self.budget:
+                    raise ValueError("request %d needs %.1f GB, more than the budget" % (r.rid, need / 1e9))
+                if used + need > self.budget:
+                    break
+                waiting.pop(0)
+                used += need
+                h = self.backend.admit(r)
+                active[r.rid] = {"req": r, "h": h, "step": 0, "ready": max(r.arrival, 0.0), "need": need}
+                self.backend.launch(h, 0)
+            # completions
+            done_any = False
+            for rid in list(active):
+                st = active[rid]
+                if self.backend.finished(st["h"]):
+                    done_any = True
+                    tdone = now()
+                    r = st["req"]
+                    records.append(StepRecord(rid, st["step"], r.ncells, r.network, st["ready"], tdone))
+                    st["step"] += 1
+                    if st["step"] < r.steps:
+                        st["ready"] = tdone
+                        self.backend.launch(st["h"], st["step"])
+                    else:
+                        results[rid] = self.backend.release(st["h"])
+                        used -= st["need"]
+                        del active[rid]
+            if not done_any:
+                time.sleep(poll_s)
+        return records, results
+
+
+def summarize(records: List[StepRecord], results: Optional[Dict[int, Result]] = None) -> dict:
+    lat = np.array([r.latency for r in records]) if records else np.zeros(1)
+    t0 = min(r.ready for r in records) if records else 0.0
+    t1 = max(r.done for r in records) if records else 1.0
+    cells = sum(r.ncells for r in records)
+    return {"request_steps": len(records), "cells": cells, "seconds": t1 - t0,
+            "cells_per_s": cells / max(t1 - t0, 1e-12),
+            "p50_ms": 1e3 * float(np.percentile(lat, 50)), "p99_ms": 1e3 * float(np.percentile(lat, 99)),
+            "max_ms": 1e3 * float(lat.max())} | (
+        {} if results is None else
+        {"failed_cells": sum(results[rid].failed for rid in {r.rid for r in records} if rid in results)})
+
+
+class GpuBackend:
+    """Each admitted request owns device buffers, a resident workspace and a
+    CUDA stream; launches are asynchronous and completion is an event."""
+
+    def __init__(self, precision: str = "fp32_lu", device: str = "cuda"):
+        import torch
+        from . import solver as S
+        self.S = S
+        self.torch = torch
+        self.precision = precision
+        self.device = device
+
+    def _solver(self, r: Request):
+        # one solver handle per request: each owns its cell counter, so
+        # concurrent launches on different streams never share one
+        ode = self.S.Odevec(r.network, RelativeTolerance=r.rtol, AbsoluteTolerance=r.atol,
+                            MinimalTimestep=r.dt_min, nvector=1, precision=self.precision,
+                            raise_on_failure=False)
+        self.S.InitOdevec(ode)
+        return ode
+
+    def bytes_needed(self, r: Request) -> float:
+        per_cell = 8 * (r.y0.shape[0] + 3 + self.S.workspace_doubles(r.network)) + 4 + 8 * 8
+        return float(per_cell * r.ncells)
+
+    def admit(self, r: Request):
+        torch = self.torch
+        ode = self._solver(r)
+        stream = torch.cuda.Stream(device=self.device)
+        with torch.cuda.stream(stream):
+            h = {"r": r, "ode": ode, "stream": stream,
+                 "y": torch.tensor(r.y0, device=self.device),
+                 "t": torch.zeros(r.ncells, dtype=torch.float64, device=self.device),
+                 "dt": torch.full((r.ncells,), r.dt_in, dtype=torch.float64, device=self.device),
+                 "ts": torch.empty(r.ncells, dtype=torch.float64, device=self.device),
+                 "ws": self.S.Workspace(ode, r.ncells, self.device),
+                 "failed": torch.zeros(r.ncells, dtype=torch.int32, device=self.device),
+                 "mask": torch.ones(r.ncells, dtype=torch.uint8, device=self.device),
+                 "ev": None}
+        return h
+
+    def launch(self, h, step: int):
+        torch = self.torch
+        r = h["r"]
+        with torch.cuda.stream(h["stream"]):
+            h["ts"].fill_(r.dt_hydro * (step + 1))
+            if step > 0:
+                h["mask"].copy_(h["failed"] == 0)
+            self.S.SolveODE(h["ode"], h["t"], h["dt"], h["ts"], h["y"], Mask=h["mask"], stream=h["stream"],
+                            want_stats=False, workspace=h["ws"], resume=step > 0)
+            st = h["ode"].status
+            torch.where(h["failed"] != 0, h["failed"], st, out=h["failed"])
+            ev = torch.cuda.Event()
+            ev.record(h["stream"])
+            h["ev"] = ev
+
+    def finished(self, h) -> bool:
+        return h["ev"] is not None and h["ev"].query()
+
+    def release(self, h):
+        h["stream"].synchronize()
+        res = Result(h["y"].cpu().numpy(), h["failed"].cpu().numpy())
+        self.S.CloseOdevec(h["ode"])
+        return res
+
+    def close(self):
+        pass
+
+
+class OracleBackend:
+    """CPU stand-in with the same interface: each step runs synchronously on
+    the oracle (used to test the scheduler without a GPU)."""
+
+    def __init__(self, nthreads: int = 1):
+        from oracle import oracle as O
+        self.O = O
+        self.nthreads = nthreads
+
+    def bytes_needed(self, r: Request) -> float:
+        return float(8 * r.y0.size + 8 * self.O.lib().ov_oracle_ws_doubles(r.network.encode(), r.ncells, 1))
+
+    def admit(self, r: Request):
+        return {"r": r, "y": r.y0.copy(), "t": np.zeros(r.ncells), "dt": np.full(r.ncells, r.dt_in),
+                "ws": self.O.workspace(r.network, r.ncells), "failed": np.zeros(r.ncells, np.int32),
+                "done": False}
+
+    def launch(self, h, step: int):
+        r = h["r"]
+        mask = None if step == 0 else (h["failed"] == 0).astype(np.uint8)
+        y, t, dt, st, _ = self.O.solve(r.network, h["y"], h["t"], h["dt"], r.dt_hydro * (step + 1), r.rtol,
+                                       r.atol, r.dt_min, mask=mask, ws=h["ws"], resume=step > 0,
+                                       nthreads=self.nthreads)
+        h["failed"] = np.where(h["failed"] != 0, h["failed"], st).astype(np.int32)
+        h["y"], h["t"], h["dt"], h["done"] = y, t, dt, True
+
+    def finished(self, h) -> bool:
+        return h["done"]
+
+    def release(self, h):
+        return Result(h["y"], h["failed"])
+
+    def close(self):
+        pass
+
+
+def make_stream(seed: int = 5, rate: float = 200.0, duration: float = 1.0,
+                networks=("ROBER_DENSE_NONE", "PRIMORDIAL_CSC_FF", "SYN64_CSC_CMK"),
+                cells=(1000, 262144), dt_hydro=(1e6, 1e11), steps: int = 50,
+                max_requests: Optional[int] = None) -> List[Request]:
+    """Poisson arrivals of requests drawn uniformly from `networks`, with
+    log-uniform cell counts and hydro time steps (the serving configuration:
+    200 requests/s, 1k-256k cells, dt 1e6-1e11 s, 50 steps each)."""
+    from . import workloads as W
+    rng = np.random.default_rng(seed)
+    out = []
+    t = 0.0
+    rid = 0
+    while True:
+        t += rng.exponential(1.0 / rate)
+        if t > duration or (max_requests is not None and rid >= max_requests):
+            break
+        net = networks[int(rng.integers(len(networks)))]
+        n = int(round(10.0 ** rng.uniform(np.log10(cells[0]), np.log10(cells[1]))))
+        name = net.split("_")[0]
+        if name not in W.BUILDERS:
+            raise ValueError("no workload generator for network %s" % net)
+        wl = W.BUILDERS[name](ncells=n, seed=1000 + rid, network=net)
+        dth = float(10.0 ** rng.uniform(np.log10(dt_hydro[0]), np.log10(dt_hydro[1])))
+        out.append(Request(rid, net, wl.y, dth, steps, t, wl.rtol, wl.atol, wl.dt_min,
+                           dt_in=float(wl.dt0[0])))
+        rid += 1
+    return out
+
+
+def main(argv=None):
+    """Serving measurement: python -m odevec_b200.serving [options]; prints one
+    JSON line per precision form."""
+    import argparse
+    import json
+    p = argparse.ArgumentParser()
+    p.add_argument("--rate", type=float, default=200.0, help="mean arrivals per second (Poisson)")
+    p.add_argument("--duration", type=float, default=0.25, help="seconds of arrivals")
+    p.add_argument("--steps", type=int, default=50, help="hydro steps per request")
+    p.add_argument("--min-cells", type=int, default=1000)
+    p.add_argument("--max-cells", type=int, default=262144)
+    p.add_argument("--dt-min", type=float, default=1e6, help="smallest hydro step (s)")
+    p.add_argument("--dt-max", type=float, default=1e11, help="largest hydro step (s)")
+    p.add_argument("--networks", default="ROBER_DENSE_NONE,PRIMORDIAL_CSC_FF,SYN64_CSC_CMK")
+    p.add_argument("--precisions", default="fp32_lu,fp64")
+    p.add_argument("--budget", type=float, default=120e9, help="HBM admission budget (bytes)")
+    p.add_argument("--slots", type=int, default=16, help="requests in flight")
+    p.add_argument("--seed", type=int, default=5)
+    p.add_argument("--isolated", action="store_true", help="also time every request alone")
+    a = p.parse_args(argv)
+    reqs = make_stream(a.seed, a.rate, a.duration, tuple(a.networks.split(",")), (a.min_cells, a.max_cells),
+                       (a.dt_min, a.dt_max), a.steps)
+    for prec in a.precisions.split(","):
+        be = GpuBackend(prec)
+        # warm-up: one small request per network (module load, first launches)
+        warm = [Request(10**6 + i, r.network, r.y0[:, :64].copy(), r.dt_hydro, 1, 0.0, r.rtol, r.atol,
+                        r.dt_min, r.dt_in) for i, r in enumerate({r.network: r for r in reqs}.values())]
+        Scheduler(be, a.budget, a.slots).run(warm, realtime=False)
+        recs, res = Scheduler(be, a.budget, a.slots).run(reqs, realtime=True)
+        out = {"form": prec, "requests": len(reqs), "rate": a.rate, "steps": a.steps,
+               "cells": [a.min_cells, a.max_cells], "dt_hydro": [a.dt_min, a.dt_max],
+               "budget_gb": a.budget / 1e9, "slots": a.slots, "mix": summarize(recs, res)}
+        by_net = {}
+        for r in recs:
+            by_net.setdefault(r.network, []).append(r)
+        out["per_network"] = {k: summarize(v, res) for k, v in by_net.items()}
+        if a.isolated:
+            iso = {}
+            for r in reqs:
+                rr, _ = Scheduler(be, a.budget, 1).run([dataclasses.replace(r, arrival=0.0)], realtime=False)
+                for x in rr:
+                    iso[(x.rid, x.step)] = x.latency
+            ratio = np.array([x.latency / iso[(x.rid, x.step)] for x in recs])
+            iso_l = np.array(list(iso.values()))
+            out["isolated"] = {"p50_ms": 1e3 * float(np.percentile(iso_l, 50)),
+                               "p99_ms": 1e3 * float(np.percentile(iso_l, 99)),
+                               "mix_over_isolated_p50": float(np.percentile(ratio, 50)),
+                               "mix_over_isolated_p99": float(np.percentile(ratio, 99))}
+        print(json.dumps(out), flush=True)
+
+
+if __name__ == "__main__":
+    main()

@@ -62,7 +62,7 @@ class _Opts(ctypes.Structure):
                 ("precision", ctypes.c_int32), ("max_attempts", ctypes.c_int32),
                 ("jac_batch", ctypes.c_int32), ("ss_batch", ctypes.c_int32), ("max_wait", ctypes.c_int32),
                 ("staging", ctypes.c_int32), ("block_threads", ctypes.c_int32), ("grid_blocks", ctypes.c_int32),
-                ("fix_restart", ctypes.c_int32)]
+                ("fix_restart", ctypes.c_int32), ("no_escalation", ctypes.c_int32)]
 
 
 _lib = None
@@ -90,6 +90,10 @@ def lib():
         L.odevec_solve.restype = i32
         L.odevec_solve_host.argtypes = [P, i64, P, P, P, P, P, P, P]
         L.odevec_solve_host.restype = i32
+        L.odevec_workspace_doubles.argtypes = [ctypes.c_char_p, ctypes.POINTER(i64)]
+        L.odevec_workspace_doubles.restype = i32
+        L.odevec_solve_resident.argtypes = [P, i64, P, P, P, P, P, P, P, P, i32, P]
+        L.odevec_solve_resident.restype = i32
         L.odevec_close.argtypes = [P]
         L.odevec_close.restype = i32
         L.odevec_last_error.restype = ctypes.c_char_p
@@ -122,7 +126,8 @@ class Odevec:
                  CheckNegatives: bool = False, nvector: Optional[int] = None,
                  precision: str = "fp64", max_attempts: int = 0, raise_on_failure: bool = True,
                  jac_batch: int = 0, ss_batch: int = 0, max_wait: int = 0, staging: int = 0,
-                 block_threads: int = 0, grid_blocks: int = 0, fix_restart: bool = False):
+                 block_threads: int = 0, grid_blocks: int = 0, fix_restart: bool = False,
+                 escalation: bool = True):
         info = network_info(network)
         self.network = network
         self.neq = info["neq"]
@@ -145,6 +150,7 @@ class Odevec:
         self.block_threads = block_threads
         self.grid_blocks = grid_blocks
         self.fix_restart = fix_restart
+        self.escalation = escalation
         self.status = None
         self.stats = None
         self._h = None
@@ -167,6 +173,7 @@ class Odevec:
         o.block_threads = int(self.block_threads)
         o.grid_blocks = int(self.grid_blocks)
         o.fix_restart = 1 if self.fix_restart else 0
+        o.no_escalation = 0 if self.escalation else 1
         return o
 
     @property
@@ -213,7 +220,21 @@ def _as_cells(a, ncells, name, torch_mod=None, device=None):
     return np.ascontiguousarray(a)
 
 
-def SolveODE(ode: Odevec, time, dt, t_stop, y, Mask=None, stream=None, want_stats=True):
+def workspace_doubles(network: str) -> int:
+    n = ctypes.c_int64()
+    _check(lib().odevec_workspace_doubles(network.encode(), ctypes.byref(n)))
+    return int(n.value)
+
+
+def Workspace(ode: Odevec, ncells: int, device=None):
+    """Device buffer for the resident integrator state of ncells cells."""
+    import torch
+    return torch.zeros(workspace_doubles(ode.network) * ncells, dtype=torch.float64,
+                       device=device or "cuda")
+
+
+def SolveODE(ode: Odevec, time, dt, t_stop, y, Mask=None, stream=None, want_stats=True,
+             workspace=None, resume=False):
     """Integrates every cell from ``time`` to ``t_stop`` (src/odevec.F90:158-214).
 
     ``y``: species-major storage of ``ncells x neq`` values: a torch CUDA
@@ -250,8 +271,16 @@ def SolveODE(ode: Odevec, time, dt, t_stop, y, Mask=None, stream=None, want_stat
         st = stream if stream is not None else torch.cuda.current_stream(dev)
         ptr = lambda a: None if a is None else ctypes.c_void_p(a.data_ptr())
         with torch.cuda.device(dev):
-            _check(lib().odevec_solve(h, ncells, ptr(y), ptr(t), ptr(d), ptr(ts), ptr(m),
-                                      ptr(status), ptr(stats), ctypes.c_void_p(st.cuda_stream)))
+            if workspace is None:
+                _check(lib().odevec_solve(h, ncells, ptr(y), ptr(t), ptr(d), ptr(ts), ptr(m),
+                                          ptr(status), ptr(stats), ctypes.c_void_p(st.cuda_stream)))
+            else:
+                if workspace.numel() < workspace_doubles(ode.network) * ncells or not workspace.is_cuda:
+                    raise ValueError("workspace too small: use Workspace(ode, ncells)")
+                _check(lib().odevec_solve_resident(h, ncells, ptr(y), ptr(t), ptr(d), ptr(ts), ptr(m),
+                                                   ptr(status), ptr(stats), ptr(workspace),
+                                                   1 if resume else 0,
+                                                   ctypes.c_void_p(st.cuda_stream)))
         ode.status, ode.stats = status, stats
         if ode.raise_on_failure:
             bad = int((status != 0).sum().item())

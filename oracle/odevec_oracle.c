@@ -664,8 +664,85 @@ static void interpolate(ode_t* o, double t, double dt, double t_out, double* y)
     }
 }
 
+/* resident state of a group (continuation across calls, no counterpart in
+   the reference): y_NS(0:5), en_old, weights, then 12 scalars */
+static size_t ws_group_doubles(int neq, int G) { return (size_t)8 * neq * G + 12; }
+
+static void save_state(ode_t* o, double t_int, double dt, double* w)
+{
+    const size_t N = (size_t)o->neq * o->G;
+    memcpy(w, o->y_NS, sizeof(double) * N * (MAXORDER + 1));
+    memcpy(w + N * (MAXORDER + 1), o->en_old, sizeof(double) * N);
+    memcpy(w + N * (MAXORDER + 2), o->w2, sizeof(double) * N);
+    double* s = w + N * (MAXORDER + 3);
+    s[0] = t_int;
+    s[1] = dt;
+    s[2] = o->ConvergenceRate;
+    s[3] = o->JacobianChange;
+    s[4] = o->order;
+    s[5] = o->SuccessesWithoutUpdate;
+    s[6] = o->LastJacobianUpdate;
+    s[7] = o->FailedErrorTests;
+    s[8] = o->FailedCorrections;
+    s[9] = o->UpdateJac;
+    s[10] = o->NeglectUpperOrder;
+    s[11] = o->FirstStep;
+}
+
+static void load_state(ode_t* o, double* t_int, double* dt, const double* w)
+{
+    const size_t N = (size_t)o->neq * o->G;
+    memcpy(o->y_NS, w, sizeof(double) * N * (MAXORDER + 1));
+    memcpy(o->en_old, w + N * (MAXORDER + 1), sizeof(double) * N);
+    memcpy(o->w2, w + N * (MAXORDER + 2), sizeof(double) * N);
+    const double* s = w + N * (MAXORDER + 3);
+    *t_int = s[0];
+    *dt = s[1];
+    o->ConvergenceRate = s[2];
+    o->JacobianChange = s[3];
+    o->order = (int)s[4];
+    o->SuccessesWithoutUpdate = (int)s[5];
+    o->LastJacobianUpdate = (int)s[6];
+    o->FailedErrorTests = (int)s[7];
+    o->FailedCorrections = (int)s[8];
+    o->UpdateJac = s[9] != 0.0;
+    o->NeglectUpperOrder = s[10] != 0.0;
+    o->FirstStep = s[11] != 0.0;
+}
+
+/* continuation: from the saved state to t_stop, the state saved again */
+static void resume_group(ode_t* o, double* time, double* dt, double t_stop, double* y, double* w)
+{
+    if (o->mask) {
+        int any = 0;
+        for (int i = 0; i < o->G; ++i)
+            any |= o->mask[i] != 0;
+        if (!any) {
+            *time = t_stop;
+            return;
+        }
+    }
+    double t_int;
+    load_state(o, &t_int, dt, w);
+    masked_copy(o, y, NS(o, 0));
+    if (o->net->nrea) {
+        for (int i = 0; i < o->G; ++i)
+            ov_rates_primordial_T(y[(size_t)o->net->idx_tgas * o->G + i], o->rT + (size_t)i * o->net->nrea);
+    }
+    o->UpdateJac = 1;
+    *time = t_int;
+    while (*time < t_stop) {
+        solve_linear_system(o, time, dt, y);
+        if (o->status)
+            return;
+    }
+    interpolate(o, *time, *dt, t_stop, y);
+    save_state(o, *time, *dt, w);
+    *time = t_stop;
+}
+
 /* SolveODE for one group (src/odevec.F90:158-214) */
-static void solve_group(ode_t* o, double* time, double* dt, double t_stop, double* y)
+static void solve_group(ode_t* o, double* time, double* dt, double t_stop, double* y, double* w)
 {
     const size_t N = (size_t)o->neq * o->G;
     o->FirstStep = 1;
@@ -706,6 +783,8 @@ static void solve_group(ode_t* o, double* time, double* dt, double t_stop, doubl
             return;
     }
     interpolate(o, *time, *dt, t_stop, y);
+    if (w)
+        save_state(o, *time, *dt, w);
     *time = t_stop;
 }
 
@@ -713,7 +792,7 @@ static void solve_group(ode_t* o, double* time, double* dt, double t_stop, doubl
 int ov_oracle_solve(const char* tag, int64_t ncells, int G, double rtol, double atol,
                     double dt_min, int check_negatives, int fix_restart, int64_t max_attempts, double* y, double* t,
                     double* dt, const double* t_stop, const uint8_t* mask, int32_t* status,
-                    int32_t* stats, int nthreads)
+                    int32_t* stats, int nthreads, double* ws, int resume)
 {
     const net_desc* net = net_find(tag);
     if (!net)
@@ -781,10 +860,13 @@ int ov_oracle_solve(const char* tag, int64_t ncells, int G, double rtol, double 
             memset(o.y_NS, 0, sizeof(double) * N * NNS);
             memset(o.en_old, 0, sizeof(double) * N);
             double time = t[c0], h = dt[c0];
+            double* w = ws ? ws + (size_t)g * ws_group_doubles(n, G) : NULL;
             if (bad)
                 o.status = OV_ERR_GROUP_MISMATCH;
+            else if (resume && w)
+                resume_group(&o, &time, &h, t_stop[c0], o.ytmp, w);
             else
-                solve_group(&o, &time, &h, t_stop[c0], o.ytmp);
+                solve_group(&o, &time, &h, t_stop[c0], o.ytmp, w);
             for (int i = 0; i < G; ++i) {
                 const int64_t c = c0 + i;
                 for (int j = 0; j < n; ++j)
@@ -848,6 +930,14 @@ int ov_oracle_netinfo(const char* tag, int* info /* neq nnz nrea dense idx_tgas 
     if (u_col_start) memcpy(u_col_start, net->u_col_start, sizeof(int) * (net->neq + 1));
     if (l_col_start) memcpy(l_col_start, net->l_col_start, sizeof(int) * net->neq);
     return 0;
+}
+
+int64_t ov_oracle_ws_doubles(const char* tag, int64_t ncells, int G)
+{
+    const net_desc* net = net_find(tag);
+    if (!net || G < 1 || ncells % G)
+        return -1;
+    return (ncells / G) * (int64_t)ws_group_doubles(net->neq, G);
 }
 
 int ov_oracle_num_nets(void) { return g_nnets; }

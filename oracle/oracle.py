@@ -22,7 +22,9 @@ def lib():
         d, i64, i32 = ctypes.c_double, ctypes.c_int64, ctypes.c_int
         P = ctypes.c_void_p
         L.ov_oracle_solve.argtypes = [ctypes.c_char_p, i64, i32, d, d, d, i32, i32, i64, P, P, P, P,
-                                      P, P, P, i32]
+                                      P, P, P, i32, P, i32]
+        L.ov_oracle_ws_doubles.argtypes = [ctypes.c_char_p, i64, i32]
+        L.ov_oracle_ws_doubles.restype = i64
         L.ov_oracle_solve.restype = i32
         L.ov_oracle_eval.argtypes = [ctypes.c_char_p, P, P, d, d, P, P]
         L.ov_oracle_rates.argtypes = [d, P]
@@ -65,9 +67,10 @@ def tags():
 
 
 def solve(tag, y, t, dt, t_stop, rtol, atol, dt_min, group=1, check_negatives=False,
-          mask=None, max_attempts=1000000, nthreads=0, fix_restart=False):
+          mask=None, max_attempts=1000000, nthreads=0, fix_restart=False, ws=None, resume=False):
     """SolveODE on all cells.  y: (neq, ncells) float64, modified copy returned
-    with t, dt, status, stats."""
+    with t, dt, status, stats.  ws: a workspace from workspace() to save the
+    integrator state into (and, with resume, to continue from)."""
     y = np.ascontiguousarray(y, dtype=np.float64).copy()
     ncells = y.shape[1]
     t = np.ascontiguousarray(np.broadcast_to(t, (ncells,)), dtype=np.float64).copy()
@@ -79,7 +82,8 @@ def solve(tag, y, t, dt, t_stop, rtol, atol, dt_min, group=1, check_negatives=Fa
     rc = lib().ov_oracle_solve(tag.encode(), ncells, group, rtol, atol, dt_min,
                                int(bool(check_negatives)), int(bool(fix_restart)), max_attempts,
                                _p(y), _p(t), _p(dt),
-                               _p(t_stop), _p(m), _p(status), _p(stats), nthreads)
+                               _p(t_stop), _p(m), _p(status), _p(stats), nthreads, _p(ws),
+                               int(bool(resume)))
     if rc != 0:
         raise ValueError("oracle solve failed rc=%d" % rc)
     return y, t, dt, status, stats
@@ -99,3 +103,10 @@ def rates(T):
     r = np.zeros(38)
     lib().ov_oracle_rates(float(T), _p(r))
     return r
+
+
+def workspace(tag, ncells, group=1):
+    n = lib().ov_oracle_ws_doubles(tag.encode(), ncells, group)
+    if n < 0:
+        raise ValueError("bad workspace request")
+    return np.zeros(n, np.float64)

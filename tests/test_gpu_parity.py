@@ -223,3 +223,88 @@ def test_syn64_mass_conservation(gpu_lib):
     assert np.all(g[3] == 0)
     m = syn64.masses()
     assert np.max(np.abs(m @ g[0] - m @ wl.y) / (m @ wl.y)) < 1e-4
+
+
+def _resident_steps(gpu_lib, oracle, wl, precision, nsteps, group):
+    """Advance the same cells through nsteps successive t_stop values with the
+    integrator state kept on the device; compare every step with the oracle's
+    continuation."""
+    import torch
+    ode = gpu_lib.Odevec(wl.network, RelativeTolerance=wl.rtol, AbsoluteTolerance=wl.atol,
+                         MinimalTimestep=wl.dt_min, nvector=group, precision=precision,
+                         raise_on_failure=False)
+    gpu_lib.InitOdevec(ode)
+    ws_g = gpu_lib.Workspace(ode, wl.ncells)
+    ws_o = oracle.workspace(wl.network, wl.ncells, group)
+    y_g = torch.tensor(wl.y, device="cuda")
+    t_g = torch.tensor(wl.t0, device="cuda")
+    d_g = torch.tensor(wl.dt0, device="cuda")
+    y_o, t_o, d_o = wl.y.copy(), wl.t0.copy(), wl.dt0.copy()
+    try:
+        for k in range(nsteps):
+            ts = wl.t_stop * (k + 1) / nsteps
+            t_g, d_g = gpu_lib.SolveODE(ode, t_g, d_g, torch.tensor(ts, device="cuda"), y_g,
+                                        workspace=ws_g, resume=k > 0)
+            torch.cuda.synchronize()
+            g = (y_g.cpu().numpy(), t_g.cpu().numpy(), d_g.cpu().numpy(), ode.status.cpu().numpy(),
+                 ode.stats.cpu().numpy())
+            o = oracle.solve(wl.network, y_o, t_o, d_o, ts, wl.rtol, wl.atol, wl.dt_min, group=group,
+                             ws=ws_o, resume=k > 0)
+            assert np.all(o[3] == 0)
+            assert_bitwise(g, o, "resident step %d" % k)
+            y_o, t_o, d_o = o[0], o[1], o[2]
+    finally:
+        gpu_lib.CloseOdevec(ode)
+    return k
+
+
+def test_resident_continuation_matches_oracle(gpu_lib, oracle):
+    wl = W.primordial(ncells=512)
+    _resident_steps(gpu_lib, oracle, wl, "fp64", 5, 1)
+    wl = W.rober(ncells=128)
+    _resident_steps(gpu_lib, oracle, wl, "fp64", 4, 32)
+
+
+def test_resident_fresh_start_equals_solve(gpu_lib):
+    # resume = 0 is SolveODE exactly (it only saves the state as well)
+    import torch
+    wl = W.primordial(ncells=1024)
+    a = run_gpu(gpu_lib, wl, "fp32_lu")
+    ode = gpu_lib.Odevec(wl.network, RelativeTolerance=wl.rtol, AbsoluteTolerance=wl.atol,
+                         MinimalTimestep=wl.dt_min, nvector=1, precision="fp32_lu", raise_on_failure=False)
+    gpu_lib.InitOdevec(ode)
+    y = torch.tensor(wl.y, device="cuda")
+    t, dt = gpu_lib.SolveODE(ode, torch.tensor(wl.t0, device="cuda"), torch.tensor(wl.dt0, device="cuda"),
+                             torch.tensor(wl.t_stop, device="cuda"), y,
+                             workspace=gpu_lib.Workspace(ode, wl.ncells))
+    b = (y.cpu().numpy(), t.cpu().numpy(), dt.cpu().numpy(), ode.status.cpu().numpy(), ode.stats.cpu().numpy())
+    gpu_lib.CloseOdevec(ode)
+    assert_bitwise(b, a, "resident fresh start")
+
+
+def test_fp32_escalation_rescues_badly_conditioned_cells(gpu_lib):
+    # ROBER advanced in hydro steps to ~1e7 s: late-time iteration matrices
+    # have condition numbers ~1e14 and an FP32 factorisation can make Newton
+    # fail until dt < dt_min.  With escalation every cell finishes, and the
+    # rescued cells equal an FP64 solve of the same steps.
+    import torch
+    wl = W.rober(ncells=51417, seed=1008)
+    res = {}
+    for prec, esc in (("fp32_lu", False), ("fp32_lu", True), ("fp64_fma", True)):
+        ode = gpu_lib.Odevec(wl.network, RelativeTolerance=wl.rtol, AbsoluteTolerance=wl.atol,
+                             MinimalTimestep=wl.dt_min, nvector=1, precision=prec, raise_on_failure=False,
+                             escalation=esc)
+        gpu_lib.InitOdevec(ode)
+        y = torch.tensor(wl.y, device="cuda")
+        t = torch.zeros(wl.ncells, dtype=torch.float64, device="cuda")
+        dt = torch.full((wl.ncells,), 1e-10, dtype=torch.float64, device="cuda")
+        ws = gpu_lib.Workspace(ode, wl.ncells)
+        fails = 0
+        for k in range(10):
+            ts = torch.full((wl.ncells,), 1013907.692225179 * (k + 1), dtype=torch.float64, device="cuda")
+            gpu_lib.SolveODE(ode, t, dt, ts, y, workspace=ws, resume=k > 0)
+            fails += int((ode.status != 0).sum().item())
+        res[(prec, esc)] = (fails, y.cpu().numpy())
+        gpu_lib.CloseOdevec(ode)
+    assert res[("fp32_lu", True)][0] == 0
+    assert res[("fp64_fma", True)][0] == 0

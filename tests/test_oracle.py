@@ -154,3 +154,22 @@ def test_syn64_mass_conservation(oracle):
     assert np.all(st == 0) and np.all(t == 1e10)
     m = syn64.masses()
     assert np.max(np.abs(m @ y - m @ wl.y) / (m @ wl.y)) < 1e-12
+
+
+def test_resident_continuation(oracle):
+    # continuation across calls: later calls start from the saved history
+    # (far fewer steps than a fresh start) and stay within tolerance of one
+    # uninterrupted solve
+    wl = W.primordial(ncells=16)
+    ws = oracle.workspace(wl.network, wl.ncells)
+    y, t, dt = wl.y, wl.t0, wl.dt0
+    steps = []
+    for k in range(1, 5):
+        y, t, dt, st, stats = oracle.solve(wl.network, y, t, dt, wl.t_stop * k / 4, wl.rtol, wl.atol,
+                                           wl.dt_min, ws=ws, resume=k > 1)
+        assert np.all(st == 0) and np.array_equal(t, wl.t_stop * k / 4)
+        steps.append(stats[:, 0].sum())
+    one, *_ = oracle.solve(wl.network, wl.y, wl.t0, wl.dt0, wl.t_stop, wl.rtol, wl.atol, wl.dt_min)
+    rel = np.abs(y[:12] - one[:12]) / np.abs(one[:12])
+    assert np.max(rel[np.abs(one[:12]) > 1e-14]) < 1e-3
+    assert steps[1] < steps[0]
