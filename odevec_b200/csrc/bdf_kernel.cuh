@@ -156,11 +156,16 @@ struct LaneHist {
    budget; SHM places the Nordsieck history and the LU in shared memory. */
 template <int STAGE>
 struct StageCfg;
-template <> struct StageCfg<1> { static constexpr bool SHM = false; static constexpr int BS = 128, MINB = 2; };
-template <> struct StageCfg<2> { static constexpr bool SHM = true;  static constexpr int BS = 128, MINB = 1; };
-template <> struct StageCfg<3> { static constexpr bool SHM = false; static constexpr int BS = 128, MINB = 3; };
-template <> struct StageCfg<4> { static constexpr bool SHM = false; static constexpr int BS = 128, MINB = 4; };
-template <> struct StageCfg<5> { static constexpr bool SHM = true;  static constexpr int BS = 192, MINB = 1; };
+template <> struct StageCfg<1> { static constexpr bool SHM = false, SYNC = false; static constexpr int BS = 128, MINB = 2; };
+template <> struct StageCfg<2> { static constexpr bool SHM = true,  SYNC = false; static constexpr int BS = 128, MINB = 1; };
+template <> struct StageCfg<3> { static constexpr bool SHM = false, SYNC = false; static constexpr int BS = 128, MINB = 3; };
+template <> struct StageCfg<4> { static constexpr bool SHM = false, SYNC = false; static constexpr int BS = 128, MINB = 4; };
+template <> struct StageCfg<5> { static constexpr bool SHM = true,  SYNC = false; static constexpr int BS = 192, MINB = 1; };
+/* one block of 12 warps per SM that moves in step: a barrier opens every
+   trip of the cell loop and the Jacobian and step-size blocks are decided
+   for the whole block, so the warps on a scheduler run the same code at the
+   same time (instruction-cache reuse) */
+template <> struct StageCfg<6> { static constexpr bool SHM = false, SYNC = true;  static constexpr int BS = 384, MINB = 1; };
 
 template <class Net, class LUT, bool SHM, int BS>
 struct Staging;
@@ -449,11 +454,7 @@ struct Cell {
     /* GetJac + LUDecompose (src/odevec.F90:301-315) */
     __device__ __forceinline__ void jacobian_lu()
     {
-        double k[NR];
-        Net::rates_k(y, rT, k);
-        if constexpr (!SCALED) {
-            Net::template jac<LUT>(y, k, lcoef(q, 0), h, a);
-        } else {
+        if constexpr (SCALED) {
             /* scale by powers of two close to the error weights (exact in
                FP64), then round to FP32 */
 #pragma unroll
@@ -464,9 +465,84 @@ struct Cell {
                 sc[j] = ov_pow2i(hexp);
                 isc[j] = ov_pow2i(-hexp);
             }
-            Net::template jac_scaled<LUT>(y, k, lcoef(q, 0), h, a, sc, isc);
         }
+        if constexpr (Net::LU_METHOD == 3) {
+            fd_jacobian();
+        } else {
+            double k[NR];
+            Net::rates_k(y, rT, k);
+            if constexpr (!SCALED)
+                Net::template jac<LUT>(y, k, lcoef(q, 0), h, a);
+            else
+                Net::template jac_scaled<LUT>(y, k, lcoef(q, 0), h, a, sc, isc);
+        }
+        /* empty for LUmethod 2: jac() wrote the symbolic factors */
         Net::template lu_factor<LUT>(a);
+    }
+
+    /* CalcJac_dense (src/odevec.F90:469-506), the DRPEPJ difference
+       quotients: P(:,k) = -(dt*beta/r) * (f(y + r e_k) - f(y)), then 1 is
+       added on the diagonal.  Only the solver-state columns are formed:
+       the rows and columns of frozen species are those of the identity
+       whatever their off-diagonal values, so they never reach a solution.
+       Every array index is a compile-time constant (the perturbed column
+       is selected, not indexed), so the state stays in registers. */
+    __device__ __forceinline__ void fd_jacobian()
+    {
+        const double uround = 2.2204460492503131e-16;  /* 2^-52 */
+        const double srur = 1.4901161193847656e-08;    /* 2^-26 */
+        const double beta = lcoef(q, 0);
+        double k[NR], f0[N];
+        Net::rates_k(y, rT, k);
+        Net::rhs(y, k, f0);
+        double e[ND];
+#pragma unroll
+        for (int j = 0; j < ND; ++j)
+            e[j] = f0[Net::dyn(j)];
+        const double fac = wnorm(e);
+        double r0 = 1e3 * fabs(h) * uround * (double)N * fac;
+        if (r0 == 0.0)
+            r0 = 1.0;
+#pragma unroll 1
+        for (int col = 0; col < ND; ++col) {
+            double yy[N];
+            double yk = 0.0, wk = 0.0;
+#pragma unroll
+            for (int j = 0; j < N; ++j)
+                yy[j] = y[j];
+#pragma unroll
+            for (int j = 0; j < ND; ++j) {
+                if (j == col) {
+                    yk = y[Net::dyn(j)];
+                    wk = w2[j];
+                }
+            }
+            const double a1 = srur * fabs(yk), a2 = r0 / sqrt(wk);
+            const double r = a1 >= a2 ? a1 : a2;
+            const double fk = -(h * beta / r);
+#pragma unroll
+            for (int j = 0; j < ND; ++j)
+                if (j == col)
+                    yy[Net::dyn(j)] = yk + r;
+            double k1[NR], f1[N];
+            Net::rates_k(yy, rT, k1);
+            Net::rhs(yy, k1, f1);
+#pragma unroll
+            for (int c = 0; c < ND; ++c) {
+                if (c == col) {
+#pragma unroll
+                    for (int i = 0; i < ND; ++i) {
+                        double v = (f1[Net::dyn(i)] - f0[Net::dyn(i)]) * fk;
+                        if (i == c)
+                            v = 1.0 + v;
+                        if constexpr (SCALED)
+                            a[Net::pidx(i, c)] = (LUT)(v * sc[i] * isc[c]);
+                        else
+                            a[Net::pidx(i, c)] = v;
+                    }
+                }
+            }
+        }
     }
 
     /* residual, solve, Newton update (src/odevec.F90:323-352) */
@@ -647,8 +723,14 @@ __global__ void __launch_bounds__(StageCfg<STAGE>::BS, StageCfg<STAGE>::MINB) bd
                     ph = cell < ncells ? PH_START : PH_EXHAUSTED;
                 }
             }
-            if (__all_sync(FULL, ph == PH_EXHAUSTED))
-                break;
+            if constexpr (StageCfg<STAGE>::SYNC) {
+                /* every thread of the block reaches this barrier once per trip */
+                if (__syncthreads_and(ph == PH_EXHAUSTED))
+                    break;
+            } else {
+                if (__all_sync(FULL, ph == PH_EXHAUSTED))
+                    break;
+            }
         } else {
             if (ph == PH_IDLE) { /* warp-uniform */
                 unsigned long long g = 0;
@@ -778,10 +860,19 @@ __global__ void __launch_bounds__(StageCfg<STAGE>::BS, StageCfg<STAGE>::MINB) bd
         {
             bool run;
             if (G == 1) {
-                const int waiting = warp_count(ph == PH_JACWAIT);
-                const int moving = warp_count(ph == PH_NEWTON || ph == PH_START || ph == PH_RESTART);
-                const bool aged = __any_sync(FULL, ph == PH_JACWAIT && c.wait >= A.max_wait);
-                run = waiting > 0 && (waiting >= A.jac_batch || moving == 0 || aged);
+                const bool mv = ph == PH_NEWTON || ph == PH_START || ph == PH_RESTART;
+                const bool old = ph == PH_JACWAIT && c.wait >= A.max_wait;
+                if constexpr (StageCfg<STAGE>::SYNC) {
+                    const int waiting = __syncthreads_count(ph == PH_JACWAIT);
+                    const int moving = __syncthreads_count(mv);
+                    const bool aged = __syncthreads_or(old);
+                    run = waiting > 0 && (waiting >= A.jac_batch * (BS / 32) || moving == 0 || aged);
+                } else {
+                    const int waiting = warp_count(ph == PH_JACWAIT);
+                    const int moving = warp_count(mv);
+                    const bool aged = __any_sync(FULL, old);
+                    run = waiting > 0 && (waiting >= A.jac_batch || moving == 0 || aged);
+                }
             } else {
                 run = ph == PH_JACWAIT;
             }
@@ -909,10 +1000,19 @@ __global__ void __launch_bounds__(StageCfg<STAGE>::BS, StageCfg<STAGE>::MINB) bd
         {
             bool run;
             if (G == 1) {
-                const int waiting = warp_count(ph == PH_SSWAIT);
-                const int moving = warp_count(ph == PH_PRED || ph == PH_NEWTON || ph == PH_RESTART);
-                const bool aged = __any_sync(FULL, ph == PH_SSWAIT && c.wait >= A.max_wait);
-                run = waiting > 0 && (waiting >= A.ss_batch || moving == 0 || aged);
+                const bool mv = ph == PH_PRED || ph == PH_NEWTON || ph == PH_RESTART;
+                const bool old = ph == PH_SSWAIT && c.wait >= A.max_wait;
+                if constexpr (StageCfg<STAGE>::SYNC) {
+                    const int waiting = __syncthreads_count(ph == PH_SSWAIT);
+                    const int moving = __syncthreads_count(mv);
+                    const bool aged = __syncthreads_or(old);
+                    run = waiting > 0 && (waiting >= A.ss_batch * (BS / 32) || moving == 0 || aged);
+                } else {
+                    const int waiting = warp_count(ph == PH_SSWAIT);
+                    const int moving = warp_count(mv);
+                    const bool aged = __any_sync(FULL, old);
+                    run = waiting > 0 && (waiting >= A.ss_batch || moving == 0 || aged);
+                }
             } else {
                 run = ph == PH_SSWAIT;
             }
@@ -972,7 +1072,7 @@ cudaError_t launch(const LaunchArgs& a, int block, int grid, cudaStream_t stream
     using Cfg = StageCfg<STAGE>;
     auto kern = bdf_kernel<Net, G, LUT, STAGE>;
     constexpr size_t smem = Staging<Net, LUT, Cfg::SHM, Cfg::BS>::smem_bytes;
-    if (Cfg::SHM || block <= 0 || block > Cfg::BS)
+    if (Cfg::SHM || Cfg::SYNC || block <= 0 || block > Cfg::BS)
         block = Cfg::BS;
     static int cached_grid[2] = {0, 0};
     if (cached_grid[0] == 0 || cached_grid[1] != block) {
@@ -1032,6 +1132,7 @@ constexpr bool shm_fits()
             OV_STAGE_CASE(NET, double, 1)                                                        \
             OV_STAGE_CASE(NET, double, 3)                                                        \
             OV_STAGE_CASE(NET, double, 4)                                                        \
+            OV_STAGE_CASE(NET, double, 6)                                                        \
             if constexpr (shm_fits<NET, double, 128>()) {                                        \
                 OV_STAGE_CASE(NET, double, 2)                                                    \
             }                                                                                    \
@@ -1042,6 +1143,7 @@ constexpr bool shm_fits()
                 OV_STAGE_CASE(NET, float, 1)                                                     \
                 OV_STAGE_CASE(NET, float, 3)                                                     \
                 OV_STAGE_CASE(NET, float, 4)                                                     \
+                OV_STAGE_CASE(NET, float, 6)                                                     \
                 if constexpr (shm_fits<NET, float, 128>()) {                                     \
                     OV_STAGE_CASE(NET, float, 2)                                                 \
                 }                                                                                \

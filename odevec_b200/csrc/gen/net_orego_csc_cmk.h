@@ -14,7 +14,7 @@
 #define OV_OREGO_CSC_CMK_NVECTOR 1
 #define OV_OREGO_CSC_CMK_DT_MIN 1e-10
 #define OV_OREGO_CSC_CMK_IDX_TGAS -1
-static const int ov_orego_csc_cmk_sizes[6] = {3, 7, 0, 0, -1, 3};
+static const int ov_orego_csc_cmk_sizes[7] = {3, 7, 0, 0, -1, 3, 1};
 static const double ov_orego_csc_cmk_defaults[2] = {1.0, 1e-10}; /* nvector, dt_min */
 static const int ov_orego_csc_cmk_perm[3] = {2, 1, 0};
 static const int ov_orego_csc_cmk_row_index[7] = {0, 1, 1, 2, 0, 1, 2};
@@ -31,7 +31,7 @@ OV_HD static OV_INLINE void ov_orego_csc_cmk_rhs(const double* OV_RESTRICT y, co
 
 OV_HD static OV_INLINE void ov_orego_csc_cmk_jac(const double* OV_RESTRICT y, const double* OV_RESTRICT k, double beta, double dt, double* OV_RESTRICT a)
 {
-  (void)y; (void)k; (void)beta; (void)dt;
+  (void)y; (void)k; (void)beta; (void)dt; (void)a;
   a[0] = 0.161*beta*dt + 1.0;  /* (0,0) */
   a[1] = -0.0129416332341141*beta*dt;  /* (1,0) */
   a[2] = -beta*dt*(-0.0129416332341141*y[0] - 0.0129416332341141) + 1.0;  /* (1,1) */

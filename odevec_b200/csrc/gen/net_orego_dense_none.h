@@ -14,7 +14,7 @@
 #define OV_OREGO_DENSE_NONE_NVECTOR 1
 #define OV_OREGO_DENSE_NONE_DT_MIN 1e-10
 #define OV_OREGO_DENSE_NONE_IDX_TGAS -1
-static const int ov_orego_dense_none_sizes[6] = {3, 8, 0, 1, -1, 3};
+static const int ov_orego_dense_none_sizes[7] = {3, 8, 0, 1, -1, 3, 1};
 static const double ov_orego_dense_none_defaults[2] = {1.0, 1e-10}; /* nvector, dt_min */
 static const int ov_orego_dense_none_perm[3] = {0, 1, 2};
 static const int ov_orego_dense_none_row_index[8] = {0, 1, 2, 0, 1, 2, 1, 2};
@@ -31,7 +31,7 @@ OV_HD static OV_INLINE void ov_orego_dense_none_rhs(const double* OV_RESTRICT y,
 
 OV_HD static OV_INLINE void ov_orego_dense_none_jac(const double* OV_RESTRICT y, const double* OV_RESTRICT k, double beta, double dt, double* OV_RESTRICT a)
 {
-  (void)y; (void)k; (void)beta; (void)dt;
+  (void)y; (void)k; (void)beta; (void)dt; (void)a;
   a[0] = -beta*dt*(-0.0012942725*y[0] - 77.27*y[1] + 77.27) + 1.0;  /* (0,0) */
   a[1] = 0.0129416332341141*beta*dt*y[1];  /* (1,0) */
   a[2] = -0.161*beta*dt;  /* (2,0) */

@@ -11,6 +11,8 @@ struct ov_net_rober_dense_none {
   static constexpr int NREA = 0;
   static constexpr int IDX_TGAS = -1;
   static constexpr bool DENSE = true;
+  /* 1: symbolic Jacobian + numeric LU, 2: symbolic LU, 3: difference quotients */
+  static constexpr int LU_METHOD = 1;
   static constexpr const char* TAG = "ROBER_DENSE_NONE";
   /* dynamic species (solver state index -> species) and frozen ones */
   OV_HD static constexpr int dyn(int i) { return i == 0 ? 0 : (i == 1 ? 1 : (2)); }
@@ -21,7 +23,7 @@ struct ov_net_rober_dense_none {
   static OV_INLINE __device__ void rates_T(const double*, double*) {}
   /* P = I - dt*beta*J on the dynamic block, packed CSC order */
   template <class T, class A> OV_HD static OV_INLINE void jac(const double* OV_RESTRICT y, const double* OV_RESTRICT k, double beta, double dt, A a) {
-    (void)y; (void)k; (void)beta; (void)dt;
+    (void)y; (void)k; (void)beta; (void)dt; (void)a;
     a[0] = (T)(0.04*beta*dt + 1.0);
     a[1] = (T)(-0.04*beta*dt);
     a[2] = (T)(-10000.0*beta*dt*y[2]);
@@ -45,7 +47,7 @@ struct ov_net_rober_dense_none {
   /* the same, each entry evaluated in FP64, scaled by powers of two and
      rounded to T on the fly */
   template <class T, class A> OV_HD static OV_INLINE void jac_scaled(const double* OV_RESTRICT y, const double* OV_RESTRICT k, double beta, double dt, A a, const double* OV_RESTRICT sc, const double* OV_RESTRICT isc) {
-    (void)y; (void)k; (void)beta; (void)dt;
+    (void)y; (void)k; (void)beta; (void)dt; (void)a; (void)sc; (void)isc;
     a[0] = (T)((0.04*beta*dt + 1.0)*sc[0]*isc[0]);
     a[1] = (T)((-0.04*beta*dt)*sc[1]*isc[0]);
     a[2] = (T)((-10000.0*beta*dt*y[2])*sc[0]*isc[1]);
@@ -58,6 +60,7 @@ struct ov_net_rober_dense_none {
   /* in-place numeric LU of the packed dynamic block a[0..NNZ-1]; A is a
      pointer or an accessor whose operator[] yields T& */
   template <class T, class A> OV_HD static OV_INLINE void lu_factor(A a) {
+    (void)a;
     a[1] = a[1] / a[0];
     a[3] = a[3] - a[1]*a[2];
     a[6] = a[6] - a[1]*a[5];

@@ -14,7 +14,7 @@
 #define OV_ROBER_DENSE_NONE_NVECTOR 32
 #define OV_ROBER_DENSE_NONE_DT_MIN 1e-20
 #define OV_ROBER_DENSE_NONE_IDX_TGAS -1
-static const int ov_rober_dense_none_sizes[6] = {3, 8, 0, 1, -1, 3};
+static const int ov_rober_dense_none_sizes[7] = {3, 8, 0, 1, -1, 3, 1};
 static const double ov_rober_dense_none_defaults[2] = {32.0, 1e-20}; /* nvector, dt_min */
 static const int ov_rober_dense_none_perm[3] = {0, 1, 2};
 static const int ov_rober_dense_none_row_index[8] = {0, 1, 0, 1, 2, 0, 1, 2};
@@ -31,7 +31,7 @@ OV_HD static OV_INLINE void ov_rober_dense_none_rhs(const double* OV_RESTRICT y,
 
 OV_HD static OV_INLINE void ov_rober_dense_none_jac(const double* OV_RESTRICT y, const double* OV_RESTRICT k, double beta, double dt, double* OV_RESTRICT a)
 {
-  (void)y; (void)k; (void)beta; (void)dt;
+  (void)y; (void)k; (void)beta; (void)dt; (void)a;
   a[0] = 0.04*beta*dt + 1.0;  /* (0,0) */
   a[1] = -0.04*beta*dt;  /* (1,0) */
   a[2] = -10000.0*beta*dt*y[2];  /* (0,1) */

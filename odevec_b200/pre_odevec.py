@@ -143,6 +143,7 @@ class System:
     nvector: int = 1
     dt_min: float = 1e-10
     lu_method: int = 1
+    lu_exprs: Optional[sp.Matrix] = None   # LUmethod 2: symbolic L\U of P_order
 
     @property
     def neq(self) -> int:
@@ -169,9 +170,20 @@ def build_system(net: networks.Network, ordering: str = "None", packaging: str =
         raise SystemExit("# Error: %s packaging is not supported" % packaging)  # pre_odevec.py:515-518
     if packaging not in ("DENSE", "CSC"):
         raise SystemExit("# Error: This format is not known.")
-    if lu_method not in (1,):
-        raise SystemExit("# Error: --LUmethod=%d is not supported by the CUDA emitter "
-                         "(1 = symbolic Jacobian + numeric LU)" % lu_method)
+    if lu_method not in (1, 2, 3):
+        raise SystemExit("# Error: --LUmethod=%d is not known (1: symbolic Jacobian + numeric LU, "
+                         "2: symbolic LU, 3: finite-difference Jacobian + numeric LU)" % lu_method)
+    if lu_method == 2 and packaging != "DENSE":
+        # the symbolic factors are Doolittle's (unit L); the reference's sparse
+        # solve (src/odevec.F90:853-891) expects Crout factors (unit U)
+        raise SystemExit("# Error: --LUmethod=2 needs --packaging=DENSE")
+    if lu_method == 3 and packaging != "DENSE":
+        # src/odevec.F90:509-523: CalcJac_sparse aborts
+        raise SystemExit("The Method Flags LUmethod=3 is not supported with sparse matrices, yet. Aborting...")
+    if lu_method == 3 and ordering not in (None, "None", "NONE", ""):
+        # CalcJac_dense (src/odevec.F90:469-506) fills P in species order, while
+        # the solve applies the permutation to the residual
+        raise SystemExit("# Error: --LUmethod=3 needs --ordering=None")
     n = net.neq
     jac = net.rhs.jacobian(net.y)
     dt, beta = sp.symbols("dt beta")
@@ -189,7 +201,31 @@ def build_system(net: networks.Network, ordering: str = "None", packaging: str =
         for j in range(n):
             P_order[i, j] = P[perm[i], perm[j]]
     pat = _pattern_of(sp.SparseMatrix(P_order))
-    if lu_pattern == "symbolic" and packaging == "CSC":
+    lu_exprs = None
+    if lu_method == 3:
+        # the difference quotients fill every entry: the rate coefficients of
+        # a network may depend on the whole state (PRIMORDIAL's floor on
+        # max_j y_j), so a perturbation of one species moves every right-hand
+        # side.  Frozen species keep identity rows and columns: their entries
+        # never reach a solution (the kernel leaves them out).
+        lu = np.ones((n, n), dtype=bool)
+        for f in _frozen_of(net):
+            lu[f, :] = False
+            lu[:, f] = False
+            lu[f, f] = True
+        pat = lu.copy()
+    elif lu_method == 2:
+        # the reference's symbolic factorisation (pre_odevec.py:493); its row
+        # permutation is dropped there, so a pivot is an error here
+        lu_exprs, piv = sp.Matrix(P_order).LUdecomposition_Simple()
+        if piv:
+            raise SystemExit("# Error: the symbolic LU of P needs row exchanges %s; use --LUmethod=1" % (piv,))
+        lu = structural_lu_pattern(pat | np.eye(n, dtype=bool))
+        for i in range(n):
+            for j in range(n):
+                if lu_exprs[i, j] != 0 and not lu[i, j]:
+                    raise SystemExit("# Error: symbolic LU entry (%d,%d) outside the fill pattern" % (i, j))
+    elif lu_pattern == "symbolic" and packaging == "CSC":
         # the dense factorisation touches every structurally non-zero entry,
         # so DENSE always uses the structural pattern
         lu = symbolic_lu_pattern(P_order)
@@ -210,8 +246,10 @@ def build_system(net: networks.Network, ordering: str = "None", packaging: str =
     u_col_start.append(len(row_index))
     if tag is None:
         tag = "%s_%s_%s" % (net.name, packaging, ordering.upper())
+        if lu_method != 1:
+            tag += "_LU%d" % lu_method
     return System(net, tag, packaging, ordering, perm, sp.Matrix(P), P_order, lu,
-                  row_index, u_col_start, l_col_start, int(pat.sum()), nvector, dt_min, lu_method)
+                  row_index, u_col_start, l_col_start, int(pat.sum()), nvector, dt_min, lu_method, lu_exprs)
 
 
 # ------------------------------------------------------------------ printer
@@ -318,8 +356,14 @@ def emit_c_header(sysm: System) -> str:
     L.append(" * network %s, packaging %s, ordering %s, neq %d, LU nnz %d (P nnz %d)."
              % (net.name, sysm.packaging, sysm.ordering, n, nnz, sysm.p_nnz))
     L.append(" * rhs(): f = dy/dt in species order (rate array k as in the reference).")
-    L.append(" * jac(): P = I - dt*beta*J at the LU pattern positions, CSC storage order")
-    L.append(" *        of the permuted matrix; fill-in positions are 0.  */")
+    if sysm.lu_method == 1:
+        L.append(" * jac(): P = I - dt*beta*J at the LU pattern positions, CSC storage order")
+        L.append(" *        of the permuted matrix; fill-in positions are 0.  */")
+    elif sysm.lu_method == 2:
+        L.append(" * jac(): LUmethod 2, the symbolic factors L\\U of P (unit L) at the")
+        L.append(" *        pattern positions, CSC storage order; no numeric factorisation.  */")
+    else:
+        L.append(" * jac(): LUmethod 3, empty: P comes from difference quotients of rhs().  */")
     L.append("#ifndef %s" % g)
     L.append("#define %s" % g)
     L.append('#include "../ov_common.h"')
@@ -338,7 +382,8 @@ def emit_c_header(sysm: System) -> str:
         L.append("static const int ov_%s_%s[%d] = {%s};" % (cid, name, len(vals),
                                                           ", ".join(str(v) for v in vals)))
     arr("sizes", [n, nnz, net.nrea if net.rates else 0, 1 if sysm.packaging == "DENSE" else 0,
-                  net.idx_tgas if net.idx_tgas is not None else -1, n - len(frozen_species(sysm))])
+                  net.idx_tgas if net.idx_tgas is not None else -1, n - len(frozen_species(sysm)),
+                  sysm.lu_method])
     L.append("static const double ov_%s_defaults[2] = {%d.0, %r}; /* nvector, dt_min */"
              % (cid, sysm.nvector, float(sysm.dt_min)))
     arr("perm", sysm.perm)
@@ -357,19 +402,28 @@ def emit_c_header(sysm: System) -> str:
     L.append("OV_HD static OV_INLINE void ov_%s_jac(const double* OV_RESTRICT y, "
              "const double* OV_RESTRICT k, double beta, double dt, double* OV_RESTRICT a)" % cid)
     L.append("{")
-    L.append("  (void)y; (void)k; (void)beta; (void)dt;")
+    L.append("  (void)y; (void)k; (void)beta; (void)dt; (void)a;")
+    src = _jac_source(sysm)
     for j in range(n):
         for kk in range(sysm.u_col_start[j], sysm.u_col_start[j + 1]):
             i = sysm.row_index[kk]
-            L.append("  a[%d] = %s;  /* (%d,%d) */" % (kk, _cexpr(sysm.P_order[i, j], pr), i, j))
+            if src is not None:
+                L.append("  a[%d] = %s;  /* (%d,%d) */" % (kk, _cexpr(src[i, j], pr), i, j))
     L.append("}")
     L.append("")
     L.append("#endif")
     return "\n".join(L) + "\n"
 
 
+def _jac_source(sysm: System):
+    """What jac() writes: P (LUmethod 1), its symbolic factors (2), nothing (3)."""
+    return {1: sysm.P_order, 2: sysm.lu_exprs, 3: None}[sysm.lu_method]
+
+
 def _lu_factor_lines(sysm: System) -> List[str]:
     """Straight-line numeric LU in the reference's operation order."""
+    if sysm.lu_method == 2:
+        return []
     n = sysm.neq
     pos = sysm.pos()
     out = []
@@ -454,7 +508,10 @@ def frozen_species(sysm: System) -> List[int]:
     right-hand side depends on.  Their Newton corrections are exact zeros,
     their state never changes and their rows and columns of P are those of
     the identity, so the CUDA kernel keeps them out of the solver state."""
-    net = sysm.net
+    return _frozen_of(sysm.net)
+
+
+def _frozen_of(net: networks.Network) -> List[int]:
     n = net.neq
     J = net.rhs.jacobian(net.y)
     out = []
@@ -509,6 +566,14 @@ def emit_cuda_header(sysm: System) -> str:
     L.append("  static constexpr int NREA = %d;" % (net.nrea if net.rates else 0))
     L.append("  static constexpr int IDX_TGAS = %d;" % (net.idx_tgas if net.idx_tgas is not None else -1))
     L.append("  static constexpr bool DENSE = %s;" % ("true" if sysm.packaging == "DENSE" else "false"))
+    L.append("  /* 1: symbolic Jacobian + numeric LU, 2: symbolic LU, 3: difference quotients */")
+    L.append("  static constexpr int LU_METHOD = %d;" % sysm.lu_method)
+    if sysm.lu_method == 3:
+        # full pattern, species order: packed index of solver-state entry (i, j)
+        for (i, j), kk in pos.items():
+            if kk in kmap:
+                assert kmap[kk] == dpos[j] * nd + dpos[i]
+        L.append("  OV_HD static constexpr int pidx(int i, int j) { return j * ND + i; }")
     L.append('  static constexpr const char* TAG = "%s";' % sysm.tag)
     L.append("  /* dynamic species (solver state index -> species) and frozen ones */")
     L.append("  OV_HD static constexpr int dyn(int i) { return %s; }"
@@ -527,12 +592,13 @@ def emit_cuda_header(sysm: System) -> str:
         L.append("  static OV_INLINE __device__ void rates_k(const double*, const double*, double*) {}")
         L.append("  static OV_INLINE __device__ void rates_T(const double*, double*) {}")
     L.append("  /* P = I - dt*beta*J on the dynamic block, packed CSC order */")
+    src = _jac_source(sysm)
     L.append("  template <class T, class A> OV_HD static OV_INLINE void jac(const double* OV_RESTRICT y, "
              "const double* OV_RESTRICT k, double beta, double dt, A a) {")
-    L.append("    (void)y; (void)k; (void)beta; (void)dt;")
+    L.append("    (void)y; (void)k; (void)beta; (void)dt; (void)a;")
     for (i, j), kk in sorted(pos.items(), key=lambda t: t[1]):
-        if kk in kmap:
-            L.append("    a[%d] = (T)(%s);" % (kmap[kk], _cexpr(sysm.P_order[i, j], pr)))
+        if kk in kmap and src is not None:
+            L.append("    a[%d] = (T)(%s);" % (kmap[kk], _cexpr(src[i, j], pr)))
     L.append("  }")
     L.append("  /* a = D P D^-1 rounded to T, D = diag(sc) over solver-state indices */")
     L.append("  template <class T, class A> OV_HD static OV_INLINE void store_scaled(const double* OV_RESTRICT P, "
@@ -547,15 +613,16 @@ def emit_cuda_header(sysm: System) -> str:
     L.append("  template <class T, class A> OV_HD static OV_INLINE void jac_scaled(const double* OV_RESTRICT y, "
              "const double* OV_RESTRICT k, double beta, double dt, A a, "
              "const double* OV_RESTRICT sc, const double* OV_RESTRICT isc) {")
-    L.append("    (void)y; (void)k; (void)beta; (void)dt;")
+    L.append("    (void)y; (void)k; (void)beta; (void)dt; (void)a; (void)sc; (void)isc;")
     for (i, j), kk in sorted(pos.items(), key=lambda t: t[1]):
-        if kk in kmap:
-            L.append("    a[%d] = (T)((%s)*sc[%d]*isc[%d]);" % (kmap[kk], _cexpr(sysm.P_order[i, j], pr),
+        if kk in kmap and src is not None:
+            L.append("    a[%d] = (T)((%s)*sc[%d]*isc[%d]);" % (kmap[kk], _cexpr(src[i, j], pr),
                                                              dpos[sysm.perm[i]], dpos[sysm.perm[j]]))
     L.append("  }")
     L.append("  /* in-place numeric LU of the packed dynamic block a[0..NNZ-1]; A is a")
     L.append("     pointer or an accessor whose operator[] yields T& */")
     L.append("  template <class T, class A> OV_HD static OV_INLINE void lu_factor(A a) {")
+    L.append("    (void)a;")
     for ln in _lu_factor_lines(sysm):
         L.append("    " + _remap_a(ln, kmap))
     L.append("  }")
@@ -606,11 +673,18 @@ def flop_counts(sysm: System) -> Dict[str, int]:
     """Static per-call FLOPs of the emitted routines."""
     f_rhs = sum(expr_flops(e) for e in sysm.net.rhs)
     pos = sysm.pos()
-    f_jac = sum(expr_flops(sysm.P_order[i, j]) for (i, j) in pos)
+    f_k = (4 + sysm.net.nrea) if sysm.net.rates else 0
+    src = _jac_source(sysm)
+    if src is not None:
+        f_jac = sum(expr_flops(src[i, j]) for (i, j) in pos)
+    else:
+        # difference quotients: ND + 1 right-hand sides, the norm of f, and per
+        # column the increment (6) and ND differences times the factor
+        nd = sysm.neq - len(frozen_species(sysm))
+        f_jac = (nd + 1) * (f_rhs + f_k) + 3 * nd + 4 + nd * (6 + 2 * nd) + nd
     f_lu = sum(_line_flops(l) for l in _lu_factor_lines(sysm))
     f_solve = sum(_line_flops(l) for l in _lu_solve_lines(sysm) if not l.startswith(("T d", "x[")))
     # rates_k of the PRIMORDIAL rate model: 3 mul + 1 div for the floor, one add per rate
-    f_k = (4 + sysm.net.nrea) if sysm.net.rates else 0
     return {"neq": sysm.neq, "nnz": sysm.nnz, "rhs": f_rhs, "jac": f_jac, "lu_factor": f_lu,
             "lu_solve": f_solve, "rates_k": f_k}
 
@@ -620,10 +694,11 @@ def write_variant(sysm: System, outdir: str = GEN_DIR) -> Tuple[str, str]:
     cid = _cid(sysm.tag)
     h = os.path.join(outdir, "net_%s.h" % cid)
     cu = os.path.join(outdir, "net_%s.cuh" % cid)
+    text_h, text_cu = emit_c_header(sysm), emit_cuda_header(sysm)
     with open(h, "w") as fh:
-        fh.write(emit_c_header(sysm))
+        fh.write(text_h)
     with open(cu, "w") as fh:
-        fh.write(emit_cuda_header(sysm))
+        fh.write(text_cu)
     import json
     fpath = os.path.join(outdir, "flops.json")
     table = json.load(open(fpath)) if os.path.exists(fpath) else {}
@@ -665,7 +740,9 @@ def parse_args(argv=None):
         description="Preprocessor for OdeVec on B200: emits straight-line C/CUDA network code.")
     p.add_argument("--example", default="PRIMORDIAL", help="ROBER | OREGO | PRIMORDIAL | KROME")
     p.add_argument("--krome_setupfile", default=None, help="python dump of a KROME network")
-    p.add_argument("--LUmethod", type=int, default=1, help="1: symbolic Jacobian + numeric LU")
+    p.add_argument("--LUmethod", type=int, default=1,
+                   help="1: symbolic Jacobian + numeric LU; 2: symbolic LU (DENSE); "
+                        "3: finite-difference Jacobian + numeric LU (DENSE, no ordering)")
     p.add_argument("--dt_min", default=1e-10, help="default minimal time step")
     p.add_argument("--nvector", type=int, required=True,
                    help="default lockstep group size (1 = per-cell control, 32 = one warp)")

@@ -4,8 +4,9 @@ Each entry is a preprocessor command line (the reference's flags).  The
 defaults follow the reference drivers: ROBER with nvector=32 lockstep and
 dt_min=1e-20 (``tests/rober.f90:44``), OREGO per cell with the default
 dt_min, PRIMORDIAL per cell with dt_min=1e-20 (``tests/primordial.f90:45``)
-in dense, FF- and CMK-ordered CSC packaging, and the synthetic 64-species
-network read from a KROME-format dump.
+in dense, FF- and CMK-ordered CSC packaging, the symbolic-LU and
+difference-quotient Jacobian methods on dense variants, and the synthetic
+64-species network read from a KROME-format dump.
 """
 import os
 
@@ -22,6 +23,12 @@ SHIPPED = [
     ["--example=PRIMORDIAL", "--packaging=DENSE", "--nvector=1", "--dt_min=1e-20"],
     ["--example=PRIMORDIAL", "--packaging=CSC", "--ordering=FF", "--nvector=1", "--dt_min=1e-20"],
     ["--example=PRIMORDIAL", "--packaging=CSC", "--ordering=CMK", "--nvector=1", "--dt_min=1e-20"],
+    # the reference's other two Jacobian methods: the symbolic LU (LUmethod 2,
+    # tractable for the small networks) and difference quotients (LUmethod 3)
+    ["--example=ROBER", "--packaging=DENSE", "--nvector=32", "--dt_min=1e-20", "--LUmethod=2"],
+    ["--example=OREGO", "--packaging=DENSE", "--nvector=1", "--LUmethod=2"],
+    ["--example=ROBER", "--packaging=DENSE", "--nvector=32", "--dt_min=1e-20", "--LUmethod=3"],
+    ["--example=PRIMORDIAL", "--packaging=DENSE", "--nvector=1", "--dt_min=1e-20", "--LUmethod=3"],
 ]
 
 

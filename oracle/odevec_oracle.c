@@ -46,12 +46,14 @@ typedef void (*jac_fn)(const double*, const double*, double, double, double*);
 typedef struct {
     const char* tag;
     int neq, nnz, nrea, dense, idx_tgas;
+    int lu_method; /* 1 GetJac + LUDecompose, 2 GetLU, 3 CalcJac + LUDecompose */
     const int *perm, *row_index, *u_col_start, *l_col_start;
     rhs_fn rhs;
     jac_fn jac;
 } net_desc;
 
-/* one entry per emitted variant; sizes[] = {neq, nnz, nrea, dense, idx_tgas} */
+/* one entry per emitted variant; sizes[] = {neq, nnz, nrea, dense, idx_tgas,
+   solver-state species, LUmethod} */
 typedef struct {
     const char* tag;
     const int *sizes, *perm, *row_index, *u_col_start, *l_col_start;
@@ -76,7 +78,8 @@ static const net_desc* net_find(const char* tag)
         for (int i = 0; i < NNETS; ++i) {
             const net_entry* e = &g_entries[i];
             net_desc d = {e->tag, e->sizes[0], e->sizes[1], e->sizes[2], e->sizes[3], e->sizes[4],
-                          e->perm, e->row_index, e->u_col_start, e->l_col_start, e->rhs, e->jac};
+                          e->sizes[6], e->perm, e->row_index, e->u_col_start, e->l_col_start, e->rhs,
+                          e->jac};
             g_nets[i] = d;
         }
         ready = 1;
@@ -181,6 +184,55 @@ static void get_jac(ode_t* o, double beta, const double* y, double dt)
         }
     }
     free(a);
+}
+
+static double wnorm(const ode_t* o, const double* e, const double* w2);
+
+/* CalcJac_dense (src/odevec.F90:469-506): P = I - dt*beta*J from the
+   DRPEPJ difference quotients, column by column, in the dense n x n layout
+   (LUmethod 3).  y is perturbed one species at a time and restored. */
+static void calc_jac_fd(ode_t* o, double beta, const double* y_in, double dt)
+{
+    const int G = o->G, n = o->neq;
+    const size_t N = (size_t)n * G;
+    const double uround = 2.2204460492503131E-016;
+    const double srur = 1.4901161193847656E-008;
+    double* y = (double*)malloc(sizeof(double) * N);
+    double* drhs = (double*)malloc(sizeof(double) * N);
+    double* r0 = (double*)malloc(sizeof(double) * G);
+    double* r = (double*)malloc(sizeof(double) * G);
+    double* fac = (double*)malloc(sizeof(double) * G);
+    double* ytmp = (double*)malloc(sizeof(double) * G);
+    memcpy(y, y_in, sizeof(double) * N);
+#define AD(row, c, i) o->LU[((size_t)(row) * n + (c)) * G + (i)]
+    get_rhs(o, y, o->rhs);
+    const double f = wnorm(o, o->rhs, o->w2); /* one value for the vector */
+    for (int i = 0; i < G; ++i) {
+        r0[i] = 1e3 * fabs(dt) * uround * (double)n * f;
+        if (r0[i] == 0.0)
+            r0[i] = 1.0;
+    }
+    for (int k = 0; k < n; ++k) {
+        for (int i = 0; i < G; ++i) {
+            ytmp[i] = y[(size_t)k * G + i];
+            const double a1 = srur * fabs(y[(size_t)k * G + i]);
+            const double a2 = r0[i] / sqrt(o->w2[(size_t)k * G + i]);
+            r[i] = a1 >= a2 ? a1 : a2;
+            y[(size_t)k * G + i] = y[(size_t)k * G + i] + r[i];
+            fac[i] = -(dt * beta / r[i]);
+        }
+        get_rhs(o, y, drhs);
+        for (int j = 0; j < n; ++j)
+            for (int i = 0; i < G; ++i)
+                AD(j, k, i) = (drhs[(size_t)j * G + i] - o->rhs[(size_t)j * G + i]) * fac[i];
+        for (int i = 0; i < G; ++i)
+            y[(size_t)k * G + i] = ytmp[i];
+    }
+    for (int j = 0; j < n; ++j)
+        for (int i = 0; i < G; ++i)
+            AD(j, j, i) = 1 + AD(j, j, i);
+#undef AD
+    free(y); free(drhs); free(r0); free(r); free(fac); free(ytmp);
 }
 
 /* WeightedNorm1 (src/odevec.F90:669-684): max over cells of sqrt(sum e^2 w / n) */
@@ -503,12 +555,20 @@ static void solve_linear_system(ode_t* o, double* t, double* dt, double* y)
             continue;
         }
         masked_copy(o, y, NS(o, 0)); /* :293-299 */
-        if (o->UpdateJac) {          /* :301-315, LUmethod 1 */
-            get_jac(o, o->coeff[o->order][0], y, *dt);
-            if (o->net->dense)
+        if (o->UpdateJac) { /* :301-315 */
+            if (o->net->lu_method == 3) {
+                calc_jac_fd(o, o->coeff[o->order][0], y, *dt);
                 lu_dense(o);
-            else
-                lu_sparse(o);
+            } else {
+                /* LUmethod 1: P, then its factors; LUmethod 2: the factors */
+                get_jac(o, o->coeff[o->order][0], y, *dt);
+                if (o->net->lu_method == 1) {
+                    if (o->net->dense)
+                        lu_dense(o);
+                    else
+                        lu_sparse(o);
+                }
+            }
             o->jacs++;
             o->UpdateJac = 0;
             o->LastJacobianUpdate = 0;

@@ -17,7 +17,8 @@ What it does:
    parses the generated Fortran: the permutation, the CSC pattern
    (``row_index``, ``u_col_start``, ``l_col_start``, 1-based in the Fortran,
    stored 0-based here), ``nnz``, and the generated ``rhs(:,i)`` and
-   ``jac(:,i,j)`` / ``jac%sdata(:,i)`` expressions.
+   ``jac(:,i,j)`` / ``jac%sdata(:,i)`` expressions, and for LUmethod 2 the
+   ``LU(:,i,j)`` expressions of the generated GetLU.
 3. Evaluates those expressions at seeded random points with Python floats.
    Python float arithmetic is IEEE binary64 without fused multiply-add and
    evaluates ``a*b*c`` and ``a+b+c`` left to right, like gfortran -O2 on
@@ -55,6 +56,9 @@ CASES = [
     ("PRIMORDIAL", "CSC", "FF"),
     ("PRIMORDIAL", "CSC", "CMK"),
     ("PRIMORDIAL", "CSC", "INVERT"),
+    # LUmethod 2: the generated GetLU (symbolic factors), dense only
+    ("ROBER", "DENSE", "None", 2),
+    ("OREGO", "DENSE", "None", 2),
 ]
 NSAMPLES = 6
 
@@ -99,8 +103,8 @@ def fortran_expr_to_python(e):
     e = re.sub(r"\b(y|k)\s*\(\s*:\s*,\s*(\d+)\s*\)", lambda m: "%s[%d]" % (m.group(1), int(m.group(2)) - 1), e)
     e = re.sub(r"(\d\.?\d*)d([+-]?\d+)", r"\1e\2", e)
     # gfortran expands small integer powers into multiplications
-    e = re.sub(r"((?:y|k)\[\d+\])\*\*2\b", r"(\1*\1)", e)
-    e = re.sub(r"((?:y|k)\[\d+\])\*\*3\b", r"(\1*(\1*\1))", e)
+    e = re.sub(r"((?:y|k)\[\d+\]|\bbeta|\bdt)\*\*2\b", r"(\1*\1)", e)
+    e = re.sub(r"((?:y|k)\[\d+\]|\bbeta|\bdt)\*\*3\b", r"(\1*(\1*\1))", e)
     if "**" in e:
         raise ValueError("unhandled power in %s" % e)
     return e
@@ -117,9 +121,13 @@ def parse_generated(build):
         out["row_index"] = [v - 1 for v in int_list(solver, "this%LU%row_index")]
         out["u_col_start"] = [v - 1 for v in int_list(solver, "this%LU%u_col_start")]
         out["l_col_start"] = [v - 1 for v in int_list(solver, "this%LU%l_col_start")]
-    rhs, jac = {}, {}
+    rhs, jac, lu = {}, {}, {}
     for line in common.split("\n"):
         s = line.strip()
+        m = re.match(r"LU\(:,(\d+),(\d+)\)\s*=\s*(.*)$", s)
+        if m:
+            lu[(int(m.group(1)) - 1, int(m.group(2)) - 1)] = fortran_expr_to_python(m.group(3))
+            continue
         m = re.match(r"rhs\(:,(\d+)\)\s*=\s*(.*)$", s)
         if m:
             rhs[int(m.group(1)) - 1] = fortran_expr_to_python(m.group(2))
@@ -131,7 +139,7 @@ def parse_generated(build):
         m = re.match(r"jac%sdata\(:,(\d+)\)\s*=\s*(.*)$", s)
         if m:
             jac[int(m.group(1)) - 1] = fortran_expr_to_python(m.group(2))
-    return out, rhs, jac
+    return out, rhs, jac, lu
 
 
 def hexs(vals):
@@ -149,13 +157,15 @@ def sample_inputs(rng, neq, nrea):
 def run_cases(work):
     results = {}
     rng = np.random.default_rng(20240611)
-    for ex, pack, order in CASES:
+    for case in CASES:
+        ex, pack, order = case[:3]
+        lum = case[3] if len(case) > 3 else 1
         for d in ("build",):
             os.makedirs(os.path.join(work, d), exist_ok=True)
         cmd = [sys.executable, "pre_odevec.py", "--nvector=32", "--example=%s" % ex,
-               "--packaging=%s" % pack, "--ordering=%s" % order]
+               "--packaging=%s" % pack, "--ordering=%s" % order, "--LUmethod=%d" % lum]
         log = subprocess.run(cmd, cwd=work, capture_output=True, text=True, check=True).stdout
-        meta, rhs, jac = parse_generated(os.path.join(work, "build"))
+        meta, rhs, jac, lu = parse_generated(os.path.join(work, "build"))
         m = re.search(r"NNZs in Jacobian: (\d+)", log)
         meta["p_nnz"] = int(m.group(1))
         neq = meta["neq"]
@@ -170,10 +180,16 @@ def run_cases(work):
                 P = [eval(jac[(i, j)], {}, env) for i in range(neq) for j in range(neq)]
             else:
                 P = [eval(jac[i], {}, env) for i in range(meta["nnz"])]
-            samples.append({"y": hexs(y), "k": hexs(k), "beta": beta.hex(), "dt": dt.hex(),
-                            "rhs": hexs(f), "P": hexs(P)})
+            smp = {"y": hexs(y), "k": hexs(k), "beta": beta.hex(), "dt": dt.hex(),
+                   "rhs": hexs(f), "P": hexs(P)}
+            if lum == 2:
+                # row-major n x n of the symbolic factors; entries GetLU does not
+                # write stay at their initial 0
+                smp["LU"] = hexs([eval(lu[(i, j)], {}, env) if (i, j) in lu else 0.0
+                                  for i in range(neq) for j in range(neq)])
+            samples.append(smp)
         meta["samples"] = samples
-        results["%s_%s_%s" % (ex, pack, order)] = meta
+        results["%s_%s_%s" % (ex, pack, order) + ("_LU%d" % lum if lum != 1 else "")] = meta
         print(ex, pack, order, "nnz", meta["nnz"], "perm", meta["perm"])
     return results
 

@@ -69,6 +69,12 @@ CASES = [
     ("PRIMORDIAL", dict(ncells=256), "PRIMORDIAL_DENSE_NONE", 1),
     ("PRIMORDIAL", dict(ncells=256), "PRIMORDIAL_DENSE_NONE", 32),
     ("SYN64", dict(ncells=128), "SYN64_CSC_CMK", 1),
+    # LUmethod 2 (symbolic factors) and 3 (difference quotients)
+    ("ROBER", dict(ncells=256), "ROBER_DENSE_NONE_LU2", 32),
+    ("OREGO", dict(ncells=256), "OREGO_DENSE_NONE_LU2", 1),
+    ("ROBER", dict(ncells=256), "ROBER_DENSE_NONE_LU3", 32),
+    ("ROBER", dict(ncells=256), "ROBER_DENSE_NONE_LU3", 1),
+    ("PRIMORDIAL", dict(ncells=256), "PRIMORDIAL_DENSE_NONE_LU3", 1),
 ]
 
 

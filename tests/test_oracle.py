@@ -173,3 +173,28 @@ def test_resident_continuation(oracle):
     rel = np.abs(y[:12] - one[:12]) / np.abs(one[:12])
     assert np.max(rel[np.abs(one[:12]) > 1e-14]) < 1e-3
     assert steps[1] < steps[0]
+
+
+@pytest.mark.parametrize("alt,tol", [("ROBER_DENSE_NONE_LU2", 1e-11), ("ROBER_DENSE_NONE_LU3", 1e-7)])
+def test_other_jacobian_methods_agree_on_rober(oracle, alt, tol):
+    # the symbolic factors (LUmethod 2) and the difference quotients
+    # (LUmethod 3) only change the iteration matrix of the modified Newton
+    # iteration: the same steps are taken and the results agree to rounding
+    # (2) or to the difference-quotient error (3)
+    wl = W.rober(ncells=256)
+    a = oracle.solve("ROBER_DENSE_NONE", wl.y, wl.t0, wl.dt0, wl.t_stop, wl.rtol, wl.atol, wl.dt_min, group=32)
+    b = oracle.solve(alt, wl.y, wl.t0, wl.dt0, wl.t_stop, wl.rtol, wl.atol, wl.dt_min, group=32)
+    assert np.all(a[3] == 0) and np.all(b[3] == 0)
+    m = np.abs(a[0]) > wl.atol / wl.rtol
+    assert np.max(np.abs(a[0][m] - b[0][m]) / np.abs(a[0][m])) < tol
+    assert np.array_equal(a[4][:, 0], b[4][:, 0])  # steps
+
+
+def test_difference_quotients_on_primordial(oracle):
+    wl = W.primordial(ncells=64, network="PRIMORDIAL_DENSE_NONE")
+    a = oracle.solve("PRIMORDIAL_DENSE_NONE", wl.y, wl.t0, wl.dt0, wl.t_stop, wl.rtol, wl.atol, wl.dt_min)
+    b = oracle.solve("PRIMORDIAL_DENSE_NONE_LU3", wl.y, wl.t0, wl.dt0, wl.t_stop, wl.rtol, wl.atol, wl.dt_min)
+    assert np.all(b[3] == 0)
+    m = np.abs(a[0]) > wl.atol / wl.rtol
+    rel = np.abs(a[0][m] - b[0][m]) / np.abs(a[0][m])
+    assert np.median(rel) < 1e-12 and rel.max() < 1e-7

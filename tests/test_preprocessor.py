@@ -3,7 +3,8 @@
 tests/golden/ref_preproc.json holds, for nine (example, packaging, ordering)
 cases, what the reference preprocessor produced (permutation, LU nnz, CSC
 arrays) and the values of its generated Fortran right-hand sides and
-iteration matrices at seeded points (tests/golden/make_golden.py).
+iteration matrices at seeded points, plus, for two dense LUmethod=2 cases,
+the values of its generated symbolic factors (tests/golden/make_golden.py).
 """
 import json
 import os
@@ -25,9 +26,14 @@ h2f = lambda l: np.array([float.fromhex(v) for v in l])
 def systems():
     out = {}
     for key in GOLDEN:
-        ex, pack, order = key.split("_")
-        out[key] = pre_odevec.build_system(networks.load(ex), order, pack)
+        ex, pack, order, lum = _case(key)
+        out[key] = pre_odevec.build_system(networks.load(ex), order, pack, lu_method=lum)
     return out
+
+
+def _case(key):
+    parts = key.split("_")
+    return parts[0], parts[1], parts[2], int(parts[3][2:]) if len(parts) > 3 else 1
 
 
 @pytest.mark.parametrize("key", sorted(GOLDEN))
@@ -61,7 +67,8 @@ def test_emitted_code_bit_identical_to_reference_expressions(oracle, key):
         f, a = oracle.evaluate(tag, h2f(smp["y"]), h2f(smp["k"]), float.fromhex(smp["beta"]),
                                float.fromhex(smp["dt"]))
         assert np.array_equal(f, h2f(smp["rhs"]))
-        P = h2f(smp["P"])
+        # LUmethod 2: jac() writes the symbolic factors, pinned by GetLU's values
+        P = h2f(smp["LU"] if "LU" in smp else smp["P"])
         if "DENSE" in key:
             full = np.zeros((n, n))
             for c in range(n):
@@ -133,7 +140,10 @@ def test_cli_writes_variant(tmp_path):
     (["--packaging=CSR"], "CSR packaging is not supported"),
     (["--packaging=XYZ"], "This format is not known"),
     (["--heatcool=1"], "heating/cooling"),
-    (["--LUmethod=2"], "LUmethod=2"),
+    (["--LUmethod=2", "--packaging=CSC"], "LUmethod=2 needs --packaging=DENSE"),
+    (["--LUmethod=3", "--packaging=CSC"], "not supported with sparse matrices"),
+    (["--LUmethod=3", "--ordering=CMK"], "LUmethod=3 needs --ordering=None"),
+    (["--LUmethod=4"], "is not known"),
     (["--equilibrium_H=1", "--packaging=CSC"], "only allowed with DENSE"),
 ])
 def test_cli_rejects(tmp_path, argv, msg):
@@ -142,3 +152,29 @@ def test_cli_rejects(tmp_path, argv, msg):
                          cwd=os.path.dirname(HERE))
     assert out.returncode != 0
     assert msg in out.stderr + out.stdout
+
+
+def test_lumethod3_pattern_is_full_dynamic_block():
+    s = pre_odevec.build_system(networks.load("PRIMORDIAL"), "None", "DENSE", lu_method=3)
+    assert s.tag == "PRIMORDIAL_DENSE_NONE_LU3"
+    fz = pre_odevec.frozen_species(s)
+    nd = s.neq - len(fz)
+    dyn = [i for i in range(s.neq) if i not in fz]
+    assert s.lu_pat[np.ix_(dyn, dyn)].all()
+    for f in fz:
+        assert s.lu_pat[f].sum() == 1 and s.lu_pat[:, f].sum() == 1 and s.lu_pat[f, f]
+    assert s.nnz == nd * nd + len(fz)
+    fl = pre_odevec.flop_counts(s)
+    assert fl["jac"] > (nd + 1) * fl["rhs"] and fl["lu_factor"] > 0
+
+
+def test_lumethod2_factors_are_lu_of_p():
+    # the emitted factors multiply back to P at a point
+    s = pre_odevec.build_system(networks.load("OREGO"), "None", "DENSE", lu_method=2)
+    pt = {**{sym: v for sym, v in zip(s.net.y, (0.3, 1.7, 2.2))}, sp.Symbol("dt"): 0.01, sp.Symbol("beta"): 0.8}
+    LU = s.lu_exprs.subs(pt).evalf()
+    n = s.neq
+    L = sp.eye(n) + sp.Matrix(n, n, lambda i, j: LU[i, j] if i > j else 0)
+    U = sp.Matrix(n, n, lambda i, j: LU[i, j] if i <= j else 0)
+    P = s.P_order.subs(pt).evalf()
+    assert max(abs(float(v)) for v in (L * U - P)) < 1e-12
