@@ -18,7 +18,16 @@ deterministic, so a request's results are the same alone and in any mix
 
 Latency of a request step = completion time - the time the step became
 ready (its arrival for step 0, the previous step's completion after that),
-so it includes any wait for admission.
+so it includes any wait for admission; service time = completion time -
+launch time.
+
+Sharing the device: the solve kernel is persistent (its blocks stay resident
+until the request's cells run out), so a launch that takes every SM would
+hold back every request behind it.  With fair sharing, each launch gets
+1/k of the device's resident blocks when k requests are in flight (all of
+them when it runs alone), and requests of at most `small_cells` cells run
+on a higher-priority stream, so their blocks are placed first whenever
+blocks retire.
 
 Failures: where the reference stops the program (src/odevec.F90:272-275,
 380-390), a cell here gets a nonzero status.  A failed cell keeps its
@@ -64,10 +73,15 @@ class StepRecord:
     network: str
     ready: float
     done: float
+    launched: float = 0.0
 
     @property
     def latency(self) -> float:
         return self.done - self.ready
+
+    @property
+    def service(self) -> float:
+        return self.done - self.launched
 
 
 @dataclasses.dataclass
@@ -117,8 +131,9 @@ class Scheduler:
                 waiting.pop(0)
                 used += need
                 h = self.backend.admit(r)
-                active[r.rid] = {"req": r, "h": h, "step": 0, "ready": max(r.arrival, 0.0), "need": need}
-                self.backend.launch(h, 0)
+                active[r.rid] = {"req": r, "h": h, "step": 0, "ready": max(r.arrival, 0.0), "need": need,
+                                 "launched": now()}
+                self.backend.launch(h, 0, len(active))
             # completions
             done_any = False
             for rid in list(active):
@@ -127,11 +142,13 @@ class Scheduler:
                     done_any = True
                     tdone = now()
                     r = st["req"]
-                    records.append(StepRecord(rid, st["step"], r.ncells, r.network, st["ready"], tdone))
+                    records.append(StepRecord(rid, st["step"], r.ncells, r.network, st["ready"], tdone,
+                                              st["launched"]))
                     st["step"] += 1
                     if st["step"] < r.steps:
                         st["ready"] = tdone
-                        self.backend.launch(st["h"], st["step"])
+                        st["launched"] = now()
+                        self.backend.launch(st["h"], st["step"], len(active))
                     else:
                         results[rid] = self.backend.release(st["h"])
                         used -= st["need"]
@@ -143,13 +160,16 @@ class Scheduler:
 
 def summarize(records: List[StepRecord], results: Optional[Dict[int, Result]] = None) -> dict:
     lat = np.array([r.latency for r in records]) if records else np.zeros(1)
+    svc = np.array([r.service for r in records]) if records else np.zeros(1)
     t0 = min(r.ready for r in records) if records else 0.0
     t1 = max(r.done for r in records) if records else 1.0
     cells = sum(r.ncells for r in records)
     return {"request_steps": len(records), "cells": cells, "seconds": t1 - t0,
             "cells_per_s": cells / max(t1 - t0, 1e-12),
             "p50_ms": 1e3 * float(np.percentile(lat, 50)), "p99_ms": 1e3 * float(np.percentile(lat, 99)),
-            "max_ms": 1e3 * float(lat.max())} | (
+            "max_ms": 1e3 * float(lat.max()),
+            "service_p50_ms": 1e3 * float(np.percentile(svc, 50)),
+            "service_p99_ms": 1e3 * float(np.percentile(svc, 99))} | (
         {} if results is None else
         {"failed_cells": sum(results[rid].failed for rid in {r.rid for r in records} if rid in results)})
 
@@ -158,13 +178,19 @@ class GpuBackend:
     """Each admitted request owns device buffers, a resident workspace and a
     CUDA stream; launches are asynchronous and completion is an event."""
 
-    def __init__(self, precision: str = "fp32_lu", device: str = "cuda"):
+    def __init__(self, precision: str = "fp32_lu", device: str = "cuda", fair_share: bool = True,
+                 small_cells: int = 16384, blocks_per_sm: int = 3):
         import torch
         from . import solver as S
         self.S = S
         self.torch = torch
         self.precision = precision
         self.device = device
+        self.fair_share = fair_share
+        self.small_cells = small_cells
+        self.sms = torch.cuda.get_device_properties(device).multi_processor_count
+        # resident blocks of the per-cell kernels (3 blocks of 128 threads per SM)
+        self.capacity = self.sms * blocks_per_sm
 
     def _solver(self, r: Request):
         # one solver handle per request: each owns its cell counter, so
@@ -182,7 +208,8 @@ class GpuBackend:
     def admit(self, r: Request):
         torch = self.torch
         ode = self._solver(r)
-        stream = torch.cuda.Stream(device=self.device)
+        lo, hi = torch.cuda.Stream.priority_range()  # (lowest, highest): numerically hi <= lo
+        stream = torch.cuda.Stream(device=self.device, priority=hi if r.ncells <= self.small_cells else lo)
         with torch.cuda.stream(stream):
             h = {"r": r, "ode": ode, "stream": stream,
                  "y": torch.tensor(r.y0, device=self.device),
@@ -195,9 +222,11 @@ class GpuBackend:
                  "ev": None}
         return h
 
-    def launch(self, h, step: int):
+    def launch(self, h, step: int, active: int = 1):
         torch = self.torch
         r = h["r"]
+        if self.fair_share:
+            h["ode"].grid_blocks = max(self.sms, self.capacity // max(active, 1))
         with torch.cuda.stream(h["stream"]):
             h["ts"].fill_(r.dt_hydro * (step + 1))
             if step > 0:
@@ -240,7 +269,7 @@ class OracleBackend:
                 "ws": self.O.workspace(r.network, r.ncells), "failed": np.zeros(r.ncells, np.int32),
                 "done": False}
 
-    def launch(self, h, step: int):
+    def launch(self, h, step: int, active: int = 1):
         r = h["r"]
         mask = None if step == 0 else (h["failed"] == 0).astype(np.uint8)
         y, t, dt, st, _ = self.O.solve(r.network, h["y"], h["t"], h["dt"], r.dt_hydro * (step + 1), r.rtol,
@@ -307,19 +336,27 @@ def main(argv=None):
     p.add_argument("--slots", type=int, default=16, help="requests in flight")
     p.add_argument("--seed", type=int, default=5)
     p.add_argument("--isolated", action="store_true", help="also time every request alone")
+    p.add_argument("--no-fair-share", action="store_true",
+                   help="every launch may take the whole device (no 1/k block share, one stream priority)")
     a = p.parse_args(argv)
     reqs = make_stream(a.seed, a.rate, a.duration, tuple(a.networks.split(",")), (a.min_cells, a.max_cells),
                        (a.dt_min, a.dt_max), a.steps)
     for prec in a.precisions.split(","):
-        be = GpuBackend(prec)
+        be = GpuBackend(prec, fair_share=not a.no_fair_share)
         # warm-up: one small request per network (module load, first launches)
         warm = [Request(10**6 + i, r.network, r.y0[:, :64].copy(), r.dt_hydro, 1, 0.0, r.rtol, r.atol,
                         r.dt_min, r.dt_in) for i, r in enumerate({r.network: r for r in reqs}.values())]
         Scheduler(be, a.budget, a.slots).run(warm, realtime=False)
         recs, res = Scheduler(be, a.budget, a.slots).run(reqs, realtime=True)
+        mix = summarize(recs, res)
+        offered = sum(r.ncells * r.steps for r in reqs) / a.duration
         out = {"form": prec, "requests": len(reqs), "rate": a.rate, "steps": a.steps,
                "cells": [a.min_cells, a.max_cells], "dt_hydro": [a.dt_min, a.dt_max],
-               "budget_gb": a.budget / 1e9, "slots": a.slots, "mix": summarize(recs, res)}
+               "budget_gb": a.budget / 1e9, "slots": a.slots, "fair_share": not a.no_fair_share,
+               "mix": mix,
+               # offered load: cell-steps asked for per second of arrivals, against
+               # the cell-steps per second the device delivered in the mix
+               "offered_cell_steps_per_s": offered, "load_factor": offered / mix["cells_per_s"]}
         by_net = {}
         for r in recs:
             by_net.setdefault(r.network, []).append(r)
@@ -332,10 +369,16 @@ def main(argv=None):
                     iso[(x.rid, x.step)] = x.latency
             ratio = np.array([x.latency / iso[(x.rid, x.step)] for x in recs])
             iso_l = np.array(list(iso.values()))
+            sratio = np.array([x.service / iso[(x.rid, x.step)] for x in recs])
+            lat_mix = np.array([x.latency for x in recs])
             out["isolated"] = {"p50_ms": 1e3 * float(np.percentile(iso_l, 50)),
                                "p99_ms": 1e3 * float(np.percentile(iso_l, 99)),
                                "mix_over_isolated_p50": float(np.percentile(ratio, 50)),
-                               "mix_over_isolated_p99": float(np.percentile(ratio, 99))}
+                               "mix_over_isolated_p99": float(np.percentile(ratio, 99)),
+                               "mix_p99_over_isolated_p99": float(np.percentile(lat_mix, 99)
+                                                                  / np.percentile(iso_l, 99)),
+                               "service_over_isolated_p50": float(np.percentile(sratio, 50)),
+                               "service_over_isolated_p99": float(np.percentile(sratio, 99))}
         print(json.dumps(out), flush=True)
 
 

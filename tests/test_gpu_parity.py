@@ -15,14 +15,14 @@ pytestmark = pytest.mark.gpu
 
 
 def run_gpu(S, wl, precision="fp64", group=None, host=False, mask=None, check_negatives=False,
-            max_attempts=0, dt_min=None, batch=(0, 0, 0)):
+            max_attempts=0, dt_min=None, batch=(0, 0, 0), staging=0):
     import torch
     ode = S.Odevec(wl.network, max_cells=wl.ncells if host else 0, RelativeTolerance=wl.rtol,
                    AbsoluteTolerance=wl.atol,
                    MinimalTimestep=wl.dt_min if dt_min is None else dt_min,
                    CheckNegatives=check_negatives, nvector=wl.group if group is None else group,
                    precision=precision, max_attempts=max_attempts, raise_on_failure=False,
-                   jac_batch=batch[0], ss_batch=batch[1], max_wait=batch[2])
+                   jac_batch=batch[0], ss_batch=batch[1], max_wait=batch[2], staging=staging)
     S.InitOdevec(ode)
     try:
         if host:
@@ -99,6 +99,12 @@ def test_scheduling_does_not_change_results(gpu_lib, precision):
     for batch in [(0, 0, 0), (32, 32, 1000), (5, 20, 2)]:
         g = run_gpu(gpu_lib, wl, precision, batch=batch)
         assert_bitwise(g, ref, "batch %s" % (batch,))
+    # every staging, the block-synchronous one (6) included, with the
+    # default batches and with per-cell blocks
+    for staging in (1, 2, 3, 4, 6) + ((5,) if precision == "fp32_lu" else ()):
+        for batch in [(0, 0, 0), (1, 1, -1)]:
+            g = run_gpu(gpu_lib, wl, precision, batch=batch, staging=staging)
+            assert_bitwise(g, ref, "staging %d batch %s" % (staging, batch))
 
 
 def test_host_entry_point_matches_device(gpu_lib, oracle):
