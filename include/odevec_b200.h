@@ -158,6 +158,20 @@ int32_t odevec_solve_resident(odevec_solver* s, int64_t ncells, double* y, doubl
                               const double* t_stop, const uint8_t* mask, int32_t* status,
                               int32_t* stats, double* workspace, int32_t resume, void* stream);
 
+/* The operator-split caller's format (tests/primordial.f90:79-87, 113-140):
+   the hydro code keeps mass fractions x and the gas density rho (g/cm^3) per
+   cell; the network integrates number densities n (1/cm^3).  direction
+   OV_X2N: n_j = (rho * x_j) * imass_j; OV_N2X: x_j = (n_j * mass_j) / rho,
+   with the network's species masses (g) and inverse masses (1/g)
+   (krome_x2n / krome_n2x).  Entries without a mass (temperature, counters)
+   are copied unchanged.  in and out: species-major [neq][ncells] device
+   arrays, may be the same array; rho: [ncells].  Asynchronous on stream;
+   allocates nothing.  OV_API_EUNSUPPORTED for a network without masses. */
+#define OV_X2N 0
+#define OV_N2X 1
+int32_t odevec_convert(const char* network, int64_t ncells, int32_t direction, const double* in,
+                       double* out, const double* rho, void* stream);
+
 /* CloseOdevec */
 int32_t odevec_close(odevec_solver* s);
 

@@ -678,6 +678,45 @@ struct Cell {
 /* number of lanes of the warp for which b holds */
 __device__ __forceinline__ int warp_count(bool b) { return __popc(__ballot_sync(FULL, b)); }
 
+/* Block-wide votes for the block-synchronous staging.  The cell loop's
+   phases leave the lanes of a warp on different paths, so each vote first
+   reconverges the warp and then uses the non-aligned barrier forms, which
+   PTX defines for threads that arrive from divergent code (the aligned
+   forms behind __syncthreads_count/_and/_or assume a converged warp).
+   Every thread of the block executes every vote once per trip. */
+__device__ __forceinline__ int block_count(bool b)
+{
+    __syncwarp();
+    int r;
+    asm volatile("{\n\t.reg .pred p;\n\tsetp.ne.u32 p, %1, 0;\n\tbarrier.red.popc.u32 %0, 0, p;\n\t}"
+                 : "=r"(r)
+                 : "r"((unsigned)b)
+                 : "memory");
+    return r;
+}
+__device__ __forceinline__ bool block_and(bool b)
+{
+    __syncwarp();
+    unsigned r;
+    asm volatile("{\n\t.reg .pred p, q;\n\tsetp.ne.u32 p, %1, 0;\n\tbarrier.red.and.pred q, 0, p;\n\t"
+                 "selp.u32 %0, 1, 0, q;\n\t}"
+                 : "=r"(r)
+                 : "r"((unsigned)b)
+                 : "memory");
+    return r != 0;
+}
+__device__ __forceinline__ bool block_or(bool b)
+{
+    __syncwarp();
+    unsigned r;
+    asm volatile("{\n\t.reg .pred p, q;\n\tsetp.ne.u32 p, %1, 0;\n\tbarrier.red.or.pred q, 0, p;\n\t"
+                 "selp.u32 %0, 1, 0, q;\n\t}"
+                 : "=r"(r)
+                 : "r"((unsigned)b)
+                 : "memory");
+    return r != 0;
+}
+
 template <class Net, int G, class LUT, int STAGE>
 __global__ void __launch_bounds__(StageCfg<STAGE>::BS, StageCfg<STAGE>::MINB) bdf_kernel(const LaunchArgs A)
 {
@@ -725,7 +764,7 @@ __global__ void __launch_bounds__(StageCfg<STAGE>::BS, StageCfg<STAGE>::MINB) bd
             }
             if constexpr (StageCfg<STAGE>::SYNC) {
                 /* every thread of the block reaches this barrier once per trip */
-                if (__syncthreads_and(ph == PH_EXHAUSTED))
+                if (block_and(ph == PH_EXHAUSTED))
                     break;
             } else {
                 if (__all_sync(FULL, ph == PH_EXHAUSTED))
@@ -863,9 +902,9 @@ __global__ void __launch_bounds__(StageCfg<STAGE>::BS, StageCfg<STAGE>::MINB) bd
                 const bool mv = ph == PH_NEWTON || ph == PH_START || ph == PH_RESTART;
                 const bool old = ph == PH_JACWAIT && c.wait >= A.max_wait;
                 if constexpr (StageCfg<STAGE>::SYNC) {
-                    const int waiting = __syncthreads_count(ph == PH_JACWAIT);
-                    const int moving = __syncthreads_count(mv);
-                    const bool aged = __syncthreads_or(old);
+                    const int waiting = block_count(ph == PH_JACWAIT);
+                    const int moving = block_count(mv);
+                    const bool aged = block_or(old);
                     run = waiting > 0 && (waiting >= A.jac_batch * (BS / 32) || moving == 0 || aged);
                 } else {
                     const int waiting = warp_count(ph == PH_JACWAIT);
@@ -1003,9 +1042,9 @@ __global__ void __launch_bounds__(StageCfg<STAGE>::BS, StageCfg<STAGE>::MINB) bd
                 const bool mv = ph == PH_PRED || ph == PH_NEWTON || ph == PH_RESTART;
                 const bool old = ph == PH_SSWAIT && c.wait >= A.max_wait;
                 if constexpr (StageCfg<STAGE>::SYNC) {
-                    const int waiting = __syncthreads_count(ph == PH_SSWAIT);
-                    const int moving = __syncthreads_count(mv);
-                    const bool aged = __syncthreads_or(old);
+                    const int waiting = block_count(ph == PH_SSWAIT);
+                    const int moving = block_count(mv);
+                    const bool aged = block_or(old);
                     run = waiting > 0 && (waiting >= A.ss_batch * (BS / 32) || moving == 0 || aged);
                 } else {
                     const int waiting = warp_count(ph == PH_SSWAIT);

@@ -16,6 +16,8 @@
 #define OV_OREGO_CSC_CMK_IDX_TGAS -1
 static const int ov_orego_csc_cmk_sizes[7] = {3, 7, 0, 0, -1, 3, 1};
 static const double ov_orego_csc_cmk_defaults[2] = {1.0, 1e-10}; /* nvector, dt_min */
+static const double ov_orego_csc_cmk_mass[3] = {0.0, 0.0, 0.0};
+static const double ov_orego_csc_cmk_imass[3] = {0.0, 0.0, 0.0};
 static const int ov_orego_csc_cmk_perm[3] = {2, 1, 0};
 static const int ov_orego_csc_cmk_row_index[7] = {0, 1, 1, 2, 0, 1, 2};
 static const int ov_orego_csc_cmk_u_col_start[4] = {0, 2, 4, 7};

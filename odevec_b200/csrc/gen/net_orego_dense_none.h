@@ -16,6 +16,8 @@
 #define OV_OREGO_DENSE_NONE_IDX_TGAS -1
 static const int ov_orego_dense_none_sizes[7] = {3, 8, 0, 1, -1, 3, 1};
 static const double ov_orego_dense_none_defaults[2] = {1.0, 1e-10}; /* nvector, dt_min */
+static const double ov_orego_dense_none_mass[3] = {0.0, 0.0, 0.0};
+static const double ov_orego_dense_none_imass[3] = {0.0, 0.0, 0.0};
 static const int ov_orego_dense_none_perm[3] = {0, 1, 2};
 static const int ov_orego_dense_none_row_index[8] = {0, 1, 2, 0, 1, 2, 1, 2};
 static const int ov_orego_dense_none_u_col_start[4] = {0, 3, 6, 8};

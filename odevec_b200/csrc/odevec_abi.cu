@@ -37,13 +37,17 @@ namespace {
 
 struct NetEntry {
     const char* tag;
-    const int* sizes;       /* neq, nnz, nrea, dense, idx_tgas */
+    const int* sizes;       /* neq, nnz, nrea, dense, idx_tgas, solver-state species, LUmethod */
     const double* defaults; /* nvector, dt_min */
+    const double* mass;     /* species masses (g), 0 where none */
+    const double* imass;    /* inverse masses (1/g) */
     ov::launch_fn exact;
     ov::launch_fn fma;
 };
 
-#define OV_NET(cid, TAG) {TAG, ov_##cid##_sizes, ov_##cid##_defaults, ov::exact::launch_##cid, ov::fma::launch_##cid},
+#define OV_NET(cid, TAG)                                                                            \
+    {TAG, ov_##cid##_sizes, ov_##cid##_defaults, ov_##cid##_mass, ov_##cid##_imass, ov::exact::launch_##cid, \
+     ov::fma::launch_##cid},
 const NetEntry g_nets[] = {
 #include "gen/registry.inc"
 };
@@ -94,6 +98,31 @@ struct odevec_solver {
 namespace {
 /* cells whose FP32-LU solve failed get their inputs back and a retry mask;
    *nfail counts them */
+/* mass fraction <-> number density (tests/primordial.f90:113-140), one
+   thread per cell, species-major so every species row is a coalesced sweep */
+#define OV_MASS_MAX 64
+struct ov_mass_tab {
+    double m[OV_MASS_MAX];
+    double im[OV_MASS_MAX];
+    int neq;
+};
+
+__global__ void __launch_bounds__(256) ov_convert(int64_t ncells, int direction, const double* in, double* out,
+                                                  const double* rho, const ov_mass_tab tab)
+{
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; c < ncells; c += stride) {
+        const double r = rho[c];
+        for (int j = 0; j < tab.neq; ++j) {
+            const double v = in[(int64_t)j * ncells + c];
+            double o = v;
+            if (tab.m[j] != 0.0)
+                o = direction == OV_X2N ? r * v * tab.im[j] : v * tab.m[j] / r;
+            out[(int64_t)j * ncells + c] = o;
+        }
+    }
+}
+
 __global__ void ov_escalate(int64_t ncells, int neq, double* y, double* t, double* dt,
                             const double* y_in, const double* t_in, const double* dt_in,
                             const int32_t* status, const uint8_t* mask, uint8_t* retry,
@@ -356,8 +385,11 @@ static int32_t solve_impl(odevec_solver* s, int64_t ncells, double* y, double* t
             b.stats = nullptr;
             b.run_if = s->d_queue + 1;
             err = cudaMemsetAsync(s->d_queue, 0, sizeof(unsigned long long), st);
+            /* staging 5 exists for FP32 factors only: the FP64 re-solve of
+               such a launch uses the thread-local default */
+            const int stage64 = stage == 5 ? 3 : stage;
             if (err == cudaSuccess)
-                err = e.fma(b, o.group_size, 0, stage, o.block_threads, o.grid_blocks, st);
+                err = e.fma(b, o.group_size, 0, stage64, o.block_threads, o.grid_blocks, st);
         }
     }
     if (err == cudaErrorNotSupported)
@@ -409,6 +441,46 @@ int32_t odevec_solve_host(odevec_solver* s, int64_t ncells, double* y, double* t
         e = cudaStreamSynchronize(st);
     if (e != cudaSuccess)
         return fail(OV_API_ECUDA, "odevec_solve_host: %s", cudaGetErrorString(e));
+    return OV_API_OK;
+}
+
+int32_t odevec_convert(const char* network, int64_t ncells, int32_t direction, const double* in, double* out,
+                       const double* rho, void* stream)
+{
+    const int ni = find_net(network);
+    if (ni < 0)
+        return fail(OV_API_ENONET, "unknown network variant '%s'", network ? network : "(null)");
+    if (ncells < 0)
+        return fail(OV_API_EINVAL, "ncells < 0");
+    if (direction != OV_X2N && direction != OV_N2X)
+        return fail(OV_API_EINVAL, "direction must be OV_X2N or OV_N2X");
+    if (ncells == 0)
+        return OV_API_OK;
+    if (!in || !out || !rho)
+        return fail(OV_API_EINVAL, "in, out and rho are required");
+    const NetEntry& e = g_nets[ni];
+    const int neq = e.sizes[0];
+    ov_mass_tab tab;
+    if (neq > OV_MASS_MAX)
+        return fail(OV_API_EUNSUPPORTED, "%s: more than %d species", e.tag, OV_MASS_MAX);
+    bool any = false;
+    for (int j = 0; j < neq; ++j) {
+        tab.m[j] = e.mass[j];
+        tab.im[j] = e.imass[j];
+        any = any || e.mass[j] != 0.0;
+    }
+    if (!any)
+        return fail(OV_API_EUNSUPPORTED, "%s has no species masses", e.tag);
+    tab.neq = neq;
+    int dev = 0, sms = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    const int64_t want = (ncells + 255) / 256;
+    const int blocks = (int)(want < (int64_t)sms * 8 ? want : (int64_t)sms * 8);
+    ov_convert<<<blocks, 256, 0, (cudaStream_t)stream>>>(ncells, direction, in, out, rho, tab);
+    const cudaError_t err = cudaGetLastError();
+    if (err != cudaSuccess)
+        return fail(OV_API_ECUDA, "odevec_convert: %s", cudaGetErrorString(err));
     return OV_API_OK;
 }
 

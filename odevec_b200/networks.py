@@ -47,6 +47,11 @@ class Network:
     # index of the gas temperature in the state vector (PRIMORDIAL only)
     idx_tgas: Optional[int] = None
     species: Optional[List[str]] = None
+    # species masses (g) and their inverses (1/g) for the mass-fraction <->
+    # number-density format of the operator-split caller; 0 marks an entry
+    # that is not a species abundance (temperature, counters)
+    masses: Optional[List[float]] = None
+    imasses: Optional[List[float]] = None
 
 
 def state_symbols(neq: int) -> List[sp.Symbol]:
@@ -83,6 +88,19 @@ def load_orego() -> Network:
 
 PRIMORDIAL_SPECIES = ["E", "H-", "H", "HE", "H2", "D", "HD", "H+", "HE+",
                       "H2+", "D+", "HE++", "CR", "g", "Tgas", "dummy"]
+
+# KROME's species masses (g) and inverse masses (1/g) for the 12 chemical
+# species, as the reference's PRIMORDIAL driver converts with them
+# (tests/primordial.f90:145-210); the inverses are KROME's own rounded
+# values, not 1/mass.  CR, g, Tgas and dummy carry no mass.
+PRIMORDIAL_MASSES = [9.10938188e-28, 1.67444345638e-24, 1.67353251819e-24, 6.69206503638e-24,
+                     3.34706503638e-24, 3.34603251819e-24, 5.01956503638e-24, 1.67262158e-24,
+                     6.69115409819e-24, 3.34615409819e-24, 3.34512158e-24, 6.69024316e-24,
+                     0.0, 0.0, 0.0, 0.0]
+PRIMORDIAL_IMASSES = [1.09776932527e+27, 5.9721335838e+23, 5.97538433901e+23, 1.49430705554e+23,
+                      2.9876921695e+23, 2.98861411108e+23, 1.99220448934e+23, 5.97863863505e+23,
+                      1.4945104915e+23, 2.98850552203e+23, 2.98942796572e+23, 1.49471398286e+23,
+                      0.0, 0.0, 0.0, 0.0]
 
 # (reactants, products) for rate coefficient k(:,i), i = 1..38.  A species
 # listed twice takes part twice (mass action: the flux is k * prod(y_r)).
@@ -155,6 +173,7 @@ def load_primordial() -> Network:
     k = rate_symbols(nrea)
     rhs = mass_action_rhs(y, k, PRIMORDIAL_SPECIES, PRIMORDIAL_REACTIONS)
     return Network("PRIMORDIAL", neq, nrea, y, rhs, k=k, rates="primordial",
+                   masses=list(PRIMORDIAL_MASSES), imasses=list(PRIMORDIAL_IMASSES),
                    idx_tgas=14, species=list(PRIMORDIAL_SPECIES))
 
 

@@ -386,6 +386,11 @@ def emit_c_header(sysm: System) -> str:
                   sysm.lu_method])
     L.append("static const double ov_%s_defaults[2] = {%d.0, %r}; /* nvector, dt_min */"
              % (cid, sysm.nvector, float(sysm.dt_min)))
+    # species masses (g) and inverse masses (1/g) for the mass-fraction format;
+    # all zero when the network has none
+    for name, vals in (("mass", net.masses), ("imass", net.imasses)):
+        vals = vals if vals is not None else [0.0] * n
+        L.append("static const double ov_%s_%s[%d] = {%s};" % (cid, name, n, ", ".join(repr(float(v)) for v in vals)))
     arr("perm", sysm.perm)
     arr("row_index", sysm.row_index)
     arr("u_col_start", sysm.u_col_start)

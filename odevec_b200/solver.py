@@ -96,6 +96,8 @@ def lib():
         L.odevec_solve_resident.restype = i32
         L.odevec_close.argtypes = [P]
         L.odevec_close.restype = i32
+        L.odevec_convert.argtypes = [ctypes.c_char_p, i64, i32, P, P, P, P]
+        L.odevec_convert.restype = i32
         L.odevec_last_error.restype = ctypes.c_char_p
         _lib = L
     return _lib

@@ -59,10 +59,11 @@ typedef struct {
     const int *sizes, *perm, *row_index, *u_col_start, *l_col_start;
     rhs_fn rhs;
     jac_fn jac;
+    const double *mass, *imass;
 } net_entry;
 #define OV_NET(cid, TAG)                                                                   \
     {TAG, ov_##cid##_sizes, ov_##cid##_perm, ov_##cid##_row_index, ov_##cid##_u_col_start, \
-     ov_##cid##_l_col_start, ov_##cid##_rhs, ov_##cid##_jac},
+     ov_##cid##_l_col_start, ov_##cid##_rhs, ov_##cid##_jac, ov_##cid##_mass, ov_##cid##_imass},
 static const net_entry g_entries[] = {
 #include "../odevec_b200/csrc/gen/registry.inc"
 };
@@ -1007,3 +1008,33 @@ const char* ov_oracle_net_tag(int i) { return (i >= 0 && i < g_nnets) ? g_entrie
 double ov_oracle_exp(double x) { return ov_exp(x); }
 double ov_oracle_log(double x) { return ov_log(x); }
 double ov_oracle_pow(double x, double y) { return ov_pow(x, y); }
+
+/* krome_x2n / krome_n2x of the reference's PRIMORDIAL driver
+   (tests/primordial.f90:117-140): direction 0, n = rhogas * x * imass;
+   direction 1, x = n * mass / rhogas; entries without a mass are copied.
+   Returns -1 for an unknown network, -5 for one without masses. */
+int ov_oracle_convert(const char* tag, int64_t ncells, int direction, const double* in, double* out,
+                      const double* rho)
+{
+    if (!net_find(tag))
+        return -1;
+    const net_entry* e = NULL;
+    for (int i = 0; i < NNETS; ++i)
+        if (strcmp(g_entries[i].tag, tag) == 0)
+            e = &g_entries[i];
+    const int n = e->sizes[0];
+    int any = 0;
+    for (int j = 0; j < n; ++j)
+        any |= e->mass[j] != 0.0;
+    if (!any)
+        return -5;
+    for (int j = 0; j < n; ++j)
+        for (int64_t c = 0; c < ncells; ++c) {
+            const double v = in[(size_t)j * ncells + c];
+            double o = v;
+            if (e->mass[j] != 0.0)
+                o = direction == 0 ? rho[c] * v * e->imass[j] : v * e->mass[j] / rho[c];
+            out[(size_t)j * ncells + c] = o;
+        }
+    return 0;
+}

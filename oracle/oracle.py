@@ -37,6 +37,8 @@ def lib():
             getattr(L, f).restype = d
         L.ov_oracle_pow.argtypes = [d, d]
         L.ov_oracle_pow.restype = d
+        L.ov_oracle_convert.argtypes = [ctypes.c_char_p, i64, i32, P, P, P]
+        L.ov_oracle_convert.restype = i32
         _lib = L
     return _lib
 
@@ -110,3 +112,41 @@ def workspace(tag, ncells, group=1):
     if n < 0:
         raise ValueError("bad workspace request")
     return np.zeros(n, np.float64)
+
+
+def convert(tag, a, rho, direction):
+    """Mass fractions -> number densities (direction 0) or back (1),
+    tests/primordial.f90:117-140; a: (neq, ncells)."""
+    a = np.ascontiguousarray(a, dtype=np.float64)
+    rho = np.ascontiguousarray(rho, dtype=np.float64)
+    out = np.empty_like(a)
+    rc = lib().ov_oracle_convert(tag.encode(), a.shape[1], direction, _p(a), _p(out), _p(rho))
+    if rc:
+        raise ValueError("convert(%s): code %d" % (tag, rc))
+    return out
+
+
+def ladder(tag, y, time, dt, t_stops, rtol, atol, dt_min, rho=None, dt_reset=None, group=1,
+           nthreads=0):
+    """The reference drivers' loop (tests/rober.f90:57-62, tests/orego.f90:
+    117-123, tests/primordial.f90:76-92): one SolveODE per entry of t_stops,
+    time and dt carried from call to call (dt set to dt_reset before each
+    call when given), and, with rho, the state kept as mass fractions and
+    converted to number densities around each call.  Where the reference
+    stops the program, a failed cell here keeps its first status and is
+    masked out of the later calls.  Returns (y, time, dt, status)."""
+    y = np.array(y, dtype=np.float64)
+    ncells = y.shape[1]
+    t = np.broadcast_to(np.asarray(time, dtype=np.float64), (ncells,)).copy()
+    d = np.broadcast_to(np.asarray(dt, dtype=np.float64), (ncells,)).copy()
+    failed = np.zeros(ncells, np.int32)
+    for k, ts in enumerate(t_stops):
+        if dt_reset is not None:
+            d[:] = dt_reset
+        n = convert(tag, y, rho, 0) if rho is not None else y
+        mask = None if k == 0 else (failed == 0).astype(np.uint8)
+        n, t, d, st, _ = solve(tag, n, t, d, np.full(ncells, ts), rtol, atol, dt_min, group=group,
+                               mask=mask, nthreads=nthreads)
+        failed = np.where(failed != 0, failed, st).astype(np.int32)
+        y = convert(tag, n, rho, 1) if rho is not None else n
+    return y, t, d, failed
