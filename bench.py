@@ -42,7 +42,9 @@ def parse():
     p.add_argument("--impl", default="product", choices=["product", "reference"])
     p.add_argument("--ncells", type=int, default=1048576)
     p.add_argument("--network", default="PRIMORDIAL_CSC_FF")
-    p.add_argument("--forms", default="fp32_lu,fp64,fp64_fma")
+    p.add_argument("--forms", default="fp32_lu,fp64,fp64_fma,plain_fp64",
+                   help="fp32_lu | fp64 | fp64_fma | plain_fp64 (FP64, one cell per thread for the "
+                        "whole launch, Jacobian and step-size blocks run where a cell needs them)")
     p.add_argument("--cpu-sample", type=int, default=65536)
     p.add_argument("--accuracy-cells", type=int, default=256)
     p.add_argument("--no-cpu", action="store_true")
@@ -219,8 +221,16 @@ def run_product(args):
     res = {}
     clocks = None
     for form in forms:
+        kw = {}
+        if form == "plain_fp64":
+            # the reference's loop structure ported one thread per cell: a grid
+            # of one cell per thread (no refill from the work queue), every
+            # Jacobian and step-size block run at once by the lanes that need
+            # it (no batching), two 128-thread blocks per SM
+            kw = dict(jac_batch=1, ss_batch=1, max_wait=-1, staging=1, grid_blocks=(N + 127) // 128)
         ode = S.Odevec(wl.network, max_cells=N, RelativeTolerance=wl.rtol, AbsoluteTolerance=wl.atol,
-                       MinimalTimestep=wl.dt_min, nvector=1, precision=form, raise_on_failure=False)
+                       MinimalTimestep=wl.dt_min, nvector=1, precision="fp64" if form == "plain_fp64" else form,
+                       raise_on_failure=False, **kw)
         S.InitOdevec(ode)
 
         def reset():
@@ -346,6 +356,8 @@ def run_product(args):
     }
     if "fp64" in res and "fp32_lu" in res:
         line["fp32lu_over_fp64"] = res["fp32_lu"]["value"] / res["fp64"]["value"]
+    if "plain_fp64" in res and "fp32_lu" in res:
+        line["fp32lu_over_plain_fp64"] = res["fp32_lu"]["value"] / res["plain_fp64"]["value"]
     if world == 1 and not args.no_cpu:
         threads = host_threads()
         v, el, f = oracle_rate(W.primordial(ncells=args.cpu_sample, seed=3, network=args.network),
@@ -371,7 +383,9 @@ def accuracy(args, wl, S, torch):
                                1e-26, wl.dt_min, group=1, nthreads=host_threads(), fix_restart=True)
     out = {"oracle_rtol": 1e-12, "oracle_fix_restart": True, "cells": n,
            "oracle_failures": int((st != 0).sum())}
-    runs = [(f, False) for f in args.forms.split(",")] + [("fp32_lu", True), ("fp64", True)]
+    # plain_fp64 schedules the fp64 form differently; its results are the same
+    runs = [(f, False) for f in args.forms.split(",") if f != "plain_fp64"] + [("fp32_lu", True),
+                                                                            ("fp64", True)]
     got = {}
     for form, fix in runs:
         ode = S.Odevec(wl.network, RelativeTolerance=wl.rtol, AbsoluteTolerance=wl.atol,

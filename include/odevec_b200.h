@@ -89,10 +89,8 @@ typedef struct odevec_opts {
        local memory, 2 blocks of 128 threads per SM; 2 = history and LU in
        shared memory, 1 block of 128 (where they fit); 3, 4 = as 1 with 3 or 4
        blocks per SM (fewer registers, more warps); 5 = as 2 with 192-thread
-       blocks (FP32 LU); 6 = as 1 with one block of 384 threads per SM whose
-       warps move in step (a barrier per trip, Jacobian and step-size blocks
-       decided for the whole block, batch thresholds scaled by its 12 warps;
-       per-cell control only).  block_threads (a multiple of 32 up to the block of
+       blocks (FP32 LU); 6 = as 3 in one block of 384 threads per SM
+       (per-cell control only).  block_threads (a multiple of 32 up to the block of
        the staging) and grid_blocks: 0 = automatic (persistent grid filling
        every SM) */
     int32_t staging;

@@ -156,16 +156,13 @@ struct LaneHist {
    budget; SHM places the Nordsieck history and the LU in shared memory. */
 template <int STAGE>
 struct StageCfg;
-template <> struct StageCfg<1> { static constexpr bool SHM = false, SYNC = false; static constexpr int BS = 128, MINB = 2; };
-template <> struct StageCfg<2> { static constexpr bool SHM = true,  SYNC = false; static constexpr int BS = 128, MINB = 1; };
-template <> struct StageCfg<3> { static constexpr bool SHM = false, SYNC = false; static constexpr int BS = 128, MINB = 3; };
-template <> struct StageCfg<4> { static constexpr bool SHM = false, SYNC = false; static constexpr int BS = 128, MINB = 4; };
-template <> struct StageCfg<5> { static constexpr bool SHM = true,  SYNC = false; static constexpr int BS = 192, MINB = 1; };
-/* one block of 12 warps per SM that moves in step: a barrier opens every
-   trip of the cell loop and the Jacobian and step-size blocks are decided
-   for the whole block, so the warps on a scheduler run the same code at the
-   same time (instruction-cache reuse) */
-template <> struct StageCfg<6> { static constexpr bool SHM = false, SYNC = true;  static constexpr int BS = 384, MINB = 1; };
+template <> struct StageCfg<1> { static constexpr bool SHM = false; static constexpr int BS = 128, MINB = 2; };
+template <> struct StageCfg<2> { static constexpr bool SHM = true;  static constexpr int BS = 128, MINB = 1; };
+template <> struct StageCfg<3> { static constexpr bool SHM = false; static constexpr int BS = 128, MINB = 3; };
+template <> struct StageCfg<4> { static constexpr bool SHM = false; static constexpr int BS = 128, MINB = 4; };
+template <> struct StageCfg<5> { static constexpr bool SHM = true;  static constexpr int BS = 192, MINB = 1; };
+/* as 3, the same register budget, in one block of 384 threads per SM */
+template <> struct StageCfg<6> { static constexpr bool SHM = false; static constexpr int BS = 384, MINB = 1; };
 
 template <class Net, class LUT, bool SHM, int BS>
 struct Staging;
@@ -678,44 +675,6 @@ struct Cell {
 /* number of lanes of the warp for which b holds */
 __device__ __forceinline__ int warp_count(bool b) { return __popc(__ballot_sync(FULL, b)); }
 
-/* Block-wide votes for the block-synchronous staging.  The cell loop's
-   phases leave the lanes of a warp on different paths, so each vote first
-   reconverges the warp and then uses the non-aligned barrier forms, which
-   PTX defines for threads that arrive from divergent code (the aligned
-   forms behind __syncthreads_count/_and/_or assume a converged warp).
-   Every thread of the block executes every vote once per trip. */
-__device__ __forceinline__ int block_count(bool b)
-{
-    __syncwarp();
-    int r;
-    asm volatile("{\n\t.reg .pred p;\n\tsetp.ne.u32 p, %1, 0;\n\tbarrier.red.popc.u32 %0, 0, p;\n\t}"
-                 : "=r"(r)
-                 : "r"((unsigned)b)
-                 : "memory");
-    return r;
-}
-__device__ __forceinline__ bool block_and(bool b)
-{
-    __syncwarp();
-    unsigned r;
-    asm volatile("{\n\t.reg .pred p, q;\n\tsetp.ne.u32 p, %1, 0;\n\tbarrier.red.and.pred q, 0, p;\n\t"
-                 "selp.u32 %0, 1, 0, q;\n\t}"
-                 : "=r"(r)
-                 : "r"((unsigned)b)
-                 : "memory");
-    return r != 0;
-}
-__device__ __forceinline__ bool block_or(bool b)
-{
-    __syncwarp();
-    unsigned r;
-    asm volatile("{\n\t.reg .pred p, q;\n\tsetp.ne.u32 p, %1, 0;\n\tbarrier.red.or.pred q, 0, p;\n\t"
-                 "selp.u32 %0, 1, 0, q;\n\t}"
-                 : "=r"(r)
-                 : "r"((unsigned)b)
-                 : "memory");
-    return r != 0;
-}
 
 template <class Net, int G, class LUT, int STAGE>
 __global__ void __launch_bounds__(StageCfg<STAGE>::BS, StageCfg<STAGE>::MINB) bdf_kernel(const LaunchArgs A)
@@ -762,14 +721,8 @@ __global__ void __launch_bounds__(StageCfg<STAGE>::BS, StageCfg<STAGE>::MINB) bd
                     ph = cell < ncells ? PH_START : PH_EXHAUSTED;
                 }
             }
-            if constexpr (StageCfg<STAGE>::SYNC) {
-                /* every thread of the block reaches this barrier once per trip */
-                if (block_and(ph == PH_EXHAUSTED))
-                    break;
-            } else {
-                if (__all_sync(FULL, ph == PH_EXHAUSTED))
-                    break;
-            }
+            if (__all_sync(FULL, ph == PH_EXHAUSTED))
+                break;
         } else {
             if (ph == PH_IDLE) { /* warp-uniform */
                 unsigned long long g = 0;
@@ -899,19 +852,10 @@ __global__ void __launch_bounds__(StageCfg<STAGE>::BS, StageCfg<STAGE>::MINB) bd
         {
             bool run;
             if (G == 1) {
-                const bool mv = ph == PH_NEWTON || ph == PH_START || ph == PH_RESTART;
-                const bool old = ph == PH_JACWAIT && c.wait >= A.max_wait;
-                if constexpr (StageCfg<STAGE>::SYNC) {
-                    const int waiting = block_count(ph == PH_JACWAIT);
-                    const int moving = block_count(mv);
-                    const bool aged = block_or(old);
-                    run = waiting > 0 && (waiting >= A.jac_batch * (BS / 32) || moving == 0 || aged);
-                } else {
-                    const int waiting = warp_count(ph == PH_JACWAIT);
-                    const int moving = warp_count(mv);
-                    const bool aged = __any_sync(FULL, old);
-                    run = waiting > 0 && (waiting >= A.jac_batch || moving == 0 || aged);
-                }
+                const int waiting = warp_count(ph == PH_JACWAIT);
+                const int moving = warp_count(ph == PH_NEWTON || ph == PH_START || ph == PH_RESTART);
+                const bool aged = __any_sync(FULL, ph == PH_JACWAIT && c.wait >= A.max_wait);
+                run = waiting > 0 && (waiting >= A.jac_batch || moving == 0 || aged);
             } else {
                 run = ph == PH_JACWAIT;
             }
@@ -1039,19 +983,10 @@ __global__ void __launch_bounds__(StageCfg<STAGE>::BS, StageCfg<STAGE>::MINB) bd
         {
             bool run;
             if (G == 1) {
-                const bool mv = ph == PH_PRED || ph == PH_NEWTON || ph == PH_RESTART;
-                const bool old = ph == PH_SSWAIT && c.wait >= A.max_wait;
-                if constexpr (StageCfg<STAGE>::SYNC) {
-                    const int waiting = block_count(ph == PH_SSWAIT);
-                    const int moving = block_count(mv);
-                    const bool aged = block_or(old);
-                    run = waiting > 0 && (waiting >= A.ss_batch * (BS / 32) || moving == 0 || aged);
-                } else {
-                    const int waiting = warp_count(ph == PH_SSWAIT);
-                    const int moving = warp_count(mv);
-                    const bool aged = __any_sync(FULL, old);
-                    run = waiting > 0 && (waiting >= A.ss_batch || moving == 0 || aged);
-                }
+                const int waiting = warp_count(ph == PH_SSWAIT);
+                const int moving = warp_count(ph == PH_PRED || ph == PH_NEWTON || ph == PH_RESTART);
+                const bool aged = __any_sync(FULL, ph == PH_SSWAIT && c.wait >= A.max_wait);
+                run = waiting > 0 && (waiting >= A.ss_batch || moving == 0 || aged);
             } else {
                 run = ph == PH_SSWAIT;
             }
@@ -1111,7 +1046,7 @@ cudaError_t launch(const LaunchArgs& a, int block, int grid, cudaStream_t stream
     using Cfg = StageCfg<STAGE>;
     auto kern = bdf_kernel<Net, G, LUT, STAGE>;
     constexpr size_t smem = Staging<Net, LUT, Cfg::SHM, Cfg::BS>::smem_bytes;
-    if (Cfg::SHM || Cfg::SYNC || block <= 0 || block > Cfg::BS)
+    if (Cfg::SHM || block <= 0 || block > Cfg::BS)
         block = Cfg::BS;
     static int cached_grid[2] = {0, 0};
     if (cached_grid[0] == 0 || cached_grid[1] != block) {

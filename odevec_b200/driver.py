@@ -76,7 +76,7 @@ class Ladder:
                  dt_reset: Optional[float] = None, graph: bool = False, chunk: int = 64):
         import torch
         self.torch = torch
-        if ode.handle is None:
+        if ode._h is None:
             raise ValueError("InitOdevec first")
         if not (torch.is_tensor(y) and y.is_cuda and y.dtype == torch.float64 and y.is_contiguous()):
             raise ValueError("y must be a contiguous float64 CUDA tensor")

@@ -129,7 +129,7 @@ class Odevec:
                  precision: str = "fp64", max_attempts: int = 0, raise_on_failure: bool = True,
                  jac_batch: int = 0, ss_batch: int = 0, max_wait: int = 0, staging: int = 0,
                  block_threads: int = 0, grid_blocks: int = 0, fix_restart: bool = False,
-                 escalation: bool = True):
+                 escalation: bool = True, autotune: bool = True):
         info = network_info(network)
         self.network = network
         self.neq = info["neq"]
@@ -153,6 +153,9 @@ class Odevec:
         self.grid_blocks = grid_blocks
         self.fix_restart = fix_restart
         self.escalation = escalation
+        # launch options left at 0 are taken from the autotuner's table at
+        # InitOdevec (odevec_b200/autotune.py); they never change results
+        self.autotune = autotune
         self.status = None
         self.stats = None
         self._h = None
@@ -191,6 +194,9 @@ def InitOdevec(ode: Odevec) -> Odevec:
     if not torch.cuda.is_available():
         raise OdevecError("odevec_b200 needs a CUDA GPU; none is visible")
     torch.cuda.init()
+    if ode.autotune:
+        from . import autotune
+        autotune.apply(ode)
     h = ctypes.c_void_p()
     o = ode._opts()
     _check(lib().odevec_init(ode.network.encode(), ode.max_cells, ctypes.byref(o), ctypes.byref(h)))
