@@ -320,3 +320,29 @@ def test_fp32_escalation_rescues_badly_conditioned_cells(gpu_lib):
         gpu_lib.CloseOdevec(ode)
     assert res[("fp32_lu", True)][0] == 0
     assert res[("fp64_fma", True)][0] == 0
+
+
+@pytest.mark.parametrize("ncells", [1, 31, 33, 65, 129])
+def test_ragged_sizes_bit_exact(gpu_lib, oracle, ncells):
+    # cell counts that leave a warp, a block and the persistent grid partly empty
+    wl = W.primordial(ncells=ncells, seed=ncells)
+    for staging in (3, 6):
+        g = run_gpu(gpu_lib, wl, "fp64", staging=staging)
+        assert_bitwise(g, run_oracle(oracle, wl), "ncells %d staging %d" % (ncells, staging))
+
+
+def test_empty_and_group_size_errors(gpu_lib):
+    import torch
+    S = gpu_lib
+    wl = W.rober(ncells=64)
+    ode = S.Odevec(wl.network, nvector=32, raise_on_failure=False)
+    S.InitOdevec(ode)
+    try:
+        y = torch.empty((3, 0), dtype=torch.float64, device="cuda")
+        z = torch.empty(0, dtype=torch.float64, device="cuda")
+        S.SolveODE(ode, z, z.clone(), z.clone(), y)  # nothing to do, no launch
+        y = torch.tensor(wl.y[:, :33], device="cuda")
+        with pytest.raises(S.OdevecError, match="divisible by 32"):
+            S.SolveODE(ode, 0.0, 1e-10, 1e5, y)
+    finally:
+        S.CloseOdevec(ode)
