@@ -4,12 +4,12 @@ What it chooses, per network variant, precision form and GPU model:
 
 * the staging -- where a cell's Nordsieck history and LU live (thread-local
   arrays in registers / local memory, or shared memory), the block size
-  (cells per block: 128, 192 or 384 threads) and the blocks per SM;
+  (cells per block: 128, 192 or 384 threads) and the blocks per SM, or one
+  warp per cell (staging 7, for the variants that have its tables);
 * the batching of the Jacobian and step-size blocks (jac_batch, ss_batch,
   max_wait).
 
-A cell is always integrated by one thread.  None of these settings changes
-a result (every cell runs the same operations whatever the interleaving;
+None of these settings changes a result (every cell runs the same operations whatever the interleaving;
 the GPU parity tests check this bit for bit), so tuning only moves time.
 
 The search is coordinate-wise on a timed sample of the caller's cells:
@@ -28,7 +28,7 @@ from typing import Callable, Dict, List, Optional, Tuple
 HERE = os.path.dirname(os.path.abspath(__file__))
 TABLE = os.path.join(HERE, "tuning.json")
 
-STAGINGS = (1, 2, 3, 4, 6)
+STAGINGS = (1, 2, 3, 4, 6, 7)
 FP32_STAGINGS = (5,)
 BATCHES = ((24, 24, 8), (16, 16, 4), (32, 32, 16), (8, 8, 4), (1, 1, -1))
 FIELDS = ("staging", "jac_batch", "ss_batch", "max_wait")

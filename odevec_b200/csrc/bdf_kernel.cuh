@@ -1086,11 +1086,15 @@ constexpr bool shm_fits()
 }  // namespace OV_MODE_NS
 }  // namespace ov
 
+#include "wpc_kernel.cuh"
+
 /* Defines the launcher of one network variant in the current mode.
    stage: 1 = thread-local arrays, 2 blocks of 128 per SM; 2 = history and
    LU in shared memory, 1 block of 128; 3, 4 = thread-local, 3 or 4 blocks of
-   128 (fewer registers, more warps); 5 = shared memory, 1 block of 192.
-   Stages 2-5 exist for per-cell control (G = 1). */
+   128 (fewer registers, more warps); 5 = shared memory, 1 block of 192;
+   6 = thread-local, 1 block of 384; 7 = one warp per cell (wpc_kernel.cuh;
+   constant-coefficient CSC variants).  Stages 2-7 exist for per-cell
+   control (G = 1). */
 #define OV_STAGE_CASE(NET, LU, ST)                                                               \
     if (stage == ST)                                                                             \
         return launch<NET, 1, LU, ST>(a, block, grid, s);
@@ -1107,6 +1111,10 @@ constexpr bool shm_fits()
             OV_STAGE_CASE(NET, double, 3)                                                        \
             OV_STAGE_CASE(NET, double, 4)                                                        \
             OV_STAGE_CASE(NET, double, 6)                                                        \
+            if constexpr (wpc_ok<NET, double>()) {                                               \
+                if (stage == 7)                                                                  \
+                    return launch_wpc<NET, double>(a, grid, s);                                  \
+            }                                                                                    \
             if constexpr (shm_fits<NET, double, 128>()) {                                        \
                 OV_STAGE_CASE(NET, double, 2)                                                    \
             }                                                                                    \
@@ -1118,6 +1126,10 @@ constexpr bool shm_fits()
                 OV_STAGE_CASE(NET, float, 3)                                                     \
                 OV_STAGE_CASE(NET, float, 4)                                                     \
                 OV_STAGE_CASE(NET, float, 6)                                                     \
+                if constexpr (wpc_ok<NET, float>()) {                                            \
+                    if (stage == 7)                                                              \
+                        return launch_wpc<NET, float>(a, grid, s);                               \
+                }                                                                                \
                 if constexpr (shm_fits<NET, float, 128>()) {                                     \
                     OV_STAGE_CASE(NET, float, 2)                                                 \
                 }                                                                                \

@@ -4,7 +4,65 @@
 #pragma once
 #include "net_orego_csc_cmk.h"
 
+
+/* warp-per-cell tables (odevec_b200/wpc.py) */
+static __device__ const int ov_wpc_orego_csc_cmk_rhs_ptr[4] = {
+    0, 4, 7, 9};
+static __device__ const double ov_wpc_orego_csc_cmk_rhs_coef[9] = {
+    -0.00064713625, -77.27, 77.27, 77.27,
+    -0.0129416332341141, -0.0129416332341141, 0.0129416332341141, 0.161,
+    -0.161};
+static __device__ const int ov_wpc_orego_csc_cmk_rhs_fac[27] = {
+    1, -1, -1, 0, 2, -1, 0, -1, -1, 2, -1, -1, 0, 2, -1, 2,
+    -1, -1, 4, -1, -1, 0, -1, -1, 4, -1, -1};
+static __device__ const int ov_wpc_orego_csc_cmk_jac_ptr[8] = {
+    0, 7, 13, 26, 36, 42, 49, 66};
+static __device__ const int ov_wpc_orego_csc_cmk_jac_code[66] = {
+    0, 2, 7, 3, 7, 16, 5, 32, 4, 2, 7, 3, 7, 2, 4, 3,
+    7, 48, 4, 1, 7, 64, 6, 7, 80, 5, 2, 4, 3, 7, 96, 112,
+    1, 7, 6, 7, 128, 4, 2, 7, 3, 7, 144, 2, 7, 3, 7, 17,
+    7, 2, 4, 3, 7, 160, 4, 1, 7, 176, 17, 7, 6, 192, 5, 7,
+    208, 5};
+static __device__ const double ov_wpc_orego_csc_cmk_jac_const[14] = {
+    0.161, 1.0, 0.0129416332341141, 0.0129416332341141,
+    0.0129416332341141, 1.0, 77.27, 77.27,
+    0.161, 0.0129416332341141, 0.0012942725, 77.27,
+    77.27, 1.0};
+static __device__ const int ov_wpc_orego_csc_cmk_jac_rc[7] = {
+    131074, 131073, 65537, 65536, 2, 1, 0};
+static __device__ const int ov_wpc_orego_csc_cmk_fac_lptr[5] = {
+    0, 1, 2, 3, 4};
+static __device__ const long long ov_wpc_orego_csc_cmk_fac_op[4] = {
+    2305840810190438408LL, 2199031644171LL, 2305840810194632714LL, 6597080252429LL};
+static __device__ const int ov_wpc_orego_csc_cmk_sol_lptr[7] = {
+    0, 1, 2, 3, 4, 5, 7};
+static __device__ const long long ov_wpc_orego_csc_cmk_sol_op[7] = {
+    2199021158400LL, 2199023255555LL, 6597067669506LL, 6597071863813LL, 15393160691716LL, 8796097216513LL, 10995120472067LL};
+static __device__ const int ov_wpc_orego_csc_cmk_srow[3] = {
+    2, 1, 0};
+static __device__ const int ov_wpc_orego_csc_cmk_dyn[3] = {
+    0, 1, 2};
+struct ov_wpc_orego_csc_cmk {
+  static constexpr int NTERM = 9, NPROG = 7, DEPTH = 4, NFL = 4, NSL = 6;
+  __device__ static const int* rhs_ptr() { return ov_wpc_orego_csc_cmk_rhs_ptr; }
+  __device__ static const int* rhs_fac() { return ov_wpc_orego_csc_cmk_rhs_fac; }
+  __device__ static const int* jac_ptr() { return ov_wpc_orego_csc_cmk_jac_ptr; }
+  __device__ static const int* jac_code() { return ov_wpc_orego_csc_cmk_jac_code; }
+  __device__ static const int* jac_rc() { return ov_wpc_orego_csc_cmk_jac_rc; }
+  __device__ static const int* fac_lptr() { return ov_wpc_orego_csc_cmk_fac_lptr; }
+  __device__ static const int* sol_lptr() { return ov_wpc_orego_csc_cmk_sol_lptr; }
+  __device__ static const int* srow() { return ov_wpc_orego_csc_cmk_srow; }
+  __device__ static const int* dyn() { return ov_wpc_orego_csc_cmk_dyn; }
+  __device__ static const double* rhs_coef() { return ov_wpc_orego_csc_cmk_rhs_coef; }
+  __device__ static const double* jac_const() { return ov_wpc_orego_csc_cmk_jac_const; }
+  __device__ static const long long* fac_op() { return ov_wpc_orego_csc_cmk_fac_op; }
+  __device__ static const long long* sol_op() { return ov_wpc_orego_csc_cmk_sol_op; }
+};
+
 struct ov_net_orego_csc_cmk {
+  /* warp-per-cell tables (staging 7) */
+  static constexpr bool HAS_WPC = true;
+  using Wpc = ov_wpc_orego_csc_cmk;
   static constexpr int NEQ = 3;   /* all species (state vector) */
   static constexpr int ND = 3;    /* species in the solver state */
   static constexpr int NNZ = 7;   /* packed LU entries of the dynamic block */

@@ -14,7 +14,7 @@
 #define OV_OREGO_CSC_CMK_NVECTOR 1
 #define OV_OREGO_CSC_CMK_DT_MIN 1e-10
 #define OV_OREGO_CSC_CMK_IDX_TGAS -1
-static const int ov_orego_csc_cmk_sizes[7] = {3, 7, 0, 0, -1, 3, 1};
+static const int ov_orego_csc_cmk_sizes[8] = {3, 7, 0, 0, -1, 3, 1, 1};
 static const double ov_orego_csc_cmk_defaults[2] = {1.0, 1e-10}; /* nvector, dt_min */
 static const double ov_orego_csc_cmk_mass[3] = {0.0, 0.0, 0.0};
 static const double ov_orego_csc_cmk_imass[3] = {0.0, 0.0, 0.0};

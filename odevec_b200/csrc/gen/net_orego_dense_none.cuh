@@ -5,6 +5,8 @@
 #include "net_orego_dense_none.h"
 
 struct ov_net_orego_dense_none {
+  static constexpr bool HAS_WPC = false;
+  using Wpc = void;
   static constexpr int NEQ = 3;   /* all species (state vector) */
   static constexpr int ND = 3;    /* species in the solver state */
   static constexpr int NNZ = 8;   /* packed LU entries of the dynamic block */

@@ -14,7 +14,7 @@
 #define OV_PRIMORDIAL_DENSE_NONE_LU3_NVECTOR 1
 #define OV_PRIMORDIAL_DENSE_NONE_LU3_DT_MIN 1e-20
 #define OV_PRIMORDIAL_DENSE_NONE_LU3_IDX_TGAS 14
-static const int ov_primordial_dense_none_lu3_sizes[7] = {16, 148, 38, 1, 14, 12, 3};
+static const int ov_primordial_dense_none_lu3_sizes[8] = {16, 148, 38, 1, 14, 12, 3, 0};
 static const double ov_primordial_dense_none_lu3_defaults[2] = {1.0, 1e-20}; /* nvector, dt_min */
 static const double ov_primordial_dense_none_lu3_mass[16] = {9.10938188e-28, 1.67444345638e-24, 1.67353251819e-24, 6.69206503638e-24, 3.34706503638e-24, 3.34603251819e-24, 5.01956503638e-24, 1.67262158e-24, 6.69115409819e-24, 3.34615409819e-24, 3.34512158e-24, 6.69024316e-24, 0.0, 0.0, 0.0, 0.0};
 static const double ov_primordial_dense_none_lu3_imass[16] = {1.09776932527e+27, 5.9721335838e+23, 5.97538433901e+23, 1.49430705554e+23, 2.9876921695e+23, 2.98861411108e+23, 1.99220448934e+23, 5.97863863505e+23, 1.4945104915e+23, 2.98850552203e+23, 2.98942796572e+23, 1.49471398286e+23, 0.0, 0.0, 0.0, 0.0};

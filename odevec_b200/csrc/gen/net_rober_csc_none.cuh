@@ -4,7 +4,62 @@
 #pragma once
 #include "net_rober_csc_none.h"
 
+
+/* warp-per-cell tables (odevec_b200/wpc.py) */
+static __device__ const int ov_wpc_rober_csc_none_rhs_ptr[4] = {
+    0, 2, 5, 6};
+static __device__ const double ov_wpc_rober_csc_none_rhs_coef[6] = {
+    -0.04, 10000.0, 0.04, -30000000.0,
+    -10000.0, 30000000.0};
+static __device__ const int ov_wpc_rober_csc_none_rhs_fac[18] = {
+    0, -1, -1, 2, 4, -1, 0, -1, -1, 3, -1, -1, 2, 4, -1, 3,
+    -1, -1};
+static __device__ const int ov_wpc_rober_csc_none_jac_ptr[9] = {
+    0, 7, 13, 21, 36, 44, 52, 59, 60};
+static __device__ const int ov_wpc_rober_csc_none_jac_code[60] = {
+    0, 2, 7, 3, 7, 16, 5, 32, 4, 2, 7, 3, 7, 48, 4, 2,
+    7, 3, 7, 33, 7, 2, 4, 3, 7, 64, 4, 17, 7, 80, 33, 7,
+    6, 7, 96, 5, 112, 4, 2, 7, 3, 7, 17, 7, 128, 4, 2, 7,
+    3, 7, 17, 7, 144, 2, 7, 3, 7, 17, 7, 160};
+static __device__ const double ov_wpc_rober_csc_none_jac_const[11] = {
+    0.04, 1.0, 0.04, 10000.0,
+    60000000.0, 10000.0, 1.0, 60000000.0,
+    10000.0, 10000.0, 1.0};
+static __device__ const int ov_wpc_rober_csc_none_jac_rc[8] = {
+    0, 1, 65536, 65537, 65538, 131072, 131073, 131074};
+static __device__ const int ov_wpc_rober_csc_none_fac_lptr[5] = {
+    0, 2, 4, 5, 6};
+static __device__ const long long ov_wpc_rober_csc_none_fac_op[6] = {
+    2305840810190438404LL, 2305840810190438410LL, 2199027449863LL, 2199033741325LL, 2305840810196729868LL, 8796105605135LL};
+static __device__ const int ov_wpc_rober_csc_none_sol_lptr[8] = {
+    0, 1, 2, 3, 4, 5, 7, 8};
+static __device__ const long long ov_wpc_rober_csc_none_sol_op[8] = {
+    2199021158400LL, 2199023255555LL, 8796090925058LL, 8796095119365LL, 17592183947268LL, 10995120472065LL, 13194143727619LL, 4398048608257LL};
+static __device__ const int ov_wpc_rober_csc_none_srow[3] = {
+    0, 1, 2};
+static __device__ const int ov_wpc_rober_csc_none_dyn[3] = {
+    0, 1, 2};
+struct ov_wpc_rober_csc_none {
+  static constexpr int NTERM = 6, NPROG = 8, DEPTH = 4, NFL = 4, NSL = 7;
+  __device__ static const int* rhs_ptr() { return ov_wpc_rober_csc_none_rhs_ptr; }
+  __device__ static const int* rhs_fac() { return ov_wpc_rober_csc_none_rhs_fac; }
+  __device__ static const int* jac_ptr() { return ov_wpc_rober_csc_none_jac_ptr; }
+  __device__ static const int* jac_code() { return ov_wpc_rober_csc_none_jac_code; }
+  __device__ static const int* jac_rc() { return ov_wpc_rober_csc_none_jac_rc; }
+  __device__ static const int* fac_lptr() { return ov_wpc_rober_csc_none_fac_lptr; }
+  __device__ static const int* sol_lptr() { return ov_wpc_rober_csc_none_sol_lptr; }
+  __device__ static const int* srow() { return ov_wpc_rober_csc_none_srow; }
+  __device__ static const int* dyn() { return ov_wpc_rober_csc_none_dyn; }
+  __device__ static const double* rhs_coef() { return ov_wpc_rober_csc_none_rhs_coef; }
+  __device__ static const double* jac_const() { return ov_wpc_rober_csc_none_jac_const; }
+  __device__ static const long long* fac_op() { return ov_wpc_rober_csc_none_fac_op; }
+  __device__ static const long long* sol_op() { return ov_wpc_rober_csc_none_sol_op; }
+};
+
 struct ov_net_rober_csc_none {
+  /* warp-per-cell tables (staging 7) */
+  static constexpr bool HAS_WPC = true;
+  using Wpc = ov_wpc_rober_csc_none;
   static constexpr int NEQ = 3;   /* all species (state vector) */
   static constexpr int ND = 3;    /* species in the solver state */
   static constexpr int NNZ = 8;   /* packed LU entries of the dynamic block */

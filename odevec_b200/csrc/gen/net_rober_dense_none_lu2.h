@@ -14,7 +14,7 @@
 #define OV_ROBER_DENSE_NONE_LU2_NVECTOR 32
 #define OV_ROBER_DENSE_NONE_LU2_DT_MIN 1e-20
 #define OV_ROBER_DENSE_NONE_LU2_IDX_TGAS -1
-static const int ov_rober_dense_none_lu2_sizes[7] = {3, 8, 0, 1, -1, 3, 2};
+static const int ov_rober_dense_none_lu2_sizes[8] = {3, 8, 0, 1, -1, 3, 2, 0};
 static const double ov_rober_dense_none_lu2_defaults[2] = {32.0, 1e-20}; /* nvector, dt_min */
 static const double ov_rober_dense_none_lu2_mass[3] = {0.0, 0.0, 0.0};
 static const double ov_rober_dense_none_lu2_imass[3] = {0.0, 0.0, 0.0};

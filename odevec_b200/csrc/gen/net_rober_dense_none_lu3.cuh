@@ -5,6 +5,8 @@
 #include "net_rober_dense_none_lu3.h"
 
 struct ov_net_rober_dense_none_lu3 {
+  static constexpr bool HAS_WPC = false;
+  using Wpc = void;
   static constexpr int NEQ = 3;   /* all species (state vector) */
   static constexpr int ND = 3;    /* species in the solver state */
   static constexpr int NNZ = 9;   /* packed LU entries of the dynamic block */

@@ -13,7 +13,7 @@
 #define OV_ROBER_DENSE_NONE_LU3_NVECTOR 32
 #define OV_ROBER_DENSE_NONE_LU3_DT_MIN 1e-20
 #define OV_ROBER_DENSE_NONE_LU3_IDX_TGAS -1
-static const int ov_rober_dense_none_lu3_sizes[7] = {3, 9, 0, 1, -1, 3, 3};
+static const int ov_rober_dense_none_lu3_sizes[8] = {3, 9, 0, 1, -1, 3, 3, 0};
 static const double ov_rober_dense_none_lu3_defaults[2] = {32.0, 1e-20}; /* nvector, dt_min */
 static const double ov_rober_dense_none_lu3_mass[3] = {0.0, 0.0, 0.0};
 static const double ov_rober_dense_none_lu3_imass[3] = {0.0, 0.0, 0.0};

@@ -65,6 +65,18 @@ int32_t fail(int32_t code, const char* fmt, ...)
     return code;
 }
 
+/* automatic staging: one warp per cell for per-cell control of networks of
+   more than 32 solver-state species that have the tables, else thread-local
+   arrays with 3 blocks of 128 per SM (per-cell) or 2 (lockstep) */
+int auto_staging(const NetEntry& e, int group_size)
+{
+    if (group_size != 1)
+        return 1;
+    if (e.sizes[7] && e.sizes[5] > 32)
+        return 7;
+    return 3;
+}
+
 int find_net(const char* tag)
 {
     if (!tag)
@@ -174,8 +186,8 @@ static int32_t resolve_opts(const NetEntry& e, const odevec_opts* in, odevec_opt
         o.max_wait = o.max_wait < 0 ? 0 : 8;
     if (o.jac_batch > 32 || o.ss_batch > 32)
         return fail(OV_API_EINVAL, "jac_batch and ss_batch must be <= 32");
-    if (o.staging < 0 || o.staging > 6)
-        return fail(OV_API_EINVAL, "staging must be 0..6");
+    if (o.staging < 0 || o.staging > 7)
+        return fail(OV_API_EINVAL, "staging must be 0..7");
     if (o.block_threads < 0 || o.block_threads > 128 || o.block_threads % 32)
         return fail(OV_API_EINVAL, "block_threads must be 32, 64, 96 or 128 (0: automatic)");
     if (o.grid_blocks < 0)
@@ -341,7 +353,7 @@ static int32_t solve_impl(odevec_solver* s, int64_t ncells, double* y, double* t
     ov::launch_fn fn = o.precision == OV_PREC_FP64 ? e.exact : e.fma;
     /* automatic: thread-local arrays with 3 blocks of 128 per SM for per-cell
        control (the fastest measured configuration), 2 blocks for lockstep */
-    const int stage = o.staging ? o.staging : (o.group_size == 1 ? 3 : 1);
+    const int stage = o.staging ? o.staging : auto_staging(e, o.group_size);
     const bool escalate = lu && !o.no_escalation;
     const int neq = e.sizes[0];
     if (escalate) {
@@ -618,7 +630,7 @@ extern "C" int32_t odevec_solve_noalloc(const char* network, const odevec_opts* 
     const NetEntry& e = g_nets[ni];
     const int lu = o.precision == OV_PREC_FP32_LU ? 1 : 0;
     ov::launch_fn fn = o.precision == OV_PREC_FP64 ? e.exact : e.fma;
-    const int stage = o.staging ? o.staging : (o.group_size == 1 ? 3 : 1);
+    const int stage = o.staging ? o.staging : auto_staging(e, o.group_size);
     err = fn(a, o.group_size, lu, stage, o.block_threads, o.grid_blocks, st);
     if (err == cudaErrorNotSupported)
         return fail(OV_API_EUNSUPPORTED, "variant %s: group %d precision %d not compiled", e.tag,

@@ -381,9 +381,10 @@ def emit_c_header(sysm: System) -> str:
     def arr(name, vals):
         L.append("static const int ov_%s_%s[%d] = {%s};" % (cid, name, len(vals),
                                                           ", ".join(str(v) for v in vals)))
+    from . import wpc
     arr("sizes", [n, nnz, net.nrea if net.rates else 0, 1 if sysm.packaging == "DENSE" else 0,
                   net.idx_tgas if net.idx_tgas is not None else -1, n - len(frozen_species(sysm)),
-                  sysm.lu_method])
+                  sysm.lu_method, 1 if wpc.eligible(sysm) else 0])
     L.append("static const double ov_%s_defaults[2] = {%d.0, %r}; /* nvector, dt_min */"
              % (cid, sysm.nvector, float(sysm.dt_min)))
     # species masses (g) and inverse masses (1/g) for the mass-fraction format;
@@ -564,7 +565,18 @@ def emit_cuda_header(sysm: System) -> str:
     pos = sysm.pos()
     ymap = {sym: "y[%d]" % i for i, sym in enumerate(net.y)}
     pr = NetPrinter(ymap)
+    from . import wpc
+    has_wpc = wpc.eligible(sysm)
+    if has_wpc:
+        L.append(wpc.emit(sysm, cid))
     L.append("struct ov_net_%s {" % cid)
+    if has_wpc:
+        L.append("  /* warp-per-cell tables (staging 7) */")
+        L.append("  static constexpr bool HAS_WPC = true;")
+        L.append("  using Wpc = ov_wpc_%s;" % cid)
+    else:
+        L.append("  static constexpr bool HAS_WPC = false;")
+        L.append("  using Wpc = void;")
     L.append("  static constexpr int NEQ = %d;   /* all species (state vector) */" % n)
     L.append("  static constexpr int ND = %d;    /* species in the solver state */" % nd)
     L.append("  static constexpr int NNZ = %d;   /* packed LU entries of the dynamic block */" % len(kmap))

@@ -237,14 +237,14 @@ def test_syn64_mass_conservation(gpu_lib):
     assert np.max(np.abs(m @ g[0] - m @ wl.y) / (m @ wl.y)) < 1e-4
 
 
-def _resident_steps(gpu_lib, oracle, wl, precision, nsteps, group):
+def _resident_steps(gpu_lib, oracle, wl, precision, nsteps, group, staging=0):
     """Advance the same cells through nsteps successive t_stop values with the
     integrator state kept on the device; compare every step with the oracle's
     continuation."""
     import torch
     ode = gpu_lib.Odevec(wl.network, RelativeTolerance=wl.rtol, AbsoluteTolerance=wl.atol,
                          MinimalTimestep=wl.dt_min, nvector=group, precision=precision,
-                         raise_on_failure=False)
+                         raise_on_failure=False, staging=staging)
     gpu_lib.InitOdevec(ode)
     ws_g = gpu_lib.Workspace(ode, wl.ncells)
     ws_o = oracle.workspace(wl.network, wl.ncells, group)
@@ -346,3 +346,64 @@ def test_empty_and_group_size_errors(gpu_lib):
             S.SolveODE(ode, 0.0, 1e-10, 1e5, y)
     finally:
         S.CloseOdevec(ode)
+
+
+# ------------------------------------------------- warp per cell (staging 7)
+WPC_CASES = [
+    ("SYN64", dict(ncells=200), "SYN64_CSC_CMK"),
+    ("ROBER", dict(ncells=256), "ROBER_CSC_NONE"),
+    ("OREGO", dict(ncells=300), "OREGO_CSC_CMK"),
+]
+
+
+@pytest.mark.parametrize("name,kw,network", WPC_CASES)
+def test_warp_per_cell_bit_exact_vs_oracle(gpu_lib, oracle, name, kw, network):
+    # one warp per cell evaluates the network from tables of the emitted code
+    # and must reproduce the oracle (and the thread-per-cell kernel) bit for bit
+    wl = W.BUILDERS[name](network=network, **kw)
+    wl.group = 1
+    g = run_gpu(gpu_lib, wl, "fp64", group=1, staging=7)
+    o = run_oracle(oracle, wl, group=1)
+    assert np.all(o[3] == 0)
+    assert_bitwise(g, o, "%s warp per cell" % network)
+    assert_bitwise(run_gpu(gpu_lib, wl, "fp64", group=1, staging=3), o, "%s thread per cell" % network)
+
+
+def test_warp_per_cell_options(gpu_lib, oracle):
+    wl = W.syn64(ncells=96)
+    mask = (np.arange(96) % 4 != 1).astype(np.uint8)
+    assert_bitwise(run_gpu(gpu_lib, wl, "fp64", mask=mask, staging=7), run_oracle(oracle, wl, mask=mask), "mask")
+    assert_bitwise(run_gpu(gpu_lib, wl, "fp64", check_negatives=True, staging=7),
+                   run_oracle(oracle, wl, check_negatives=True), "check negatives")
+    g = run_gpu(gpu_lib, wl, "fp64", max_attempts=9, staging=7)
+    assert np.all(g[3] == 4)
+    assert_bitwise(g, run_oracle(oracle, wl, max_attempts=9), "max attempts")
+
+
+def test_warp_per_cell_resident(gpu_lib, oracle):
+    wl = W.syn64(ncells=64)
+    _resident_steps(gpu_lib, oracle, wl, "fp64", 3, 1, staging=7)
+
+
+def test_warp_per_cell_fast_forms(gpu_lib, oracle):
+    from odevec_b200 import syn64
+    wl = W.syn64(ncells=256)
+    o = run_oracle(oracle, wl)
+    m = syn64.masses()
+    # FMA and FP32 factors change roundings and with them the step sequence;
+    # on this network tiny species then move by far more than rtol, in either
+    # kernel.  Errors are taken relative to the species or 1e-6 of the cell's
+    # largest one, and the warp kernel must do no worse than the thread kernel.
+    floor = 1e-6 * np.max(np.abs(o[0]), axis=0)
+
+    def err(g):
+        return np.max(np.abs(g[0] - o[0]) / np.maximum(np.abs(o[0]), floor))
+
+    for precision in ("fp64_fma", "fp32_lu"):
+        g = run_gpu(gpu_lib, wl, precision, staging=7)
+        assert np.all(g[3] == 0)
+        assert np.max(np.abs(m @ g[0] - m @ wl.y) / (m @ wl.y)) < 1e-4
+        ref = err(run_gpu(gpu_lib, wl, precision, staging=3))
+        assert err(g) <= max(100 * wl.rtol, 2 * ref), (precision, err(g), ref)
+    # the automatic choice above 32 species is the warp kernel
+    assert_bitwise(run_gpu(gpu_lib, wl, "fp64"), run_gpu(gpu_lib, wl, "fp64", staging=7), "automatic staging")
