@@ -85,13 +85,13 @@ typedef struct odevec_opts {
     int32_t ss_batch;
     int32_t max_wait;
     /* launch shape, no effect on results.  staging: 0 = automatic (3 for
-       per-cell control, 7 above 32 species where compiled, 1 for lockstep); 1 = per-cell arrays in registers /
+       per-cell control up to 32 species, 1 above and for lockstep); 1 = per-cell arrays in registers /
        local memory, 2 blocks of 128 threads per SM; 2 = history and LU in
        shared memory, 1 block of 128 (where they fit); 3, 4 = as 1 with 3 or 4
        blocks per SM (fewer registers, more warps); 5 = as 2 with 192-thread
        blocks (FP32 LU); 6 = as 3 in one block of 384 threads per SM; 7 = one
        warp per cell (lanes share a cell's species; constant-coefficient
-       networks in CSC packaging; the automatic choice above 32 species)
+       networks in CSC packaging)
        (2-7: per-cell control only).  block_threads (a multiple of 32 up to the block of
        the staging) and grid_blocks: 0 = automatic (persistent grid filling
        every SM) */

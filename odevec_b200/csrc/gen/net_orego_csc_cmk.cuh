@@ -30,14 +30,48 @@ static __device__ const double ov_wpc_orego_csc_cmk_jac_const[14] = {
     77.27, 1.0};
 static __device__ const int ov_wpc_orego_csc_cmk_jac_rc[7] = {
     131074, 131073, 65537, 65536, 2, 1, 0};
-static __device__ const int ov_wpc_orego_csc_cmk_fac_lptr[5] = {
-    0, 1, 2, 3, 4};
-static __device__ const long long ov_wpc_orego_csc_cmk_fac_op[4] = {
-    2305840810190438408LL, 2199031644171LL, 2305840810194632714LL, 6597080252429LL};
-static __device__ const int ov_wpc_orego_csc_cmk_sol_lptr[7] = {
-    0, 1, 2, 3, 4, 5, 7};
-static __device__ const long long ov_wpc_orego_csc_cmk_sol_op[7] = {
-    2199021158400LL, 2199023255555LL, 6597067669506LL, 6597071863813LL, 15393160691716LL, 8796097216513LL, 10995120472067LL};
+static __device__ const long long ov_wpc_orego_csc_cmk_fac_op[128] = {
+    2305840810190438408LL, -1LL, -1LL, -1LL, -1LL, -1LL, -1LL, -1LL,
+    -1LL, -1LL, -1LL, -1LL, -1LL, -1LL, -1LL, -1LL,
+    -1LL, -1LL, -1LL, -1LL, -1LL, -1LL, -1LL, -1LL,
+    -1LL, -1LL, -1LL, -1LL, -1LL, -1LL, -1LL, -1LL,
+    2199031644171LL, -1LL, -1LL, -1LL, -1LL, -1LL, -1LL, -1LL,
+    -1LL, -1LL, -1LL, -1LL, -1LL, -1LL, -1LL, -1LL,
+    -1LL, -1LL, -1LL, -1LL, -1LL, -1LL, -1LL, -1LL,
+    -1LL, -1LL, -1LL, -1LL, -1LL, -1LL, -1LL, -1LL,
+    2305840810194632714LL, -1LL, -1LL, -1LL, -1LL, -1LL, -1LL, -1LL,
+    -1LL, -1LL, -1LL, -1LL, -1LL, -1LL, -1LL, -1LL,
+    -1LL, -1LL, -1LL, -1LL, -1LL, -1LL, -1LL, -1LL,
+    -1LL, -1LL, -1LL, -1LL, -1LL, -1LL, -1LL, -1LL,
+    6597080252429LL, -1LL, -1LL, -1LL, -1LL, -1LL, -1LL, -1LL,
+    -1LL, -1LL, -1LL, -1LL, -1LL, -1LL, -1LL, -1LL,
+    -1LL, -1LL, -1LL, -1LL, -1LL, -1LL, -1LL, -1LL,
+    -1LL, -1LL, -1LL, -1LL, -1LL, -1LL, -1LL, -1LL};
+static __device__ const long long ov_wpc_orego_csc_cmk_sol_op[192] = {
+    2199021158400LL, -1LL, -1LL, -1LL, -1LL, -1LL, -1LL, -1LL,
+    -1LL, -1LL, -1LL, -1LL, -1LL, -1LL, -1LL, -1LL,
+    -1LL, -1LL, -1LL, -1LL, -1LL, -1LL, -1LL, -1LL,
+    -1LL, -1LL, -1LL, -1LL, -1LL, -1LL, -1LL, -1LL,
+    2199023255555LL, -1LL, -1LL, -1LL, -1LL, -1LL, -1LL, -1LL,
+    -1LL, -1LL, -1LL, -1LL, -1LL, -1LL, -1LL, -1LL,
+    -1LL, -1LL, -1LL, -1LL, -1LL, -1LL, -1LL, -1LL,
+    -1LL, -1LL, -1LL, -1LL, -1LL, -1LL, -1LL, -1LL,
+    6597067669506LL, -1LL, -1LL, -1LL, -1LL, -1LL, -1LL, -1LL,
+    -1LL, -1LL, -1LL, -1LL, -1LL, -1LL, -1LL, -1LL,
+    -1LL, -1LL, -1LL, -1LL, -1LL, -1LL, -1LL, -1LL,
+    -1LL, -1LL, -1LL, -1LL, -1LL, -1LL, -1LL, -1LL,
+    6597071863813LL, -1LL, -1LL, -1LL, -1LL, -1LL, -1LL, -1LL,
+    -1LL, -1LL, -1LL, -1LL, -1LL, -1LL, -1LL, -1LL,
+    -1LL, -1LL, -1LL, -1LL, -1LL, -1LL, -1LL, -1LL,
+    -1LL, -1LL, -1LL, -1LL, -1LL, -1LL, -1LL, -1LL,
+    15393160691716LL, -1LL, -1LL, -1LL, -1LL, -1LL, -1LL, -1LL,
+    -1LL, -1LL, -1LL, -1LL, -1LL, -1LL, -1LL, -1LL,
+    -1LL, -1LL, -1LL, -1LL, -1LL, -1LL, -1LL, -1LL,
+    -1LL, -1LL, -1LL, -1LL, -1LL, -1LL, -1LL, -1LL,
+    8796097216513LL, 10995120472067LL, -1LL, -1LL, -1LL, -1LL, -1LL, -1LL,
+    -1LL, -1LL, -1LL, -1LL, -1LL, -1LL, -1LL, -1LL,
+    -1LL, -1LL, -1LL, -1LL, -1LL, -1LL, -1LL, -1LL,
+    -1LL, -1LL, -1LL, -1LL, -1LL, -1LL, -1LL, -1LL};
 static __device__ const int ov_wpc_orego_csc_cmk_srow[3] = {
     2, 1, 0};
 static __device__ const int ov_wpc_orego_csc_cmk_dyn[3] = {
@@ -49,8 +83,6 @@ struct ov_wpc_orego_csc_cmk {
   __device__ static const int* jac_ptr() { return ov_wpc_orego_csc_cmk_jac_ptr; }
   __device__ static const int* jac_code() { return ov_wpc_orego_csc_cmk_jac_code; }
   __device__ static const int* jac_rc() { return ov_wpc_orego_csc_cmk_jac_rc; }
-  __device__ static const int* fac_lptr() { return ov_wpc_orego_csc_cmk_fac_lptr; }
-  __device__ static const int* sol_lptr() { return ov_wpc_orego_csc_cmk_sol_lptr; }
   __device__ static const int* srow() { return ov_wpc_orego_csc_cmk_srow; }
   __device__ static const int* dyn() { return ov_wpc_orego_csc_cmk_dyn; }
   __device__ static const double* rhs_coef() { return ov_wpc_orego_csc_cmk_rhs_coef; }

@@ -27,14 +27,52 @@ static __device__ const double ov_wpc_rober_csc_none_jac_const[11] = {
     10000.0, 10000.0, 1.0};
 static __device__ const int ov_wpc_rober_csc_none_jac_rc[8] = {
     0, 1, 65536, 65537, 65538, 131072, 131073, 131074};
-static __device__ const int ov_wpc_rober_csc_none_fac_lptr[5] = {
-    0, 2, 4, 5, 6};
-static __device__ const long long ov_wpc_rober_csc_none_fac_op[6] = {
-    2305840810190438404LL, 2305840810190438410LL, 2199027449863LL, 2199033741325LL, 2305840810196729868LL, 8796105605135LL};
-static __device__ const int ov_wpc_rober_csc_none_sol_lptr[8] = {
-    0, 1, 2, 3, 4, 5, 7, 8};
-static __device__ const long long ov_wpc_rober_csc_none_sol_op[8] = {
-    2199021158400LL, 2199023255555LL, 8796090925058LL, 8796095119365LL, 17592183947268LL, 10995120472065LL, 13194143727619LL, 4398048608257LL};
+static __device__ const long long ov_wpc_rober_csc_none_fac_op[128] = {
+    2305840810190438404LL, 2305840810190438410LL, -1LL, -1LL, -1LL, -1LL, -1LL, -1LL,
+    -1LL, -1LL, -1LL, -1LL, -1LL, -1LL, -1LL, -1LL,
+    -1LL, -1LL, -1LL, -1LL, -1LL, -1LL, -1LL, -1LL,
+    -1LL, -1LL, -1LL, -1LL, -1LL, -1LL, -1LL, -1LL,
+    2199027449863LL, 2199033741325LL, -1LL, -1LL, -1LL, -1LL, -1LL, -1LL,
+    -1LL, -1LL, -1LL, -1LL, -1LL, -1LL, -1LL, -1LL,
+    -1LL, -1LL, -1LL, -1LL, -1LL, -1LL, -1LL, -1LL,
+    -1LL, -1LL, -1LL, -1LL, -1LL, -1LL, -1LL, -1LL,
+    2305840810196729868LL, -1LL, -1LL, -1LL, -1LL, -1LL, -1LL, -1LL,
+    -1LL, -1LL, -1LL, -1LL, -1LL, -1LL, -1LL, -1LL,
+    -1LL, -1LL, -1LL, -1LL, -1LL, -1LL, -1LL, -1LL,
+    -1LL, -1LL, -1LL, -1LL, -1LL, -1LL, -1LL, -1LL,
+    8796105605135LL, -1LL, -1LL, -1LL, -1LL, -1LL, -1LL, -1LL,
+    -1LL, -1LL, -1LL, -1LL, -1LL, -1LL, -1LL, -1LL,
+    -1LL, -1LL, -1LL, -1LL, -1LL, -1LL, -1LL, -1LL,
+    -1LL, -1LL, -1LL, -1LL, -1LL, -1LL, -1LL, -1LL};
+static __device__ const long long ov_wpc_rober_csc_none_sol_op[224] = {
+    2199021158400LL, -1LL, -1LL, -1LL, -1LL, -1LL, -1LL, -1LL,
+    -1LL, -1LL, -1LL, -1LL, -1LL, -1LL, -1LL, -1LL,
+    -1LL, -1LL, -1LL, -1LL, -1LL, -1LL, -1LL, -1LL,
+    -1LL, -1LL, -1LL, -1LL, -1LL, -1LL, -1LL, -1LL,
+    2199023255555LL, -1LL, -1LL, -1LL, -1LL, -1LL, -1LL, -1LL,
+    -1LL, -1LL, -1LL, -1LL, -1LL, -1LL, -1LL, -1LL,
+    -1LL, -1LL, -1LL, -1LL, -1LL, -1LL, -1LL, -1LL,
+    -1LL, -1LL, -1LL, -1LL, -1LL, -1LL, -1LL, -1LL,
+    8796090925058LL, -1LL, -1LL, -1LL, -1LL, -1LL, -1LL, -1LL,
+    -1LL, -1LL, -1LL, -1LL, -1LL, -1LL, -1LL, -1LL,
+    -1LL, -1LL, -1LL, -1LL, -1LL, -1LL, -1LL, -1LL,
+    -1LL, -1LL, -1LL, -1LL, -1LL, -1LL, -1LL, -1LL,
+    8796095119365LL, -1LL, -1LL, -1LL, -1LL, -1LL, -1LL, -1LL,
+    -1LL, -1LL, -1LL, -1LL, -1LL, -1LL, -1LL, -1LL,
+    -1LL, -1LL, -1LL, -1LL, -1LL, -1LL, -1LL, -1LL,
+    -1LL, -1LL, -1LL, -1LL, -1LL, -1LL, -1LL, -1LL,
+    17592183947268LL, -1LL, -1LL, -1LL, -1LL, -1LL, -1LL, -1LL,
+    -1LL, -1LL, -1LL, -1LL, -1LL, -1LL, -1LL, -1LL,
+    -1LL, -1LL, -1LL, -1LL, -1LL, -1LL, -1LL, -1LL,
+    -1LL, -1LL, -1LL, -1LL, -1LL, -1LL, -1LL, -1LL,
+    10995120472065LL, 13194143727619LL, -1LL, -1LL, -1LL, -1LL, -1LL, -1LL,
+    -1LL, -1LL, -1LL, -1LL, -1LL, -1LL, -1LL, -1LL,
+    -1LL, -1LL, -1LL, -1LL, -1LL, -1LL, -1LL, -1LL,
+    -1LL, -1LL, -1LL, -1LL, -1LL, -1LL, -1LL, -1LL,
+    4398048608257LL, -1LL, -1LL, -1LL, -1LL, -1LL, -1LL, -1LL,
+    -1LL, -1LL, -1LL, -1LL, -1LL, -1LL, -1LL, -1LL,
+    -1LL, -1LL, -1LL, -1LL, -1LL, -1LL, -1LL, -1LL,
+    -1LL, -1LL, -1LL, -1LL, -1LL, -1LL, -1LL, -1LL};
 static __device__ const int ov_wpc_rober_csc_none_srow[3] = {
     0, 1, 2};
 static __device__ const int ov_wpc_rober_csc_none_dyn[3] = {
@@ -46,8 +84,6 @@ struct ov_wpc_rober_csc_none {
   __device__ static const int* jac_ptr() { return ov_wpc_rober_csc_none_jac_ptr; }
   __device__ static const int* jac_code() { return ov_wpc_rober_csc_none_jac_code; }
   __device__ static const int* jac_rc() { return ov_wpc_rober_csc_none_jac_rc; }
-  __device__ static const int* fac_lptr() { return ov_wpc_rober_csc_none_fac_lptr; }
-  __device__ static const int* sol_lptr() { return ov_wpc_rober_csc_none_sol_lptr; }
   __device__ static const int* srow() { return ov_wpc_rober_csc_none_srow; }
   __device__ static const int* dyn() { return ov_wpc_rober_csc_none_dyn; }
   __device__ static const double* rhs_coef() { return ov_wpc_rober_csc_none_rhs_coef; }

@@ -65,16 +65,16 @@ int32_t fail(int32_t code, const char* fmt, ...)
     return code;
 }
 
-/* automatic staging: one warp per cell for per-cell control of networks of
-   more than 32 solver-state species that have the tables, else thread-local
-   arrays with 3 blocks of 128 per SM (per-cell) or 2 (lockstep) */
+/* automatic staging (the measured best on B200 without a tuning table):
+   thread-local arrays, 3 blocks of 128 threads per SM for per-cell control
+   up to 32 solver-state species, 2 blocks above (more registers per cell),
+   2 blocks for lockstep groups.  The warp-per-cell staging (7) is slower on
+   the shipped networks and is only used when asked for. */
 int auto_staging(const NetEntry& e, int group_size)
 {
     if (group_size != 1)
         return 1;
-    if (e.sizes[7] && e.sizes[5] > 32)
-        return 7;
-    return 3;
+    return e.sizes[5] > 32 ? 1 : 3;
 }
 
 int find_net(const char* tag)

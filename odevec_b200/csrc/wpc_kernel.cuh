@@ -145,14 +145,19 @@ struct WCell {
         }
     }
 
+    /* Loops over the runtime order run to MAXQ with predicates (the same
+       operations in the same order), so the history stays in registers. */
     __device__ __forceinline__ void predict()
     {
         ppass += q * (q + 1) / 2;
 #pragma unroll
         for (int m = 0; m < NS; ++m) {
-            for (int l = 0; l <= q - 1; ++l)
-                for (int k = q; k >= l + 1; --k)
-                    yns[k - 1][m] = yns[k][m] + yns[k - 1][m];
+#pragma unroll
+            for (int l = 0; l < MAXQ; ++l)
+#pragma unroll
+                for (int k = MAXQ; k >= 1; --k)
+                    if (l <= q - 1 && k <= q && k >= l + 1)
+                        yns[k - 1][m] = yns[k][m] + yns[k - 1][m];
             en[m] = 0.0;
         }
     }
@@ -162,19 +167,25 @@ struct WCell {
         ppass += q * (q + 1) / 2;
 #pragma unroll
         for (int m = 0; m < NS; ++m)
-            for (int k = 0; k <= q - 1; ++k)
-                for (int jj = q; jj >= k + 1; --jj)
-                    yns[jj - 1][m] = yns[jj - 1][m] - yns[jj][m];
+#pragma unroll
+            for (int k = 0; k < MAXQ; ++k)
+#pragma unroll
+                for (int jj = MAXQ; jj >= 1; --jj)
+                    if (k <= q - 1 && jj <= q && jj >= k + 1)
+                        yns[jj - 1][m] = yns[jj - 1][m] - yns[jj][m];
     }
 
     __device__ __forceinline__ void set_step(double dt_scale)
     {
         double dtt = 1.0;
-        for (int k = 1; k <= q; ++k) {
-            dtt = dt_scale * dtt;
 #pragma unroll
-            for (int m = 0; m < NS; ++m)
-                yns[k][m] = yns[k][m] * dtt;
+        for (int k = 1; k <= MAXQ; ++k) {
+            if (k <= q) {
+                dtt = dt_scale * dtt;
+#pragma unroll
+                for (int m = 0; m < NS; ++m)
+                    yns[k][m] = yns[k][m] * dtt;
+            }
         }
         h = h * dt_scale;
         jchg = jchg * dt_scale;
@@ -182,12 +193,26 @@ struct WCell {
 
     __device__ __forceinline__ void update_nordsieck()
     {
-        for (int k = 0; k <= q; ++k) {
-            const double c = lcoef(q, k);
 #pragma unroll
-            for (int m = 0; m < NS; ++m)
-                yns[k][m] = yns[k][m] + en[m] * c;
+        for (int k = 0; k <= MAXQ; ++k) {
+            if (k <= q) {
+                const double c = lcoef(q, k);
+#pragma unroll
+                for (int m = 0; m < NS; ++m)
+                    yns[k][m] = yns[k][m] + en[m] * c;
+            }
         }
+    }
+
+    /* yns[k] for a runtime k, selected with compile-time indices */
+    __device__ __forceinline__ double hist(int k, int m) const
+    {
+        double v = 0.0;
+#pragma unroll
+        for (int kk = 0; kk <= MAXQ; ++kk)
+            if (kk == k)
+                v = yns[kk][m];
+        return v;
     }
 
     __device__ __forceinline__ void set_y_from(const double (&v)[NS])
@@ -206,9 +231,11 @@ struct WCell {
         double v[NS];
 #pragma unroll
         for (int m = 0; m < NS; ++m) {
-            double acc = yns[q][m];
-            for (int k = q - 1; k >= 0; --k)
-                acc = yns[k][m] + rel_t * acc;
+            double acc = hist(q, m);
+#pragma unroll
+            for (int k = MAXQ - 1; k >= 0; --k)
+                if (k <= q - 1)
+                    acc = yns[k][m] + rel_t * acc;
             v[m] = acc;
         }
         set_y_from(v);
@@ -224,7 +251,7 @@ struct WCell {
             double e[NS];
 #pragma unroll
             for (int m = 0; m < NS; ++m)
-                e[m] = yns[order][m];
+                e[m] = hist(order, m);
             down = 1.0 / ((double)1.3f * pow_dev(wnorm(e) / tau(order, order - 1), 1.0 / order) + 1e-6);
         }
         same = 1.0 / ((double)1.2f * pow_dev(wnorm(en) / tau(order, order), 1.0 / (order + 1.0)) + 1e-6);
@@ -254,8 +281,11 @@ struct WCell {
                 if (order != MAXQ) {
                     const double c = lcoef(order, order);
 #pragma unroll
-                    for (int m = 0; m < NS; ++m)
-                        yns[order + 1][m] = c * en[m] / (order + 1.0);
+                    for (int kk = 1; kk <= MAXQ; ++kk)
+                        if (kk == order + 1)
+#pragma unroll
+                            for (int m = 0; m < NS; ++m)
+                                yns[kk][m] = c * en[m] / (order + 1.0);
                     q = order + 1;
                 } else
                     status = OV_ERR_ORDER;
@@ -341,11 +371,13 @@ struct WCell {
             }
         }
         __syncwarp();
-        const int* lp = W::fac_lptr();
+        /* one row of 32 statement slots per level (a negative slot is
+           empty); the rows run in order with the warp reconverged between */
         const long long* ops = W::fac_op();
+#pragma unroll 4
         for (int l = 0; l < W::NFL; ++l) {
-            for (int i = lp[l] + lane; i < lp[l + 1]; i += 32) {
-                const long long o = ops[i];
+            const long long o = ops[l * 32 + lane];
+            if (o >= 0) {
                 const int x = (int)((o >> 1) & 0xfffff), y = (int)((o >> 21) & 0xfffff);
                 if ((o & 1) == 0)
                     a[x] = a[x] / a[y];
@@ -370,11 +402,11 @@ struct WCell {
                     dv[srow[lane + 32 * m]] = (LUT)(res * 1.0);
             }
         __syncwarp();
-        const int* lp = W::sol_lptr();
         const long long* ops = W::sol_op();
+#pragma unroll 4
         for (int l = 0; l < W::NSL; ++l) {
-            for (int i = lp[l] + lane; i < lp[l + 1]; i += 32) {
-                const long long o = ops[i];
+            const long long o = ops[l * 32 + lane];
+            if (o >= 0) {
                 const int x = (int)((o >> 1) & 0xfffff), k = (int)((o >> 41) & 0xfffff);
                 if ((o & 1) == 0)
                     dv[x] = dv[x] / a[k];
@@ -454,6 +486,7 @@ struct WCell {
 
     __device__ void save_state(double* ws, int64_t n, int64_t cell) const
     {
+#pragma unroll
         for (int k = 0; k <= MAXQ; ++k)
 #pragma unroll
             for (int m = 0; m < NS; ++m)
@@ -477,6 +510,7 @@ struct WCell {
 
     __device__ void load_state(const double* ws, int64_t n, int64_t cell)
     {
+#pragma unroll
         for (int k = 0; k <= MAXQ; ++k)
 #pragma unroll
             for (int m = 0; m < NS; ++m)

@@ -429,16 +429,17 @@ def emit(sysm, cid: str) -> str:
     L.append(_arr("int", "ov_wpc_%s_jac_code" % cid, code))
     L.append(_arr("double", "ov_wpc_%s_jac_const" % cid, [_dbl(c) for c in t["consts"]], 4))
     L.append(_arr("int", "ov_wpc_%s_jac_rc" % cid, [r | (c << 16) for r, c in zip(t["rows"], t["cols"])]))
-    # factorisation and solve statements, level by level
+    # factorisation and solve statements: one row of 32 slots per level (a
+    # level of more than 32 statements takes several rows: its statements
+    # are independent, so running them one row after another is the same)
     def lev_tables(name, ops, lev, enc):
-        lptr, flat = [0], []
+        rows = []
         for idx in lev:
-            for i in idx:
-                flat.append(enc(ops[i]))
-            lptr.append(len(flat))
-        L.append(_arr("int", "ov_wpc_%s_%s_lptr" % (cid, name), lptr))
-        L.append(_arr("long long", "ov_wpc_%s_%s_op" % (cid, name), flat, 8))
-        return len(lev)
+            for r in range(0, len(idx), 32):
+                part = idx[r:r + 32]
+                rows.append([enc(ops[i]) for i in part] + ["-1LL"] * (32 - len(part)))
+        L.append(_arr("long long", "ov_wpc_%s_%s_op" % (cid, name), [v for row in rows for v in row], 8))
+        return len(rows)
 
     enc = lambda o: "%dLL" % (o[0] | (o[1] << 1) | ((o[2] & 0xfffff) << 21) | ((o[3] & 0xfffff) << 41))
     nfl = lev_tables("fac", t["fops"], t["flev"], enc)
@@ -455,7 +456,7 @@ def emit(sysm, cid: str) -> str:
     L.append("struct ov_wpc_%s {" % cid)
     L.append("  static constexpr int NTERM = %d, NPROG = %d, DEPTH = %d, NFL = %d, NSL = %d;"
              % (len(coef), len(t["progs"]), dmax, nfl, nsl))
-    for nm in ("rhs_ptr", "rhs_fac", "jac_ptr", "jac_code", "jac_rc", "fac_lptr", "sol_lptr", "srow", "dyn"):
+    for nm in ("rhs_ptr", "rhs_fac", "jac_ptr", "jac_code", "jac_rc", "srow", "dyn"):
         L.append("  __device__ static const int* %s() { return ov_wpc_%s_%s; }" % (nm, cid, nm))
     for nm in ("rhs_coef", "jac_const"):
         L.append("  __device__ static const double* %s() { return ov_wpc_%s_%s; }" % (nm, cid, nm))

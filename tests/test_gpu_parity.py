@@ -405,5 +405,5 @@ def test_warp_per_cell_fast_forms(gpu_lib, oracle):
         assert np.max(np.abs(m @ g[0] - m @ wl.y) / (m @ wl.y)) < 1e-4
         ref = err(run_gpu(gpu_lib, wl, precision, staging=3))
         assert err(g) <= max(100 * wl.rtol, 2 * ref), (precision, err(g), ref)
-    # the automatic choice above 32 species is the warp kernel
+    # the automatic staging gives the warp kernel's bits as well
     assert_bitwise(run_gpu(gpu_lib, wl, "fp64"), run_gpu(gpu_lib, wl, "fp64", staging=7), "automatic staging")
