@@ -91,8 +91,9 @@ typedef struct odevec_opts {
        blocks per SM (fewer registers, more warps); 5 = as 2 with 192-thread
        blocks (FP32 LU); 6 = as 3 in one block of 384 threads per SM; 7 = one
        warp per cell (lanes share a cell's species; constant-coefficient
-       networks in CSC packaging)
-       (2-7: per-cell control only).  block_threads (a multiple of 32 up to the block of
+       networks in CSC packaging); 8 = as 6 with the block's warps held in
+       soft lockstep at the top of every trip (bounded polling, no barrier)
+       (2-8: per-cell control only).  block_threads (a multiple of 32 up to the block of
        the staging) and grid_blocks: 0 = automatic (persistent grid filling
        every SM) */
     int32_t staging;

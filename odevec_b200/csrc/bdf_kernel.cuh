@@ -156,13 +156,69 @@ struct LaneHist {
    budget; SHM places the Nordsieck history and the LU in shared memory. */
 template <int STAGE>
 struct StageCfg;
-template <> struct StageCfg<1> { static constexpr bool SHM = false; static constexpr int BS = 128, MINB = 2; };
-template <> struct StageCfg<2> { static constexpr bool SHM = true;  static constexpr int BS = 128, MINB = 1; };
-template <> struct StageCfg<3> { static constexpr bool SHM = false; static constexpr int BS = 128, MINB = 3; };
-template <> struct StageCfg<4> { static constexpr bool SHM = false; static constexpr int BS = 128, MINB = 4; };
-template <> struct StageCfg<5> { static constexpr bool SHM = true;  static constexpr int BS = 192, MINB = 1; };
+template <> struct StageCfg<1> { static constexpr bool SHM = false, SOFT = false; static constexpr int BS = 128, MINB = 2; };
+template <> struct StageCfg<2> { static constexpr bool SHM = true,  SOFT = false; static constexpr int BS = 128, MINB = 1; };
+template <> struct StageCfg<3> { static constexpr bool SHM = false, SOFT = false; static constexpr int BS = 128, MINB = 3; };
+template <> struct StageCfg<4> { static constexpr bool SHM = false, SOFT = false; static constexpr int BS = 128, MINB = 4; };
+template <> struct StageCfg<5> { static constexpr bool SHM = true,  SOFT = false; static constexpr int BS = 192, MINB = 1; };
 /* as 3, the same register budget, in one block of 384 threads per SM */
-template <> struct StageCfg<6> { static constexpr bool SHM = false; static constexpr int BS = 384, MINB = 1; };
+template <> struct StageCfg<6> { static constexpr bool SHM = false, SOFT = false; static constexpr int BS = 384, MINB = 1; };
+/* as 6, with the block's warps held in soft lockstep (SoftSync) */
+template <> struct StageCfg<8> { static constexpr bool SHM = false, SOFT = true;  static constexpr int BS = 384, MINB = 1; };
+
+/* Soft lockstep.  The warps of a block wait for each other at the top of
+   every trip of the cell loop, so they run the same phase code at the same
+   time and share instruction fetches.  No barrier instruction is used: lane
+   0 of a warp counts itself in with a shared-memory atomic and polls a
+   generation word, sleeping between polls, at most SOFT_SPIN_LIMIT times;
+   after that it goes on alone.  Nothing a cell computes depends on the
+   lockstep (every decision stays per lane or per warp), so a late, lost or
+   early arrival costs time and never changes a result, and no wait is
+   unbounded. */
+struct SoftSync {
+    unsigned arrive; /* warps counted in for the current generation */
+    unsigned gen;    /* generation, bumped by the warp that completes it */
+    unsigned active; /* warps still in the cell loop */
+};
+constexpr int SOFT_SPIN_LIMIT = 4096; /* polls of >= 64 ns: about 0.3 ms at most */
+
+/* completes the current generation */
+__device__ __forceinline__ void soft_release(SoftSync* s)
+{
+    atomicExch(&s->arrive, 0u);
+    __threadfence_block();
+    atomicAdd(&s->gen, 1u);
+}
+
+__device__ __forceinline__ void soft_sync(SoftSync* s, int lane)
+{
+    __syncwarp();
+    if (lane == 0) {
+        const unsigned g = *(volatile unsigned*)&s->gen;
+        const unsigned n = atomicAdd(&s->arrive, 1u) + 1u;
+        if (n >= *(volatile unsigned*)&s->active) {
+            soft_release(s);
+        } else {
+            for (int i = 0; i < SOFT_SPIN_LIMIT; ++i) {
+                if (*(volatile unsigned*)&s->gen != g)
+                    break;
+                __nanosleep(64);
+            }
+        }
+    }
+    __syncwarp();
+}
+
+/* a warp leaves the cell loop: if the others already wait for it, release them */
+__device__ __forceinline__ void soft_leave(SoftSync* s, int lane)
+{
+    if (lane == 0) {
+        const unsigned left = atomicSub(&s->active, 1u) - 1u;
+        if (left > 0 && *(volatile unsigned*)&s->arrive >= left)
+            soft_release(s);
+    }
+}
+
 
 template <class Net, class LUT, bool SHM, int BS>
 struct Staging;
@@ -705,10 +761,21 @@ __global__ void __launch_bounds__(StageCfg<STAGE>::BS, StageCfg<STAGE>::MINB) bd
     int ph = PH_IDLE;
     int64_t cell = -1;
     bool write_y = false;
+    __shared__ SoftSync soft;
+    if constexpr (StageCfg<STAGE>::SOFT) {
+        if (threadIdx.x == 0) {
+            soft.arrive = 0u;
+            soft.gen = 0u;
+            soft.active = blockDim.x / 32u;
+        }
+        __syncthreads(); /* once, at entry, with every thread converged */
+    }
 
     for (;;) {
         /* ---- 1. idle lanes take new cells ---------------------------- */
         if (G == 1) {
+            if constexpr (StageCfg<STAGE>::SOFT)
+                soft_sync(&soft, lane);
             const unsigned need = __ballot_sync(FULL, ph == PH_IDLE);
             if (need) {
                 const int leader = __ffs(need) - 1;
@@ -721,8 +788,11 @@ __global__ void __launch_bounds__(StageCfg<STAGE>::BS, StageCfg<STAGE>::MINB) bd
                     ph = cell < ncells ? PH_START : PH_EXHAUSTED;
                 }
             }
-            if (__all_sync(FULL, ph == PH_EXHAUSTED))
+            if (__all_sync(FULL, ph == PH_EXHAUSTED)) {
+                if constexpr (StageCfg<STAGE>::SOFT)
+                    soft_leave(&soft, lane);
                 break;
+            }
         } else {
             if (ph == PH_IDLE) { /* warp-uniform */
                 unsigned long long g = 0;
@@ -1093,8 +1163,8 @@ constexpr bool shm_fits()
    LU in shared memory, 1 block of 128; 3, 4 = thread-local, 3 or 4 blocks of
    128 (fewer registers, more warps); 5 = shared memory, 1 block of 192;
    6 = thread-local, 1 block of 384; 7 = one warp per cell (wpc_kernel.cuh;
-   constant-coefficient CSC variants).  Stages 2-7 exist for per-cell
-   control (G = 1). */
+   constant-coefficient CSC variants); 8 = as 6 in soft lockstep.  Stages
+   2-8 exist for per-cell control (G = 1). */
 #define OV_STAGE_CASE(NET, LU, ST)                                                               \
     if (stage == ST)                                                                             \
         return launch<NET, 1, LU, ST>(a, block, grid, s);
@@ -1111,6 +1181,7 @@ constexpr bool shm_fits()
             OV_STAGE_CASE(NET, double, 3)                                                        \
             OV_STAGE_CASE(NET, double, 4)                                                        \
             OV_STAGE_CASE(NET, double, 6)                                                        \
+            OV_STAGE_CASE(NET, double, 8)                                                        \
             if constexpr (wpc_ok<NET, double>()) {                                               \
                 if (stage == 7)                                                                  \
                     return launch_wpc<NET, double>(a, grid, s);                                  \
@@ -1126,6 +1197,7 @@ constexpr bool shm_fits()
                 OV_STAGE_CASE(NET, float, 3)                                                     \
                 OV_STAGE_CASE(NET, float, 4)                                                     \
                 OV_STAGE_CASE(NET, float, 6)                                                     \
+                OV_STAGE_CASE(NET, float, 8)                                                     \
                 if constexpr (wpc_ok<NET, float>()) {                                            \
                     if (stage == 7)                                                              \
                         return launch_wpc<NET, float>(a, grid, s);                               \
