@@ -30,7 +30,7 @@ TABLE = os.path.join(HERE, "tuning.json")
 
 STAGINGS = (1, 2, 3, 4, 6, 7, 8)
 FP32_STAGINGS = (5,)
-BATCHES = ((24, 24, 8), (16, 16, 4), (32, 32, 16), (8, 8, 4), (1, 1, -1))
+BATCHES = ((24, 24, 8), (16, 16, 4), (32, 32, 16), (8, 8, 4), (4, 4, 2), (2, 2, 1), (1, 1, -1))
 FIELDS = ("staging", "jac_batch", "ss_batch", "max_wait")
 
 
