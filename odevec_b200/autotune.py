@@ -12,9 +12,8 @@ What it chooses, per network variant, precision form and GPU model:
 None of these settings changes a result (every cell runs the same operations whatever the interleaving;
 the GPU parity tests check this bit for bit), so tuning only moves time.
 
-The search is coordinate-wise on a timed sample of the caller's cells:
-every compiled staging with the default batches, then a few batch settings
-on the best staging.  Results go to a JSON table (``tuning.json`` beside this
+The search times every compiled staging with every batch setting on a
+sample of the caller's cells (about fifty short solves).  Results go to a JSON table (``tuning.json`` beside this
 file) that InitOdevec consults for options left at 0 (automatic).
 
     python -m odevec_b200.autotune --network PRIMORDIAL_CSC_FF --precision fp32_lu
@@ -78,29 +77,23 @@ def candidates(precision: str) -> List[int]:
 
 def search(time_config: Callable[[dict], Optional[float]], precision: str,
            batches=BATCHES) -> Tuple[dict, List[Tuple[dict, float]]]:
-    """Coordinate search; time_config(cfg) returns seconds, or None for a
-    configuration that is not compiled for the variant."""
+    """Every compiled staging with every batch setting (the two interact:
+    soft lockstep is best without batching, thread-local stagings with it);
+    time_config(cfg) returns seconds, or None for a configuration that is
+    not compiled for the variant (then the staging is skipped)."""
     tried: List[Tuple[dict, float]] = []
     best, best_t = None, None
     for st in candidates(precision):
-        cfg = {"staging": st, "jac_batch": 0, "ss_batch": 0, "max_wait": 0}
-        t = time_config(cfg)
-        if t is None:
-            continue
-        tried.append((cfg, t))
-        if best_t is None or t < best_t:
-            best, best_t = cfg, t
+        for b in batches:
+            cfg = {"staging": st, "jac_batch": b[0], "ss_batch": b[1], "max_wait": b[2]}
+            t = time_config(cfg)
+            if t is None:
+                break
+            tried.append((cfg, t))
+            if best_t is None or t < best_t:
+                best, best_t = cfg, t
     if best is None:
         raise RuntimeError("no compiled configuration could be timed")
-    st = best["staging"]
-    for b in batches:
-        cfg = {"staging": st, "jac_batch": b[0], "ss_batch": b[1], "max_wait": b[2]}
-        t = time_config(cfg)
-        if t is None:
-            continue
-        tried.append((cfg, t))
-        if t < best_t:
-            best, best_t = cfg, t
     return dict(best, seconds=best_t), tried
 
 

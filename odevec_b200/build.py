@@ -42,6 +42,33 @@ def variants():
     return re.findall(r'OV_NET\((\w+), "([^"]+)"\)', open(reg).read())
 
 
+PREC_CODE = {"fp64": 0, "fp64_fma": 1, "fp32_lu": 2}
+
+
+def write_tuning_table() -> str:
+    """gen/tuning.inc: the autotuner's table (odevec_b200/tuning.json) as C,
+    so the C ABI picks the tuned launch shape for options left at 0."""
+    import json
+    src = os.path.join(HERE, "tuning.json")
+    table = json.load(open(src)) if os.path.exists(src) else {}
+    lines = ["/* Generated by odevec_b200/build.py from odevec_b200/tuning.json -- do not edit.",
+             "   OV_TUNE(tag, precision, group, device, staging, jac_batch, ss_batch, max_wait) */"]
+    for key in sorted(table):
+        net, prec, grp, dev = key.split("/")
+        v = table[key]
+        if prec not in PREC_CODE or '"' in dev or "\\" in dev:
+            continue
+        lines.append('OV_TUNE("%s", %d, %d, "%s", %d, %d, %d, %d)' % (
+            net, PREC_CODE[prec], int(grp[1:]), dev, int(v["staging"]), int(v["jac_batch"]),
+            int(v["ss_batch"]), int(v["max_wait"])))
+    path = os.path.join(GEN, "tuning.inc")
+    text = "\n".join(lines) + "\n"
+    if not os.path.exists(path) or open(path).read() != text:
+        with open(path, "w") as fh:
+            fh.write(text)
+    return path
+
+
 def ensure_generated():
     if not variants():
         from . import shipped
@@ -105,8 +132,9 @@ def build(force: bool = False, jobs: int = 0, verbose: bool = False) -> str:
     objs.append(probe_obj)
     abi_src = os.path.join(CSRC, "odevec_abi.cu")
     abi_obj = os.path.join(BUILD, "odevec_abi.o")
+    tune_inc = write_tuning_table()
     key = _hash_files(hdrs + [abi_src, os.path.join(GEN, "registry.inc"),
-                              os.path.join(GEN, "includes_c.inc")] +
+                              os.path.join(GEN, "includes_c.inc"), tune_inc] +
                       [os.path.join(GEN, "net_%s.h" % c) for c, _ in variants()], " ".join(COMMON))
     if force or not os.path.exists(abi_obj) or not os.path.exists(abi_obj + ".key") or \
             open(abi_obj + ".key").read() != key:

@@ -54,6 +54,40 @@ const NetEntry g_nets[] = {
 #undef OV_NET
 constexpr int g_nnets = (int)(sizeof g_nets / sizeof g_nets[0]);
 
+/* tuned launch options per (variant, precision, group size, GPU model),
+   generated from the autotuner's table (odevec_b200/autotune.py) */
+struct TuneEntry {
+    const char* tag;
+    int precision, group;
+    const char* device;
+    int staging, jac_batch, ss_batch, max_wait;
+};
+#define OV_TUNE(tag, prec, grp, dev, st, jb, sb, mw) {tag, prec, grp, dev, st, jb, sb, mw},
+const TuneEntry g_tune[] = {
+#include "gen/tuning.inc"
+    {nullptr, 0, 0, nullptr, 0, 0, 0, 0}};
+#undef OV_TUNE
+
+/* name of the current device, read once per device */
+const char* current_device_name()
+{
+    static std::mutex mu;
+    static char names[16][256];
+    static bool known[16];
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 16)
+        return "";
+    std::lock_guard<std::mutex> lock(mu);
+    if (!known[dev]) {
+        cudaDeviceProp p;
+        if (cudaGetDeviceProperties(&p, dev) != cudaSuccess)
+            return "";
+        std::snprintf(names[dev], sizeof names[dev], "%s", p.name);
+        known[dev] = true;
+    }
+    return names[dev];
+}
+
 thread_local char g_err[512] = "";
 
 int32_t fail(int32_t code, const char* fmt, ...)
@@ -178,6 +212,23 @@ static int32_t resolve_opts(const NetEntry& e, const odevec_opts* in, odevec_opt
         return fail(OV_API_EINVAL, "unknown precision %d", o.precision);
     if (o.max_attempts <= 0)
         o.max_attempts = 1000000;
+    if (o.staging == 0 || o.jac_batch == 0 || o.ss_batch == 0 || o.max_wait == 0) {
+        /* options left at 0 take the tuned values for this GPU, if any */
+        const char* dev = nullptr;
+        for (const TuneEntry* t = g_tune; t->tag; ++t) {
+            if (t->precision != o.precision || t->group != o.group_size || std::strcmp(t->tag, e.tag) != 0)
+                continue;
+            if (!dev)
+                dev = current_device_name();
+            if (std::strcmp(t->device, dev) != 0)
+                continue;
+            if (o.staging == 0) o.staging = t->staging;
+            if (o.jac_batch == 0) o.jac_batch = t->jac_batch;
+            if (o.ss_batch == 0) o.ss_batch = t->ss_batch;
+            if (o.max_wait == 0) o.max_wait = t->max_wait;
+            break;
+        }
+    }
     if (o.jac_batch <= 0)
         o.jac_batch = 24;
     if (o.ss_batch <= 0)

@@ -10,7 +10,7 @@ from odevec_b200 import autotune as A
 
 
 def test_search_picks_fastest_and_skips_uncompiled():
-    cost = {1: 3.0, 2: None, 3: 2.0, 4: 2.5, 6: 1.5, 5: 1.0}
+    cost = {1: 3.0, 2: None, 3: 2.0, 4: 2.5, 6: 1.5, 7: 1.9, 8: 1.7, 5: 1.0}
 
     def timer(cfg):
         base = cost[cfg["staging"]]
@@ -23,6 +23,7 @@ def test_search_picks_fastest_and_skips_uncompiled():
     best, tried = A.search(timer, "fp64")
     assert best["staging"] == 6 and best["jac_batch"] == 16 and best["seconds"] == pytest.approx(1.35)
     assert all(c["staging"] != 2 for c, _ in tried)
+    assert len(tried) == len(A.BATCHES) * (len(A.STAGINGS) - 1)
     best32, _ = A.search(timer, "fp32_lu")
     assert best32["staging"] == 5  # FP32-only staging considered for fp32_lu
 
@@ -70,3 +71,16 @@ def test_tuned_solver_gives_identical_results(gpu_lib):
         out.append(y.cpu().numpy())
         gpu_lib.CloseOdevec(ode)
     assert np.array_equal(out[0], out[1])
+
+
+def test_c_table_mirrors_tuning_json():
+    import re
+    from odevec_b200 import build as B
+    text = open(B.write_tuning_table()).read()
+    rows = re.findall(r'OV_TUNE\("([^"]+)", (\d), (\d+), "([^"]+)", (-?\d+), (-?\d+), (-?\d+), (-?\d+)\)', text)
+    table = A.load()
+    assert len(rows) == len(table)
+    codes = {v: k for k, v in B.PREC_CODE.items()}
+    for tag, prec, grp, dev, st, jb, sb, mw in rows:
+        v = table[A.key(tag, codes[int(prec)], int(grp), dev)]
+        assert (v["staging"], v["jac_batch"], v["ss_batch"], v["max_wait"]) == (int(st), int(jb), int(sb), int(mw))
