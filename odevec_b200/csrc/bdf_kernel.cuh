@@ -156,15 +156,20 @@ struct LaneHist {
    budget; SHM places the Nordsieck history and the LU in shared memory. */
 template <int STAGE>
 struct StageCfg;
-template <> struct StageCfg<1> { static constexpr bool SHM = false, SOFT = false; static constexpr int BS = 128, MINB = 2; };
-template <> struct StageCfg<2> { static constexpr bool SHM = true,  SOFT = false; static constexpr int BS = 128, MINB = 1; };
-template <> struct StageCfg<3> { static constexpr bool SHM = false, SOFT = false; static constexpr int BS = 128, MINB = 3; };
-template <> struct StageCfg<4> { static constexpr bool SHM = false, SOFT = false; static constexpr int BS = 128, MINB = 4; };
-template <> struct StageCfg<5> { static constexpr bool SHM = true,  SOFT = false; static constexpr int BS = 192, MINB = 1; };
+/* SHM: 0 = history and LU in thread-local arrays, 1 = both in shared memory,
+   2 = the history in shared memory and the LU thread-local */
+template <> struct StageCfg<1> { static constexpr int SHM = 0; static constexpr bool SOFT = false; static constexpr int BS = 128, MINB = 2; };
+template <> struct StageCfg<2> { static constexpr int SHM = 1; static constexpr bool SOFT = false; static constexpr int BS = 128, MINB = 1; };
+template <> struct StageCfg<3> { static constexpr int SHM = 0; static constexpr bool SOFT = false; static constexpr int BS = 128, MINB = 3; };
+template <> struct StageCfg<4> { static constexpr int SHM = 0; static constexpr bool SOFT = false; static constexpr int BS = 128, MINB = 4; };
+template <> struct StageCfg<5> { static constexpr int SHM = 1; static constexpr bool SOFT = false; static constexpr int BS = 192, MINB = 1; };
 /* as 3, the same register budget, in one block of 384 threads per SM */
-template <> struct StageCfg<6> { static constexpr bool SHM = false, SOFT = false; static constexpr int BS = 384, MINB = 1; };
+template <> struct StageCfg<6> { static constexpr int SHM = 0; static constexpr bool SOFT = false; static constexpr int BS = 384, MINB = 1; };
 /* as 6, with the block's warps held in soft lockstep (SoftSync) */
-template <> struct StageCfg<8> { static constexpr bool SHM = false, SOFT = true;  static constexpr int BS = 384, MINB = 1; };
+template <> struct StageCfg<8> { static constexpr int SHM = 0; static constexpr bool SOFT = true;  static constexpr int BS = 384, MINB = 1; };
+/* soft lockstep, one block of 256 threads per SM, the history in shared
+   memory (the rest of L1 for the other per-cell arrays) */
+template <> struct StageCfg<9> { static constexpr int SHM = 2; static constexpr bool SOFT = true;  static constexpr int BS = 256, MINB = 1; };
 
 /* Soft lockstep.  The warps of a block wait for each other at the top of
    every trip of the cell loop, so they run the same phase code at the same
@@ -220,25 +225,33 @@ __device__ __forceinline__ void soft_leave(SoftSync* s, int lane)
 }
 
 
-template <class Net, class LUT, bool SHM, int BS>
+template <class Net, class LUT, int SHM, int BS>
 struct Staging;
 
 template <class Net, class LUT, int BS>
-struct Staging<Net, LUT, false, BS> { /* thread-local arrays (registers / local memory) */
+struct Staging<Net, LUT, 0, BS> { /* thread-local arrays (registers / local memory) */
     using Hist = double (*)[Net::ND];
     using LU = LUT*;
     static constexpr size_t smem_bytes = 0;
 };
 
 template <class Net, class LUT, int BS>
-struct Staging<Net, LUT, true, BS> { /* shared memory, [entry][lane] */
+struct Staging<Net, LUT, 1, BS> { /* shared memory, [entry][lane] */
     using Hist = LaneHist<Net::ND, BS>;
     using LU = LaneCol<LUT, BS>;
     static constexpr size_t hist_bytes = sizeof(double) * (MAXQ + 1) * Net::ND * BS;
     static constexpr size_t smem_bytes = hist_bytes + sizeof(LUT) * Net::NNZ * BS;
 };
 
-template <class Net, int G, class LUT, bool SHM = false, int BS = 128>
+template <class Net, class LUT, int BS>
+struct Staging<Net, LUT, 2, BS> { /* history in shared memory, LU thread-local */
+    using Hist = LaneHist<Net::ND, BS>;
+    using LU = LUT*;
+    static constexpr size_t hist_bytes = sizeof(double) * (MAXQ + 1) * Net::ND * BS;
+    static constexpr size_t smem_bytes = hist_bytes;
+};
+
+template <class Net, int G, class LUT, int SHM = 0, int BS = 128>
 struct Cell {
     static constexpr int N = Net::NEQ;  /* full state */
     static constexpr int ND = Net::ND;  /* solver state */
@@ -735,7 +748,7 @@ __device__ __forceinline__ int warp_count(bool b) { return __popc(__ballot_sync(
 template <class Net, int G, class LUT, int STAGE>
 __global__ void __launch_bounds__(StageCfg<STAGE>::BS, StageCfg<STAGE>::MINB) bdf_kernel(const LaunchArgs A)
 {
-    constexpr bool SHM = StageCfg<STAGE>::SHM;
+    constexpr int SHM = StageCfg<STAGE>::SHM;
     constexpr int BS = StageCfg<STAGE>::BS;
     using C = Cell<Net, G, LUT, SHM, BS>;
     constexpr int N = C::N;
@@ -746,18 +759,19 @@ __global__ void __launch_bounds__(StageCfg<STAGE>::BS, StageCfg<STAGE>::MINB) bd
         return;
 
     C c;
-    if constexpr (SHM) {
+    if constexpr (SHM != 0) {
         extern __shared__ __align__(16) unsigned char ov_smem[];
         c.yns = LaneHist<ND, BS>{reinterpret_cast<double*>(ov_smem) + threadIdx.x};
-        c.a = LaneCol<LUT, BS>{reinterpret_cast<LUT*>(ov_smem + Staging<Net, LUT, true, BS>::hist_bytes)
-                               + threadIdx.x};
+        if constexpr (SHM == 1)
+            c.a = LaneCol<LUT, BS>{reinterpret_cast<LUT*>(ov_smem + Staging<Net, LUT, 1, BS>::hist_bytes)
+                                   + threadIdx.x};
     }
-    double history[SHM ? 1 : MAXQ + 1][ND];
-    LUT lu_local[SHM ? 1 : C::NNZ];
-    if constexpr (!SHM) {
+    double history[SHM != 0 ? 1 : MAXQ + 1][ND];
+    LUT lu_local[SHM == 1 ? 1 : C::NNZ];
+    if constexpr (SHM == 0)
         c.yns = history;
+    if constexpr (SHM != 1)
         c.a = lu_local;
-    }
     int ph = PH_IDLE;
     int64_t cell = -1;
     bool write_y = false;
@@ -1150,7 +1164,14 @@ cudaError_t launch(const LaunchArgs& a, int block, int grid, cudaStream_t stream
 template <class Net, class LUT, int BS>
 constexpr bool shm_fits()
 {
-    return Staging<Net, LUT, true, BS>::smem_bytes <= 200 * 1024;
+    return Staging<Net, LUT, 1, BS>::smem_bytes <= 200 * 1024;
+}
+
+/* the same for the history alone */
+template <class Net, int BS>
+constexpr bool hist_fits()
+{
+    return Staging<Net, double, 2, BS>::smem_bytes <= 200 * 1024;
 }
 
 }  // namespace OV_MODE_NS
@@ -1163,8 +1184,9 @@ constexpr bool shm_fits()
    LU in shared memory, 1 block of 128; 3, 4 = thread-local, 3 or 4 blocks of
    128 (fewer registers, more warps); 5 = shared memory, 1 block of 192;
    6 = thread-local, 1 block of 384; 7 = one warp per cell (wpc_kernel.cuh;
-   constant-coefficient CSC variants); 8 = as 6 in soft lockstep.  Stages
-   2-8 exist for per-cell control (G = 1). */
+   constant-coefficient CSC variants); 8 = as 6 in soft lockstep; 9 = soft
+   lockstep in one block of 256 with the history in shared memory.  Stages
+   2-9 exist for per-cell control (G = 1). */
 #define OV_STAGE_CASE(NET, LU, ST)                                                               \
     if (stage == ST)                                                                             \
         return launch<NET, 1, LU, ST>(a, block, grid, s);
@@ -1182,6 +1204,9 @@ constexpr bool shm_fits()
             OV_STAGE_CASE(NET, double, 4)                                                        \
             OV_STAGE_CASE(NET, double, 6)                                                        \
             OV_STAGE_CASE(NET, double, 8)                                                        \
+            if constexpr (hist_fits<NET, 256>()) {                                               \
+                OV_STAGE_CASE(NET, double, 9)                                                    \
+            }                                                                                    \
             if constexpr (wpc_ok<NET, double>()) {                                               \
                 if (stage == 7)                                                                  \
                     return launch_wpc<NET, double>(a, grid, s);                                  \
@@ -1198,6 +1223,9 @@ constexpr bool shm_fits()
                 OV_STAGE_CASE(NET, float, 4)                                                     \
                 OV_STAGE_CASE(NET, float, 6)                                                     \
                 OV_STAGE_CASE(NET, float, 8)                                                     \
+                if constexpr (hist_fits<NET, 256>()) {                                           \
+                    OV_STAGE_CASE(NET, float, 9)                                                 \
+                }                                                                                \
                 if constexpr (wpc_ok<NET, float>()) {                                            \
                     if (stage == 7)                                                              \
                         return launch_wpc<NET, float>(a, grid, s);                               \

@@ -101,7 +101,7 @@ def test_scheduling_does_not_change_results(gpu_lib, precision):
         assert_bitwise(g, ref, "batch %s" % (batch,))
     # every staging, the block-synchronous one (6) included, with the
     # default batches and with per-cell blocks
-    for staging in (1, 2, 3, 4, 6, 8) + ((5,) if precision == "fp32_lu" else ()):
+    for staging in (1, 2, 3, 4, 6, 8, 9) + ((5,) if precision == "fp32_lu" else ()):
         for batch in [(0, 0, 0), (1, 1, -1)]:
             g = run_gpu(gpu_lib, wl, precision, batch=batch, staging=staging)
             assert_bitwise(g, ref, "staging %d batch %s" % (staging, batch))
@@ -326,7 +326,7 @@ def test_fp32_escalation_rescues_badly_conditioned_cells(gpu_lib):
 def test_ragged_sizes_bit_exact(gpu_lib, oracle, ncells):
     # cell counts that leave a warp, a block and the persistent grid partly empty
     wl = W.primordial(ncells=ncells, seed=ncells)
-    for staging in (3, 6, 8):
+    for staging in (3, 6, 8, 9):
         g = run_gpu(gpu_lib, wl, "fp64", staging=staging)
         assert_bitwise(g, run_oracle(oracle, wl), "ncells %d staging %d" % (ncells, staging))
 
