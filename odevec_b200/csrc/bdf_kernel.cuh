@@ -170,6 +170,8 @@ template <> struct StageCfg<8> { static constexpr int SHM = 0; static constexpr 
 /* soft lockstep, one block of 256 threads per SM, the history in shared
    memory (the rest of L1 for the other per-cell arrays) */
 template <> struct StageCfg<9> { static constexpr int SHM = 2; static constexpr bool SOFT = true;  static constexpr int BS = 256, MINB = 1; };
+/* as 9 with 320 threads (10 warps) per SM */
+template <> struct StageCfg<10> { static constexpr int SHM = 2; static constexpr bool SOFT = true;  static constexpr int BS = 320, MINB = 1; };
 
 /* Soft lockstep.  The warps of a block wait for each other at the top of
    every trip of the cell loop, so they run the same phase code at the same
@@ -1184,9 +1186,9 @@ constexpr bool hist_fits()
    LU in shared memory, 1 block of 128; 3, 4 = thread-local, 3 or 4 blocks of
    128 (fewer registers, more warps); 5 = shared memory, 1 block of 192;
    6 = thread-local, 1 block of 384; 7 = one warp per cell (wpc_kernel.cuh;
-   constant-coefficient CSC variants); 8 = as 6 in soft lockstep; 9 = soft
-   lockstep in one block of 256 with the history in shared memory.  Stages
-   2-9 exist for per-cell control (G = 1). */
+   constant-coefficient CSC variants); 8 = as 6 in soft lockstep; 9, 10 =
+   soft lockstep in one block of 256 or 320 with the history in shared
+   memory.  Stages 2-10 exist for per-cell control (G = 1). */
 #define OV_STAGE_CASE(NET, LU, ST)                                                               \
     if (stage == ST)                                                                             \
         return launch<NET, 1, LU, ST>(a, block, grid, s);
@@ -1207,6 +1209,9 @@ constexpr bool hist_fits()
             if constexpr (hist_fits<NET, 256>()) {                                               \
                 OV_STAGE_CASE(NET, double, 9)                                                    \
             }                                                                                    \
+            if constexpr (hist_fits<NET, 320>()) {                                               \
+                OV_STAGE_CASE(NET, double, 10)                                                   \
+            }                                                                                    \
             if constexpr (wpc_ok<NET, double>()) {                                               \
                 if (stage == 7)                                                                  \
                     return launch_wpc<NET, double>(a, grid, s);                                  \
@@ -1225,6 +1230,9 @@ constexpr bool hist_fits()
                 OV_STAGE_CASE(NET, float, 8)                                                     \
                 if constexpr (hist_fits<NET, 256>()) {                                           \
                     OV_STAGE_CASE(NET, float, 9)                                                 \
+                }                                                                                \
+                if constexpr (hist_fits<NET, 320>()) {                                           \
+                    OV_STAGE_CASE(NET, float, 10)                                                \
                 }                                                                                \
                 if constexpr (wpc_ok<NET, float>()) {                                            \
                     if (stage == 7)                                                              \
