@@ -21,7 +21,7 @@ class SolveMany:
     matching cell counts (time/dt updated in place, y in place).  Each ode
     must be initialised and must not be shared between jobs."""
 
-    def __init__(self, jobs: Sequence[tuple], share: bool = True, blocks_per_sm: int = 3):
+    def __init__(self, jobs: Sequence[tuple], share: bool = True):
         import torch
         self.torch = torch
         self.jobs: List[tuple] = list(jobs)
@@ -35,7 +35,8 @@ class SolveMany:
             sms = torch.cuda.get_device_properties(self.jobs[0][4].device).multi_processor_count
             k = len(self.jobs)
             for ode, *_ in self.jobs:
-                ode.grid_blocks = max(sms, sms * blocks_per_sm // k)
+                # 1/k of the resident blocks of the staging each solve runs with
+                ode.grid_blocks = max(1, sms * S.BLOCKS_PER_SM.get(ode.staging, 3) // k)
         self.graph = None
         self.statuses = None
 

@@ -179,7 +179,7 @@ class GpuBackend:
     CUDA stream; launches are asynchronous and completion is an event."""
 
     def __init__(self, precision: str = "fp32_lu", device: str = "cuda", fair_share: bool = True,
-                 small_cells: int = 16384, blocks_per_sm: int = 3):
+                 small_cells: int = 16384):
         import torch
         from . import solver as S
         self.S = S
@@ -189,8 +189,6 @@ class GpuBackend:
         self.fair_share = fair_share
         self.small_cells = small_cells
         self.sms = torch.cuda.get_device_properties(device).multi_processor_count
-        # resident blocks of the per-cell kernels (3 blocks of 128 threads per SM)
-        self.capacity = self.sms * blocks_per_sm
 
     def _solver(self, r: Request):
         # one solver handle per request: each owns its cell counter, so
@@ -226,7 +224,9 @@ class GpuBackend:
         torch = self.torch
         r = h["r"]
         if self.fair_share:
-            h["ode"].grid_blocks = max(self.sms, self.capacity // max(active, 1))
+            # 1/k of the resident blocks of the staging this request runs with
+            capacity = self.sms * self.S.BLOCKS_PER_SM.get(h["ode"].staging, 3)
+            h["ode"].grid_blocks = max(1, capacity // max(active, 1))
         with torch.cuda.stream(h["stream"]):
             h["ts"].fill_(r.dt_hydro * (step + 1))
             if step > 0:
