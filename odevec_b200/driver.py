@@ -279,11 +279,26 @@ def main(argv=None):
         sch = orego_schedule(a.cells, t_end=a.t_end)
     else:
         sch = primordial_schedule(a.cells)
-    run_schedule(sch, a.precision, a.graph, a.chunk)  # warm-up (and graph capture on its own ladder)
+    ode = S.Odevec(sch.network, RelativeTolerance=sch.rtol, AbsoluteTolerance=sch.atol, MinimalTimestep=sch.dt_min,
+                   nvector=sch.group, precision=a.precision, raise_on_failure=False)
+    S.InitOdevec(ode)
+    y0 = torch.tensor(sch.y0, device="cuda")
+    y = y0.clone()
+    rho = None if sch.rho is None else torch.tensor(sch.rho, device="cuda")
+    lad = Ladder(ode, y, sch.time, sch.dt, sch.t_stops, rho=rho, dt_reset=sch.dt_reset, graph=a.graph,
+                 chunk=a.chunk)
+    t_in, d_in = lad.t.clone(), lad.d.clone()
+    lad.run()  # warm-up; with --graph this captures the graphs
+    y.copy_(y0)
+    lad.t.copy_(t_in)
+    lad.d.copy_(d_in)
     torch.cuda.synchronize()
     t0 = time.perf_counter()
-    y, t, d, st = run_schedule(sch, a.precision, a.graph, a.chunk)
+    _, _, st = lad.run()
+    torch.cuda.synchronize()
     el = time.perf_counter() - t0
+    st = st.cpu().numpy()
+    S.CloseOdevec(ode)
     print(json.dumps({"schedule": a.schedule, "network": sch.network, "cells": a.cells, "calls": len(sch.t_stops),
                       "graph": a.graph, "precision": a.precision, "seconds": el,
                       "ms_per_call": 1e3 * el / len(sch.t_stops), "failed_cells": int((st != 0).sum())}))

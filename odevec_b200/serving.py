@@ -179,7 +179,7 @@ class GpuBackend:
     CUDA stream; launches are asynchronous and completion is an event."""
 
     def __init__(self, precision: str = "fp32_lu", device: str = "cuda", fair_share: bool = True,
-                 small_cells: int = 16384):
+                 small_cells: int = 16384, staging: int = 3):
         import torch
         from . import solver as S
         self.S = S
@@ -188,6 +188,11 @@ class GpuBackend:
         self.device = device
         self.fair_share = fair_share
         self.small_cells = small_cells
+        # launch shape for requests: three 128-thread blocks per SM, so blocks
+        # of up to three requests share an SM.  The single-solve optimum (one
+        # block per SM holding its shared memory) would leave SMs to a single
+        # request and most of the device idle under many small requests.
+        self.staging = staging
         self.sms = torch.cuda.get_device_properties(device).multi_processor_count
 
     def _solver(self, r: Request):
@@ -195,7 +200,7 @@ class GpuBackend:
         # concurrent launches on different streams never share one
         ode = self.S.Odevec(r.network, RelativeTolerance=r.rtol, AbsoluteTolerance=r.atol,
                             MinimalTimestep=r.dt_min, nvector=1, precision=self.precision,
-                            raise_on_failure=False)
+                            raise_on_failure=False, staging=self.staging)
         self.S.InitOdevec(ode)
         return ode
 
