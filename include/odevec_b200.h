@@ -84,8 +84,9 @@ typedef struct odevec_opts {
     int32_t jac_batch;
     int32_t ss_batch;
     int32_t max_wait;
-    /* launch shape, no effect on results.  staging: 0 = automatic (3 for
-       per-cell control up to 32 species, 1 above and for lockstep); 1 = per-cell arrays in registers /
+    /* launch shape, no effect on results.  staging: 0 = automatic (the
+       library's tuning table for this GPU where it has the variant, else 3
+       for per-cell control up to 32 species, 1 above and for lockstep); 1 = per-cell arrays in registers /
        local memory, 2 blocks of 128 threads per SM; 2 = history and LU in
        shared memory, 1 block of 128 (where they fit); 3, 4 = as 1 with 3 or 4
        blocks per SM (fewer registers, more warps); 5 = as 2 with 192-thread

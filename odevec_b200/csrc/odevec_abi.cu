@@ -402,8 +402,8 @@ static int32_t solve_impl(odevec_solver* s, int64_t ncells, double* y, double* t
         return fail(OV_API_ECUDA, "odevec_solve: %s", cudaGetErrorString(err));
     const int lu = o.precision == OV_PREC_FP32_LU ? 1 : 0;
     ov::launch_fn fn = o.precision == OV_PREC_FP64 ? e.exact : e.fma;
-    /* automatic: thread-local arrays with 3 blocks of 128 per SM for per-cell
-       control (the fastest measured configuration), 2 blocks for lockstep */
+    /* automatic (options left at 0): the tuning table for this GPU, else
+       auto_staging() */
     const int stage = o.staging ? o.staging : auto_staging(e, o.group_size);
     const bool escalate = lu && !o.no_escalation;
     const int neq = e.sizes[0];
