@@ -3,10 +3,14 @@
 
 Metric: PRIMORDIAL cells/s to t_end at rtol 1e-6 (the 16-species primordial
 network, 1,048,576 cells per GPU, per-cell temperature and t_end), reported
-for the FP32-LU/FP64-residual form (``value``) beside the plain FP64 path
-and the FP64 path with fused multiply-add.  One step = one complete solve of
-all cells from the initial state to their t_end; inputs are reset from a
-device copy before each step (159 MB of inputs, larger than the 126 MB L2).
+for the FP32-LU/FP64-residual form (``value``) beside the FP64 form of the
+same kernel (bit-identical to the CPU oracle), the FP64 form with fused
+multiply-add, and a plain FP64 port (one cell per thread for the whole
+launch, no batching).  Launch options come from the autotuner's table
+(odevec_b200/tuning.json).  One step = one complete solve of all cells from
+the initial state to their t_end; inputs are reset from a device copy before
+each step (159 MB of inputs, larger than the 126 MB L2).  ``e2e`` is the same
+solve through the C-ABI host entry with pinned host buffers.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl product|reference]
 

@@ -95,7 +95,9 @@ typedef struct odevec_opts {
        networks in CSC packaging); 8 = as 6 with the block's warps held in
        soft lockstep at the top of every trip (bounded polling, no barrier);
        9, 10 = soft lockstep in one block of 256 or 320 threads per SM with the
-       history in shared memory (where it fits) (2-10: per-cell control only).  block_threads (a multiple of 32 up to the block of
+       history in shared memory (where it fits); 11 = soft lockstep in one
+       block of 192 with history and LU in shared memory (where they fit,
+       typically with FP32 factors) (2-11: per-cell control only).  block_threads (a multiple of 32 up to the block of
        the staging) and grid_blocks: 0 = automatic (persistent grid filling
        every SM) */
     int32_t staging;

@@ -29,10 +29,13 @@
  * the reference, so leaving them out changes no result.  Norms still divide
  * by the full neq.
  *
- * Per-cell state lives in thread-local arrays with compile-time indices
- * (Nordsieck history y_NS(0:5), en, en_old, error weights, packed LU);
- * loops over the runtime order are unrolled to the maximum order with
- * predicates so no array is indexed dynamically.
+ * Per-cell state: en, en_old, error weights, the state and the packed LU in
+ * thread-local arrays with compile-time indices (the LU in shared memory for
+ * stagings 2 and 5); the Nordsieck history y_NS(0:5), which loops over the
+ * runtime order index, in a thread-local array or, for stagings 2, 5, 9 and
+ * 10, in shared memory laid out [entry][lane].  The staging (StageCfg) also
+ * fixes the block size, the blocks per SM and whether the block's warps run
+ * in soft lockstep.
  *
  * Every loop is bounded: at most max_attempts predictor attempts per cell
  * (status OV_ERR_MAX_STEPS), at most 4 Newton iterations per attempt and 10
@@ -172,6 +175,9 @@ template <> struct StageCfg<8> { static constexpr int SHM = 0; static constexpr 
 template <> struct StageCfg<9> { static constexpr int SHM = 2; static constexpr bool SOFT = true;  static constexpr int BS = 256, MINB = 1; };
 /* as 9 with 320 threads (10 warps) per SM */
 template <> struct StageCfg<10> { static constexpr int SHM = 2; static constexpr bool SOFT = true;  static constexpr int BS = 320, MINB = 1; };
+/* soft lockstep, one block of 192 threads per SM with history and LU in
+   shared memory (fits with FP32 factors) */
+template <> struct StageCfg<11> { static constexpr int SHM = 1; static constexpr bool SOFT = true;  static constexpr int BS = 192, MINB = 1; };
 
 /* Soft lockstep.  The warps of a block wait for each other at the top of
    every trip of the cell loop, so they run the same phase code at the same
@@ -1188,7 +1194,9 @@ constexpr bool hist_fits()
    6 = thread-local, 1 block of 384; 7 = one warp per cell (wpc_kernel.cuh;
    constant-coefficient CSC variants); 8 = as 6 in soft lockstep; 9, 10 =
    soft lockstep in one block of 256 or 320 with the history in shared
-   memory.  Stages 2-10 exist for per-cell control (G = 1). */
+   memory; 11 = soft lockstep in one block of 192 with history and LU in
+   shared memory (where they fit).  Stages 2-11 exist for per-cell control
+   (G = 1). */
 #define OV_STAGE_CASE(NET, LU, ST)                                                               \
     if (stage == ST)                                                                             \
         return launch<NET, 1, LU, ST>(a, block, grid, s);
@@ -1212,6 +1220,9 @@ constexpr bool hist_fits()
             if constexpr (hist_fits<NET, 320>()) {                                               \
                 OV_STAGE_CASE(NET, double, 10)                                                   \
             }                                                                                    \
+            if constexpr (shm_fits<NET, double, 192>()) {                                        \
+                OV_STAGE_CASE(NET, double, 11)                                                   \
+            }                                                                                    \
             if constexpr (wpc_ok<NET, double>()) {                                               \
                 if (stage == 7)                                                                  \
                     return launch_wpc<NET, double>(a, grid, s);                                  \
@@ -1233,6 +1244,9 @@ constexpr bool hist_fits()
                 }                                                                                \
                 if constexpr (hist_fits<NET, 320>()) {                                           \
                     OV_STAGE_CASE(NET, float, 10)                                                \
+                }                                                                                \
+                if constexpr (shm_fits<NET, float, 192>()) {                                     \
+                    OV_STAGE_CASE(NET, float, 11)                                                \
                 }                                                                                \
                 if constexpr (wpc_ok<NET, float>()) {                                            \
                     if (stage == 7)                                                              \

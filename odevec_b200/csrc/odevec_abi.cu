@@ -237,8 +237,8 @@ static int32_t resolve_opts(const NetEntry& e, const odevec_opts* in, odevec_opt
         o.max_wait = o.max_wait < 0 ? 0 : 8;
     if (o.jac_batch > 32 || o.ss_batch > 32)
         return fail(OV_API_EINVAL, "jac_batch and ss_batch must be <= 32");
-    if (o.staging < 0 || o.staging > 10)
-        return fail(OV_API_EINVAL, "staging must be 0..10");
+    if (o.staging < 0 || o.staging > 11)
+        return fail(OV_API_EINVAL, "staging must be 0..11");
     if (o.block_threads < 0 || o.block_threads > 128 || o.block_threads % 32)
         return fail(OV_API_EINVAL, "block_threads must be 32, 64, 96 or 128 (0: automatic)");
     if (o.grid_blocks < 0)
@@ -448,9 +448,10 @@ static int32_t solve_impl(odevec_solver* s, int64_t ncells, double* y, double* t
             b.stats = nullptr;
             b.run_if = s->d_queue + 1;
             err = cudaMemsetAsync(s->d_queue, 0, sizeof(unsigned long long), st);
-            /* staging 5 exists for FP32 factors only: the FP64 re-solve of
-               such a launch uses the thread-local default */
-            const int stage64 = stage == 5 ? 3 : stage;
+            /* the FP64 re-solve runs rarely and only for failed cells: it
+               uses the thread-local staging compiled for every variant (some
+               stagings exist for FP32 factors only) */
+            const int stage64 = o.group_size == 1 ? 3 : 1;
             if (err == cudaSuccess)
                 err = e.fma(b, o.group_size, 0, stage64, o.block_threads, o.grid_blocks, st);
         }

@@ -36,7 +36,7 @@ class SolveMany:
             k = len(self.jobs)
             for ode, *_ in self.jobs:
                 # 1/k of the resident blocks of the staging each solve runs with
-                ode.grid_blocks = max(1, sms * S.BLOCKS_PER_SM.get(ode.staging, 3) // k)
+                ode.grid_blocks = max(sms, sms * S.BLOCKS_PER_SM.get(ode.staging, 3) // k)
         self.graph = None
         self.statuses = None
 

@@ -25,7 +25,8 @@ Sharing the device: the solve kernel is persistent (its blocks stay resident
 until the request's cells run out), so a launch that takes every SM would
 hold back every request behind it.  With fair sharing, each launch gets
 1/k of the device's resident blocks when k requests are in flight (all of
-them when it runs alone), and requests of at most `small_cells` cells run
+them when it runs alone; never fewer than one block per SM), and requests
+of at most `small_cells` cells run
 on a higher-priority stream, so their blocks are placed first whenever
 blocks retire.
 
@@ -229,9 +230,11 @@ class GpuBackend:
         torch = self.torch
         r = h["r"]
         if self.fair_share:
-            # 1/k of the resident blocks of the staging this request runs with
+            # 1/k of the resident blocks of the staging this request runs with,
+            # but at least one block per SM: a persistent grid keeps its size
+            # after other requests finish, so a narrower one would leave SMs idle
             capacity = self.sms * self.S.BLOCKS_PER_SM.get(h["ode"].staging, 3)
-            h["ode"].grid_blocks = max(1, capacity // max(active, 1))
+            h["ode"].grid_blocks = max(self.sms, capacity // max(active, 1))
         with torch.cuda.stream(h["stream"]):
             h["ts"].fill_(r.dt_hydro * (step + 1))
             if step > 0:

@@ -101,7 +101,7 @@ def test_scheduling_does_not_change_results(gpu_lib, precision):
         assert_bitwise(g, ref, "batch %s" % (batch,))
     # every staging, the block-synchronous one (6) included, with the
     # default batches and with per-cell blocks
-    for staging in (1, 2, 3, 4, 6, 8, 9, 10) + ((5,) if precision == "fp32_lu" else ()):
+    for staging in (1, 2, 3, 4, 6, 8, 9, 10) + ((5, 11) if precision == "fp32_lu" else ()):
         for batch in [(0, 0, 0), (1, 1, -1)]:
             g = run_gpu(gpu_lib, wl, precision, batch=batch, staging=staging)
             assert_bitwise(g, ref, "staging %d batch %s" % (staging, batch))
