@@ -31,11 +31,11 @@
  *
  * Per-cell state: en, en_old, error weights, the state and the packed LU in
  * thread-local arrays with compile-time indices (the LU in shared memory for
- * stagings 2 and 5); the Nordsieck history y_NS(0:5), which loops over the
- * runtime order index, in a thread-local array or, for stagings 2, 5, 9 and
- * 10, in shared memory laid out [entry][lane].  The staging (StageCfg) also
- * fixes the block size, the blocks per SM and whether the block's warps run
- * in soft lockstep.
+ * stagings 2, 5 and 11); the Nordsieck history y_NS(0:5), which loops over
+ * the runtime order index, in a thread-local array or, for stagings 2, 5 and
+ * 9-11, in shared memory laid out [entry][lane].  The staging (StageCfg) also
+ * fixes the block size, the blocks per SM, whether the block's warps run in
+ * soft lockstep and how often idle lanes take new cells.
  *
  * Every loop is bounded: at most max_attempts predictor attempts per cell
  * (status OV_ERR_MAX_STEPS), at most 4 Newton iterations per attempt and 10
@@ -160,24 +160,26 @@ struct LaneHist {
 template <int STAGE>
 struct StageCfg;
 /* SHM: 0 = history and LU in thread-local arrays, 1 = both in shared memory,
-   2 = the history in shared memory and the LU thread-local */
-template <> struct StageCfg<1> { static constexpr int SHM = 0; static constexpr bool SOFT = false; static constexpr int BS = 128, MINB = 2; };
-template <> struct StageCfg<2> { static constexpr int SHM = 1; static constexpr bool SOFT = false; static constexpr int BS = 128, MINB = 1; };
-template <> struct StageCfg<3> { static constexpr int SHM = 0; static constexpr bool SOFT = false; static constexpr int BS = 128, MINB = 3; };
-template <> struct StageCfg<4> { static constexpr int SHM = 0; static constexpr bool SOFT = false; static constexpr int BS = 128, MINB = 4; };
-template <> struct StageCfg<5> { static constexpr int SHM = 1; static constexpr bool SOFT = false; static constexpr int BS = 192, MINB = 1; };
+   2 = the history in shared memory and the LU thread-local.  REFILL: idle
+   lanes take new cells on every REFILL-th trip of the cell loop only; the
+   lockstep stagings align the cell set-ups of all their warps that way. */
+template <> struct StageCfg<1> { static constexpr int SHM = 0; static constexpr bool SOFT = false; static constexpr int BS = 128, MINB = 2, REFILL = 1; };
+template <> struct StageCfg<2> { static constexpr int SHM = 1; static constexpr bool SOFT = false; static constexpr int BS = 128, MINB = 1, REFILL = 1; };
+template <> struct StageCfg<3> { static constexpr int SHM = 0; static constexpr bool SOFT = false; static constexpr int BS = 128, MINB = 3, REFILL = 1; };
+template <> struct StageCfg<4> { static constexpr int SHM = 0; static constexpr bool SOFT = false; static constexpr int BS = 128, MINB = 4, REFILL = 1; };
+template <> struct StageCfg<5> { static constexpr int SHM = 1; static constexpr bool SOFT = false; static constexpr int BS = 192, MINB = 1, REFILL = 1; };
 /* as 3, the same register budget, in one block of 384 threads per SM */
-template <> struct StageCfg<6> { static constexpr int SHM = 0; static constexpr bool SOFT = false; static constexpr int BS = 384, MINB = 1; };
+template <> struct StageCfg<6> { static constexpr int SHM = 0; static constexpr bool SOFT = false; static constexpr int BS = 384, MINB = 1, REFILL = 1; };
 /* as 6, with the block's warps held in soft lockstep (SoftSync) */
-template <> struct StageCfg<8> { static constexpr int SHM = 0; static constexpr bool SOFT = true;  static constexpr int BS = 384, MINB = 1; };
+template <> struct StageCfg<8> { static constexpr int SHM = 0; static constexpr bool SOFT = true;  static constexpr int BS = 384, MINB = 1, REFILL = 16; };
 /* soft lockstep, one block of 256 threads per SM, the history in shared
    memory (the rest of L1 for the other per-cell arrays) */
-template <> struct StageCfg<9> { static constexpr int SHM = 2; static constexpr bool SOFT = true;  static constexpr int BS = 256, MINB = 1; };
+template <> struct StageCfg<9> { static constexpr int SHM = 2; static constexpr bool SOFT = true;  static constexpr int BS = 256, MINB = 1, REFILL = 16; };
 /* as 9 with 320 threads (10 warps) per SM */
-template <> struct StageCfg<10> { static constexpr int SHM = 2; static constexpr bool SOFT = true;  static constexpr int BS = 320, MINB = 1; };
+template <> struct StageCfg<10> { static constexpr int SHM = 2; static constexpr bool SOFT = true;  static constexpr int BS = 320, MINB = 1, REFILL = 16; };
 /* soft lockstep, one block of 192 threads per SM with history and LU in
    shared memory (fits with FP32 factors) */
-template <> struct StageCfg<11> { static constexpr int SHM = 1; static constexpr bool SOFT = true;  static constexpr int BS = 192, MINB = 1; };
+template <> struct StageCfg<11> { static constexpr int SHM = 1; static constexpr bool SOFT = true;  static constexpr int BS = 192, MINB = 1, REFILL = 16; };
 
 /* Soft lockstep.  The warps of a block wait for each other at the top of
    every trip of the cell loop, so they run the same phase code at the same
@@ -793,12 +795,19 @@ __global__ void __launch_bounds__(StageCfg<STAGE>::BS, StageCfg<STAGE>::MINB) bd
         __syncthreads(); /* once, at entry, with every thread converged */
     }
 
+    unsigned trip = 0;
     for (;;) {
         /* ---- 1. idle lanes take new cells ---------------------------- */
         if (G == 1) {
             if constexpr (StageCfg<STAGE>::SOFT)
                 soft_sync(&soft, lane);
-            const unsigned need = __ballot_sync(FULL, ph == PH_IDLE);
+            /* with REFILL > 1, idle lanes wait for every REFILL-th trip, the
+               same trip in every warp of a lockstep block, so the costly
+               cell set-up (loads, temperature rates, first right-hand side)
+               runs in all warps at once instead of stretching random trips */
+            const bool refill = StageCfg<STAGE>::REFILL <= 1 || trip % StageCfg<STAGE>::REFILL == 0u;
+            ++trip;
+            const unsigned need = refill ? __ballot_sync(FULL, ph == PH_IDLE) : 0u;
             if (need) {
                 const int leader = __ffs(need) - 1;
                 unsigned long long base = 0;
@@ -1195,7 +1204,8 @@ constexpr bool hist_fits()
    constant-coefficient CSC variants); 8 = as 6 in soft lockstep; 9, 10 =
    soft lockstep in one block of 256 or 320 with the history in shared
    memory; 11 = soft lockstep in one block of 192 with history and LU in
-   shared memory (where they fit).  Stages 2-11 exist for per-cell control
+   shared memory (where they fit).  The lockstep stagings 8-11 refill idle
+   lanes on every 16th trip.  Stages 2-11 exist for per-cell control
    (G = 1). */
 #define OV_STAGE_CASE(NET, LU, ST)                                                               \
     if (stage == ST)                                                                             \

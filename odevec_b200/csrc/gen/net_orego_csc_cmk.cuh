@@ -148,10 +148,13 @@ struct ov_net_orego_csc_cmk {
      pointer or an accessor whose operator[] yields T& */
   template <class T, class A> OV_HD static OV_INLINE void lu_factor(A a) {
     (void)a;
-    a[4] = a[4] / a[0];
+    a[0] = ov_pivot<T>(a[0]);
+    a[4] = ov_divp<T>(a[4], a[0]);
     a[5] = a[5] - a[4]*a[1];
-    a[5] = a[5] / a[2];
+    a[2] = ov_pivot<T>(a[2]);
+    a[5] = ov_divp<T>(a[5], a[2]);
     a[6] = a[6] - a[5]*a[3];
+    a[6] = ov_pivot<T>(a[6]);
   }
   /* x = P^-1 r on the dynamic block; r, x over solver-state indices.  sc/isc
      scale entry i by sc[i] on the way in and isc[i] on the way out (pass
@@ -162,11 +165,11 @@ struct ov_net_orego_csc_cmk {
     T d0 = (T)(r[2]*OV_SC(2));
     T d1 = (T)(r[1]*OV_SC(1));
     T d2 = (T)(r[0]*OV_SC(0));
-    d0 = d0 / a[0];
+    d0 = ov_divp<T>(d0, a[0]);
     d1 = d1 - d0*a[1];
-    d1 = d1 / a[2];
+    d1 = ov_divp<T>(d1, a[2]);
     d2 = d2 - d1*a[3];
-    d2 = d2 / a[6];
+    d2 = ov_divp<T>(d2, a[6]);
     d0 = d0 - d2*a[4];
     d1 = d1 - d2*a[5];
     x[2] = (double)d0*OV_ISC(2);

@@ -63,6 +63,9 @@ struct ov_net_orego_dense_none_lu2 {
      pointer or an accessor whose operator[] yields T& */
   template <class T, class A> OV_HD static OV_INLINE void lu_factor(A a) {
     (void)a;
+    a[7] = ov_pivot<T>(a[7]);
+    a[4] = ov_pivot<T>(a[4]);
+    a[0] = ov_pivot<T>(a[0]);
   }
   /* x = P^-1 r on the dynamic block; r, x over solver-state indices.  sc/isc
      scale entry i by sc[i] on the way in and isc[i] on the way out (pass
@@ -75,9 +78,9 @@ struct ov_net_orego_dense_none_lu2 {
     T d2 = (T)(r[2]*OV_SC(2));
     d1 = d1 - a[1]*d0;
     d2 = d2 - (a[2]*d0 + a[5]*d1);
-    d2 = d2 / a[7];
-    d1 = (d1 - a[6]*d2) / a[4];
-    d0 = (d0 - a[3]*d1) / a[0];
+    d2 = ov_divp<T>(d2, a[7]);
+    d1 = ov_divp<T>((d1 - a[6]*d2), a[4]);
+    d0 = ov_divp<T>((d0 - a[3]*d1), a[0]);
     x[0] = (double)d0*OV_ISC(0);
     x[1] = (double)d1*OV_ISC(1);
     x[2] = (double)d2*OV_ISC(2);

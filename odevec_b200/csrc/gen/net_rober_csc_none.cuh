@@ -152,12 +152,15 @@ struct ov_net_rober_csc_none {
      pointer or an accessor whose operator[] yields T& */
   template <class T, class A> OV_HD static OV_INLINE void lu_factor(A a) {
     (void)a;
-    a[2] = a[2] / a[0];
+    a[0] = ov_pivot<T>(a[0]);
+    a[2] = ov_divp<T>(a[2], a[0]);
     a[3] = a[3] - a[2]*a[1];
-    a[5] = a[5] / a[0];
+    a[5] = ov_divp<T>(a[5], a[0]);
     a[6] = a[6] - a[5]*a[1];
-    a[6] = a[6] / a[3];
+    a[3] = ov_pivot<T>(a[3]);
+    a[6] = ov_divp<T>(a[6], a[3]);
     a[7] = a[7] - a[6]*a[4];
+    a[7] = ov_pivot<T>(a[7]);
   }
   /* x = P^-1 r on the dynamic block; r, x over solver-state indices.  sc/isc
      scale entry i by sc[i] on the way in and isc[i] on the way out (pass
@@ -168,11 +171,11 @@ struct ov_net_rober_csc_none {
     T d0 = (T)(r[0]*OV_SC(0));
     T d1 = (T)(r[1]*OV_SC(1));
     T d2 = (T)(r[2]*OV_SC(2));
-    d0 = d0 / a[0];
+    d0 = ov_divp<T>(d0, a[0]);
     d1 = d1 - d0*a[1];
-    d1 = d1 / a[3];
+    d1 = ov_divp<T>(d1, a[3]);
     d2 = d2 - d1*a[4];
-    d2 = d2 / a[7];
+    d2 = ov_divp<T>(d2, a[7]);
     d0 = d0 - d2*a[5];
     d1 = d1 - d2*a[6];
     d0 = d0 - d1*a[2];

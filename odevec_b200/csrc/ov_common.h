@@ -184,4 +184,21 @@ OV_HD static OV_INLINE double ov_pow(double x, double y)
     return ov_exp(y * ov_log(x));
 }
 
+/* Pivots of the numeric LU.  In FP64 the factorisation and the solves divide
+   by each pivot as the reference does (src/odevec.F90:906-969, :864-889).
+   An FP32 LU stores each pivot's reciprocal in place once the pivot is final
+   (ov_pivot) and multiplies by it (ov_divp): one correctly rounded division
+   per pivot instead of one per use, at most one more rounding per product,
+   which the modified Newton iteration's FP64 residual absorbs. */
+#ifdef __cplusplus
+template <class T>
+OV_HD static OV_INLINE T ov_pivot(T p) { return p; }
+template <>
+OV_HD OV_INLINE float ov_pivot<float>(float p) { return 1.0f / p; }
+template <class T>
+OV_HD static OV_INLINE T ov_divp(T x, T p) { return x / p; }
+template <>
+OV_HD OV_INLINE float ov_divp<float>(float x, float p) { return x * p; }
+#endif
+
 #endif /* OV_COMMON_H */

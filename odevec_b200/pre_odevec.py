@@ -543,6 +543,53 @@ def _reduced(sysm: System):
     return dyn, dpos, kmap
 
 
+_DIV_LINE = re.compile(r"^(\S+) = (.+) / a\[(\d+)\];$")
+
+
+def reciprocal_pivots(factor: List[str], solve: List[str]):
+    """Rewrites the straight-line factorisation and solve so that every
+    division x / a[p] becomes ov_divp<T>(x, a[p]), and the factorisation sets
+    a[p] = ov_pivot<T>(a[p]) once the pivot a[p] is final: before the first
+    factor line that divides by it, or at the end when only the solve does.
+    ov_pivot and ov_divp are the identity and a division in FP64, so the FP64
+    code divides exactly as the reference; an FP32 LU keeps reciprocals.
+    Raises ValueError if a pivot is read other than as a divisor after that
+    point (the factorisations emitted here never do)."""
+    def rewrite(lines):
+        out, used = [], []
+        for ln in lines:
+            m = _DIV_LINE.match(ln)
+            if m:
+                p = int(m.group(3))
+                used.append(p)
+                ln = "%s = ov_divp<T>(%s, a[%d]);" % (m.group(1), m.group(2), p)
+            out.append(ln)
+        return out, used
+    f_out, f_used = rewrite(factor)
+    s_out, s_used = rewrite(solve)
+    first = {}
+    for i, ln in enumerate(factor):
+        m = _DIV_LINE.match(ln)
+        if m:
+            first.setdefault(int(m.group(3)), i)
+    at = {}
+    for p in dict.fromkeys(f_used + s_used):
+        i = first.get(p, len(factor))
+        ref = re.compile(r"a\[%d\](?!\d)" % p)
+        for ln in factor[i:] + solve:
+            m = _DIV_LINE.match(ln)
+            rest = "%s = %s" % (m.group(1), m.group(2)) if m else ln
+            if ref.search(rest):
+                raise ValueError("pivot a[%d] is used other than as a divisor after it is final" % p)
+        at.setdefault(i, []).append(p)
+    res = []
+    for i in range(len(factor) + 1):
+        res += ["a[%d] = ov_pivot<T>(a[%d]);" % (p, p) for p in at.get(i, [])]
+        if i < len(factor):
+            res.append(f_out[i])
+    return res, s_out
+
+
 def _remap_a(line: str, kmap: Dict[int, int]) -> str:
     return re.sub(r"a\[(\d+)\]", lambda m: "a[%d]" % kmap[int(m.group(1))], line)
 
@@ -638,10 +685,12 @@ def emit_cuda_header(sysm: System) -> str:
     L.append("  }")
     L.append("  /* in-place numeric LU of the packed dynamic block a[0..NNZ-1]; A is a")
     L.append("     pointer or an accessor whose operator[] yields T& */")
+    f_lines, s_lines = reciprocal_pivots([_remap_a(l, kmap) for l in _lu_factor_lines(sysm)],
+                                         [_remap_a(l, kmap) for l in _lu_solve_lines(sysm, dpos=dpos)])
     L.append("  template <class T, class A> OV_HD static OV_INLINE void lu_factor(A a) {")
     L.append("    (void)a;")
-    for ln in _lu_factor_lines(sysm):
-        L.append("    " + _remap_a(ln, kmap))
+    for ln in f_lines:
+        L.append("    " + ln)
     L.append("  }")
     L.append("  /* x = P^-1 r on the dynamic block; r, x over solver-state indices.  sc/isc")
     L.append("     scale entry i by sc[i] on the way in and isc[i] on the way out (pass")
@@ -651,8 +700,8 @@ def emit_cuda_header(sysm: System) -> str:
              "const double* OV_RESTRICT isc) {")
     L.append("#define OV_SC(i) (sc ? sc[i] : 1.0)")
     L.append("#define OV_ISC(i) (isc ? isc[i] : 1.0)")
-    for ln in _lu_solve_lines(sysm, dpos=dpos):
-        L.append("    " + _remap_a(ln, kmap))
+    for ln in s_lines:
+        L.append("    " + ln)
     L.append("#undef OV_SC")
     L.append("#undef OV_ISC")
     L.append("  }")

@@ -8,6 +8,7 @@ the values of its generated symbolic factors (tests/golden/make_golden.py).
 """
 import json
 import os
+import re
 import subprocess
 import sys
 
@@ -178,3 +179,47 @@ def test_lumethod2_factors_are_lu_of_p():
     U = sp.Matrix(n, n, lambda i, j: LU[i, j] if i <= j else 0)
     P = s.P_order.subs(pt).evalf()
     assert max(abs(float(v)) for v in (L * U - P)) < 1e-12
+
+
+def _run_lines(lines, a, r, recip):
+    """Evaluates emitted factor/solve lines in Python doubles; with recip the
+    pivots are reciprocals (the FP32 convention of ov_pivot / ov_divp)."""
+    env = {"a": a, "r": r, "x": [0.0] * len(r),
+           "piv": (lambda p: 1.0 / p) if recip else (lambda p: p),
+           "divp": (lambda v, p: v * p) if recip else (lambda v, p: v / p)}
+    for ln in lines:
+        ln = re.sub(r"OV_I?SC\(\d+\)", "1.0", ln.rstrip(";"))
+        ln = ln.replace("ov_divp<T>(", "divp(").replace("ov_pivot<T>(", "piv(")
+        ln = ln.replace("(T)", "").replace("(double)", "")
+        if ln.startswith("T "):
+            ln = ln[2:]
+        exec(ln, env)
+    return np.array(env["x"])
+
+
+@pytest.mark.parametrize("example,order,pack", [("PRIMORDIAL", "FF", "CSC"), ("PRIMORDIAL", "CMK", "CSC"),
+                                                ("PRIMORDIAL", "None", "DENSE"), ("ROBER", "None", "DENSE"),
+                                                ("OREGO", "CMK", "CSC")])
+def test_reciprocal_pivots_solve_the_same_system(example, order, pack):
+    # the FP32 LU's pivot reciprocals are placed where each pivot is final:
+    # factor + solve with reciprocals gives the solution of the divisions
+    s = pre_odevec.build_system(networks.load(example), order, pack)
+    fl, sl = pre_odevec._lu_factor_lines(s), pre_odevec._lu_solve_lines(s)
+    rf, rs = pre_odevec.reciprocal_pivots(fl, sl)
+    assert sum("ov_pivot" in l for l in rf) == s.neq
+    rng = np.random.default_rng(7)
+    a0 = rng.uniform(-1.0, 1.0, s.nnz)
+    for (i, j), k in s.pos().items():
+        if i == j:
+            a0[k] += 2.0 * s.neq
+    r = list(rng.uniform(-1.0, 1.0, s.neq))
+    x_div = _run_lines(fl + sl, list(a0), r, recip=False)
+    x_rec = _run_lines(rf + rs, list(a0), r, recip=True)
+    assert np.max(np.abs(x_rec - x_div)) <= 1e-13 * np.max(np.abs(x_div))
+    # and the rewritten lines with FP64 pivots are the original arithmetic
+    assert np.array_equal(_run_lines(rf + rs, list(a0), r, recip=False), x_div)
+
+
+def test_reciprocal_pivots_rejects_a_pivot_read_after_it_is_final():
+    with pytest.raises(ValueError, match="other than as a divisor"):
+        pre_odevec.reciprocal_pivots(["a[1] = a[1] / a[0];", "a[2] = a[2] - a[0]*a[1];"], [])
