@@ -87,8 +87,9 @@ static __constant__ double c_lcoef[7][7] = {
 
 __device__ __forceinline__ double lcoef(int q, int k) { return c_lcoef[q][k]; }
 
-/* x^y out of line: the step-size selection calls it three times */
-static __device__ __noinline__ double pow_dev(double x, double y) { return ov_pow(x, y); }
+/* 1/k for k = 1..7, correctly rounded at compile time: the same bits as the
+   division 1.0 / k the reference evaluates (1/order, 1/(order+1), ...) */
+static __constant__ double c_inv[8] = {0.0, 1.0, 1.0 / 2.0, 1.0 / 3.0, 1.0 / 4.0, 1.0 / 5.0, 1.0 / 6.0, 1.0 / 7.0};
 
 /* tau (src/odevec.F90:1034-1054), evaluated at compile time with the same
    IEEE operations: q! by repeated multiplication, then one division */
@@ -415,27 +416,27 @@ struct Cell {
     }
 
     /* CalcStepSizeOrder (src/odevec.F90:547-618); returns dt_scale.  The
-       literals 1.3, 1.2, 1.4 and 1.1 are single precision in the reference. */
+       literals 1.3, 1.2, 1.4 and 1.1 are single precision in the reference.
+       The three candidate factors are independent: all three are evaluated
+       (the unused ones are discarded) with the branch-free power, so their
+       dependency chains interleave instead of running one after another.
+       Each kept value is the same IEEE expression as in the reference. */
     __device__ __forceinline__ double step_size_order()
     {
         const int order = q;
-        double down, same, up;
-        if (order == 1)
-            down = 0.0;
-        else
-            down = 1.0 / ((double)1.3f * pow_dev(wnorm_ns(order) / tau(order, order - 1), 1.0 / order)
-                          + 1e-6);
-        same = 1.0 / ((double)1.2f * pow_dev(wnorm(en) / tau(order, order), 1.0 / (order + 1.0)) + 1e-6);
-        if (order == MAXQ || nuo)
-            up = 0.0;
-        else {
-            double d[ND];
+        double d[ND];
 #pragma unroll
-            for (int j = 0; j < ND; ++j)
-                d[j] = en[j] - eno[j];
-            up = 1.0 / ((double)1.4f * pow_dev(wnorm(d) / tau(order, order + 1), 1.0 / (order + 2.0))
-                        + 1e-6);
-        }
+        for (int j = 0; j < ND; ++j)
+            d[j] = en[j] - eno[j];
+        const double n_down = wnorm_ns(order) / tau(order, order - 1);
+        const double n_same = wnorm(en) / tau(order, order);
+        const double n_up = wnorm(d) / tau(order, order + 1);
+        const double p_down = ov_pow_sel(n_down, c_inv[order]);
+        const double p_same = ov_pow_sel(n_same, c_inv[order + 1]);
+        const double p_up = ov_pow_sel(n_up, c_inv[order + 2]);
+        const double down = order == 1 ? 0.0 : 1.0 / ((double)1.3f * p_down + 1e-6);
+        const double same = 1.0 / ((double)1.2f * p_same + 1e-6);
+        const double up = (order == MAXQ || nuo) ? 0.0 : 1.0 / ((double)1.4f * p_up + 1e-6);
         int loc = 1;
         double mx = down;
         if (same > mx) { mx = same; loc = 2; }

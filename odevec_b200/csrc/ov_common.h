@@ -184,6 +184,99 @@ OV_HD static OV_INLINE double ov_pow(double x, double y)
     return ov_exp(y * ov_log(x));
 }
 
+/* Branch-free restatements of ov_exp, ov_log and ov_pow.  Every input runs
+   the main path (special inputs on a harmless stand-in) and the special
+   cases are selected afterwards, in the order the branches above test them,
+   so each result is bit-identical to the branching function's; factors of
+   1.0 stand in for the skipped scalings and are exact.  Without branches the
+   compiler can interleave independent calls (the step-size selection needs
+   three powers at once). */
+OV_HD static OV_INLINE double ov_scale2_sel(double p, int k)
+{
+    const int a = k > 1000 ? 1000 : (k < -1000 ? k + 1000 : k);
+    const int b = k > 1000 ? k - 1000 : (k < -1000 ? -1000 : 0);
+    return p * ov_pow2i(a) * ov_pow2i(b);
+}
+
+OV_HD static OV_INLINE double ov_exp_sel(double x)
+{
+    const int ok = x >= -745.1332191019412 && x <= 709.782712893384;
+    const double xs = ok ? x : 0.0;
+    const double shift = 6755399441055744.0; /* 1.5 * 2^52 */
+    double kd = (xs * OV_INV_LN2 + shift) - shift;
+    int k = (int)kd;
+    double r = (xs - kd * OV_LN2_HI) - kd * OV_LN2_LO;
+    double p = 1.0 / 6227020800.0;
+    p = 1.0 / 479001600.0 + r * p;
+    p = 1.0 / 39916800.0 + r * p;
+    p = 1.0 / 3628800.0 + r * p;
+    p = 1.0 / 362880.0 + r * p;
+    p = 1.0 / 40320.0 + r * p;
+    p = 1.0 / 5040.0 + r * p;
+    p = 1.0 / 720.0 + r * p;
+    p = 1.0 / 120.0 + r * p;
+    p = 1.0 / 24.0 + r * p;
+    p = 1.0 / 6.0 + r * p;
+    p = 0.5 + r * p;
+    p = 1.0 + r * p;
+    p = 1.0 + r * p;
+    double v = ov_scale2_sel(p, k);
+    v = x < -745.1332191019412 ? 0.0 : v;
+    v = x > 709.782712893384 ? INFINITY : v;
+    v = x != x ? x : v;
+    return v;
+}
+
+OV_HD static OV_INLINE double ov_log_sel(double x)
+{
+    const int ok = x > 0.0 && x < INFINITY;
+    double xs = ok ? x : 1.0;
+    uint64_t b = ov_d2bits(xs);
+    const int sub = (b >> 52) == 0;
+    xs = xs * (sub ? 18014398509481984.0 : 1.0); /* 2^54 */
+    int e = sub ? -54 : 0;
+    b = ov_d2bits(xs);
+    e += (int)(b >> 52) - 1023;
+    double m = ov_bits2d((b & 0x000fffffffffffffULL) | 0x3ff0000000000000ULL); /* [1,2) */
+    const int hi = m > OV_SQRT2;
+    m = m * (hi ? 0.5 : 1.0);
+    e += hi;
+    double f = m - 1.0;
+    double u = f / (2.0 + f);
+    double z = u * u;
+    double R = 2.0 / 23.0;
+    R = 2.0 / 21.0 + z * R;
+    R = 2.0 / 19.0 + z * R;
+    R = 2.0 / 17.0 + z * R;
+    R = 2.0 / 15.0 + z * R;
+    R = 2.0 / 13.0 + z * R;
+    R = 2.0 / 11.0 + z * R;
+    R = 2.0 / 9.0 + z * R;
+    R = 2.0 / 7.0 + z * R;
+    R = 2.0 / 5.0 + z * R;
+    R = 2.0 / 3.0 + z * R;
+    R = z * R;
+    double ed = (double)e;
+    double lm = f - u * (f - R);
+    double v = ed * OV_LN2_HI + (lm + ed * OV_LN2_LO);
+    v = x == INFINITY ? x : v;
+    v = x == 0.0 ? -INFINITY : v;
+    v = x < 0.0 ? NAN : v;
+    v = x != x ? x : v;
+    return v;
+}
+
+OV_HD static OV_INLINE double ov_pow_sel(double x, double y)
+{
+    const double a = ov_exp_sel(y * ov_log_sel(x < 0.0 ? -x : x));
+    const double h = 0.5 * y;
+    double v = x < 0.0 ? (floor(y) != y ? NAN : (floor(h) == h ? a : -a)) : a;
+    v = x == 0.0 ? (y > 0.0 ? 0.0 : INFINITY) : v;
+    v = (x != x || y != y) ? x + y : v;
+    v = (y == 0.0 || x == 1.0) ? 1.0 : v;
+    return v;
+}
+
 /* Pivots of the numeric LU.  In FP64 the factorisation and the solves divide
    by each pivot as the reference does (src/odevec.F90:906-969, :864-889).
    An FP32 LU stores each pivot's reciprocal in place once the pivot is final

@@ -25,6 +25,9 @@
 namespace ov {
 namespace OV_MODE_NS {
 
+/* x^y out of line: the step-size selection calls it three times */
+static __device__ __noinline__ double pow_dev(double x, double y) { return ov_pow(x, y); }
+
 template <class Net, class LUT>
 struct WpcLayout {
     static constexpr int N = Net::NEQ, ND = Net::ND, NNZ = Net::NNZ;

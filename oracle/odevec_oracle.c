@@ -1008,6 +1008,9 @@ const char* ov_oracle_net_tag(int i) { return (i >= 0 && i < g_nnets) ? g_entrie
 double ov_oracle_exp(double x) { return ov_exp(x); }
 double ov_oracle_log(double x) { return ov_log(x); }
 double ov_oracle_pow(double x, double y) { return ov_pow(x, y); }
+double ov_oracle_pow_sel(double x, double y) { return ov_pow_sel(x, y); }
+double ov_oracle_exp_sel(double x) { return ov_exp_sel(x); }
+double ov_oracle_log_sel(double x) { return ov_log_sel(x); }
 
 /* krome_x2n / krome_n2x of the reference's PRIMORDIAL driver
    (tests/primordial.f90:117-140): direction 0, n = rhogas * x * imass;

@@ -32,11 +32,12 @@ def lib():
         L.ov_oracle_num_nets.restype = i32
         L.ov_oracle_net_tag.restype = ctypes.c_char_p
         L.ov_oracle_net_tag.argtypes = [i32]
-        for f in ("ov_oracle_exp", "ov_oracle_log"):
+        for f in ("ov_oracle_exp", "ov_oracle_log", "ov_oracle_exp_sel", "ov_oracle_log_sel"):
             getattr(L, f).argtypes = [d]
             getattr(L, f).restype = d
-        L.ov_oracle_pow.argtypes = [d, d]
-        L.ov_oracle_pow.restype = d
+        for f in ("ov_oracle_pow", "ov_oracle_pow_sel"):
+            getattr(L, f).argtypes = [d, d]
+            getattr(L, f).restype = d
         L.ov_oracle_convert.argtypes = [ctypes.c_char_p, i64, i32, P, P, P]
         L.ov_oracle_convert.restype = i32
         _lib = L

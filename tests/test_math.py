@@ -52,3 +52,36 @@ def test_pow(lib):
     assert np.max(rel / (1.0 + np.abs(y * np.log(x)))) < 4e-16
     assert lib.ov_oracle_pow(0.0, 0.5) == 0.0 and lib.ov_oracle_pow(7.0, 0.0) == 1.0
     assert abs(lib.ov_oracle_pow(-2.0, 3.0) + 8.0) < 1e-14 and np.isnan(lib.ov_oracle_pow(-2.0, 0.5))
+
+
+def _bits(v):
+    return np.float64(v).view(np.int64)
+
+
+def _same(a, b):
+    return _bits(a) == _bits(b) or (np.isnan(a) and np.isnan(b))
+
+
+SPECIAL = [0.0, -0.0, 1.0, -1.0, 2.0, -2.0, 0.5, -0.5, 3.0, -3.0, np.inf, -np.inf, np.nan, 5e-324, -5e-324,
+           1e-310, 2.2250738585072014e-308, 1.7976931348623157e308, 709.782712893384, 709.7827128933841,
+           -745.1332191019412, -745.1332191019413, 700.0, -740.0, 1e-300, 1e300]
+
+
+def test_branch_free_functions_are_bit_identical(lib):
+    # the step-size selection evaluates its three powers with the branch-free
+    # forms; every result must be the branching function's, bit for bit
+    rng = np.random.default_rng(5)
+    xs = np.concatenate([rng.uniform(-800, 800, 4000), 10.0 ** rng.uniform(-320, 308, 4000),
+                         -(10.0 ** rng.uniform(-320, 308, 1000)), SPECIAL])
+    for x in xs:
+        assert _same(lib.ov_oracle_exp_sel(float(x)), lib.ov_oracle_exp(float(x))), x
+        assert _same(lib.ov_oracle_log_sel(float(x)), lib.ov_oracle_log(float(x))), x
+    px = np.concatenate([10.0 ** rng.uniform(-30, 30, 3000), -(10.0 ** rng.uniform(-5, 5, 500)), SPECIAL])
+    py = np.concatenate([rng.uniform(-4, 4, 3000), rng.integers(-5, 6, 500).astype(float), SPECIAL])
+    ys = np.concatenate([py, [1.0 / k for k in range(1, 8)], SPECIAL])
+    for x in px:
+        for y in rng.choice(ys, 8):
+            assert _same(lib.ov_oracle_pow_sel(float(x), float(y)), lib.ov_oracle_pow(float(x), float(y))), (x, y)
+    for x in SPECIAL:
+        for y in SPECIAL + [1.0 / k for k in range(1, 8)]:
+            assert _same(lib.ov_oracle_pow_sel(float(x), float(y)), lib.ov_oracle_pow(float(x), float(y))), (x, y)
