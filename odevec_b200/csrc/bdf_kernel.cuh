@@ -162,15 +162,18 @@ template <int STAGE>
 struct StageCfg;
 /* SHM: 0 = history and LU in thread-local arrays, 1 = both in shared memory,
    2 = the history in shared memory and the LU thread-local.  REFILL: idle
-   lanes take new cells on every REFILL-th trip of the cell loop only; the
-   lockstep stagings align the cell set-ups of all their warps that way. */
+   lanes take new cells on every REFILL-th trip of the cell loop only (the
+   first trip included), so a warp sets up several cells at once instead of
+   one every few trips, and the lockstep stagings set up cells in all their
+   warps in the same trip. */
+/* staging 1 keeps the straight port's refill on every trip */
 template <> struct StageCfg<1> { static constexpr int SHM = 0; static constexpr bool SOFT = false; static constexpr int BS = 128, MINB = 2, REFILL = 1; };
-template <> struct StageCfg<2> { static constexpr int SHM = 1; static constexpr bool SOFT = false; static constexpr int BS = 128, MINB = 1, REFILL = 1; };
-template <> struct StageCfg<3> { static constexpr int SHM = 0; static constexpr bool SOFT = false; static constexpr int BS = 128, MINB = 3, REFILL = 1; };
-template <> struct StageCfg<4> { static constexpr int SHM = 0; static constexpr bool SOFT = false; static constexpr int BS = 128, MINB = 4, REFILL = 1; };
-template <> struct StageCfg<5> { static constexpr int SHM = 1; static constexpr bool SOFT = false; static constexpr int BS = 192, MINB = 1, REFILL = 1; };
+template <> struct StageCfg<2> { static constexpr int SHM = 1; static constexpr bool SOFT = false; static constexpr int BS = 128, MINB = 1, REFILL = 16; };
+template <> struct StageCfg<3> { static constexpr int SHM = 0; static constexpr bool SOFT = false; static constexpr int BS = 128, MINB = 3, REFILL = 16; };
+template <> struct StageCfg<4> { static constexpr int SHM = 0; static constexpr bool SOFT = false; static constexpr int BS = 128, MINB = 4, REFILL = 16; };
+template <> struct StageCfg<5> { static constexpr int SHM = 1; static constexpr bool SOFT = false; static constexpr int BS = 192, MINB = 1, REFILL = 16; };
 /* as 3, the same register budget, in one block of 384 threads per SM */
-template <> struct StageCfg<6> { static constexpr int SHM = 0; static constexpr bool SOFT = false; static constexpr int BS = 384, MINB = 1, REFILL = 1; };
+template <> struct StageCfg<6> { static constexpr int SHM = 0; static constexpr bool SOFT = false; static constexpr int BS = 384, MINB = 1, REFILL = 16; };
 /* as 6, with the block's warps held in soft lockstep (SoftSync) */
 template <> struct StageCfg<8> { static constexpr int SHM = 0; static constexpr bool SOFT = true;  static constexpr int BS = 384, MINB = 1, REFILL = 16; };
 /* soft lockstep, one block of 256 threads per SM, the history in shared
@@ -802,10 +805,11 @@ __global__ void __launch_bounds__(StageCfg<STAGE>::BS, StageCfg<STAGE>::MINB) bd
         if (G == 1) {
             if constexpr (StageCfg<STAGE>::SOFT)
                 soft_sync(&soft, lane);
-            /* with REFILL > 1, idle lanes wait for every REFILL-th trip, the
-               same trip in every warp of a lockstep block, so the costly
+            /* with REFILL > 1, idle lanes wait for every REFILL-th trip (the
+               same trip in every warp of a lockstep block), so the costly
                cell set-up (loads, temperature rates, first right-hand side)
-               runs in all warps at once instead of stretching random trips */
+               runs for several lanes and warps at once instead of stretching
+               trip after trip for one lane */
             const bool refill = StageCfg<STAGE>::REFILL <= 1 || trip % StageCfg<STAGE>::REFILL == 0u;
             ++trip;
             const unsigned need = refill ? __ballot_sync(FULL, ph == PH_IDLE) : 0u;
@@ -1205,9 +1209,9 @@ constexpr bool hist_fits()
    constant-coefficient CSC variants); 8 = as 6 in soft lockstep; 9, 10 =
    soft lockstep in one block of 256 or 320 with the history in shared
    memory; 11 = soft lockstep in one block of 192 with history and LU in
-   shared memory (where they fit).  The lockstep stagings 8-11 refill idle
-   lanes on every 16th trip.  Stages 2-11 exist for per-cell control
-   (G = 1). */
+   shared memory (where they fit).  With per-cell control stagings 2-11
+   refill idle lanes on every 16th trip, staging 1 on every trip.  Stages
+   2-11 exist for per-cell control (G = 1). */
 #define OV_STAGE_CASE(NET, LU, ST)                                                               \
     if (stage == ST)                                                                             \
         return launch<NET, 1, LU, ST>(a, block, grid, s);
