@@ -39,6 +39,7 @@ DATA = "synthetic: seeded inputs with the configuration's distributions (no publ
 
 
 def parse():
+    from odevec_b200 import workloads as W
     p = argparse.ArgumentParser()
     p.add_argument("--gpus", type=int, default=1)
     p.add_argument("--steps", type=int, default=5)
@@ -46,9 +47,12 @@ def parse():
     p.add_argument("--impl", default="product", choices=["product", "reference"])
     p.add_argument("--ncells", type=int, default=1048576)
     p.add_argument("--network", default="PRIMORDIAL_CSC_FF")
+    p.add_argument("--workload", default="PRIMORDIAL", choices=sorted(W.BUILDERS),
+                   help="seeded input set (odevec_b200.workloads); the headline is PRIMORDIAL")
     p.add_argument("--forms", default="fp32_lu,fp64,fp64_fma,plain_fp64",
-                   help="fp32_lu | fp64 | fp64_fma | plain_fp64 (FP64, one cell per thread for the "
-                        "whole launch, Jacobian and step-size blocks run where a cell needs them)")
+                   help="fp32_lu | fp64 | fp64_fma | plain_fp64 (FP64, a thread per cell, refilled from "
+                        "the work queue on every trip, Jacobian and step-size blocks run where a cell "
+                        "needs them)")
     p.add_argument("--cpu-sample", type=int, default=65536)
     p.add_argument("--accuracy-cells", type=int, default=256)
     p.add_argument("--no-cpu", action="store_true")
@@ -131,6 +135,13 @@ def fma_peaks(torch):
     return out
 
 
+def workload_label(args, n):
+    if args.workload == "PRIMORDIAL":
+        return WORKLOAD % n
+    return "%s seeded synthetic cells (odevec_b200.workloads.%s), %d cells per GPU" % (
+        args.workload, args.workload.lower(), n)
+
+
 def traffic_per_cell():
     """DRAM bytes per cell of the solve kernel from the committed ncu summary."""
     path = os.path.join(ROOT, "profiles", "bdf_kernel_primordial_ncu.txt")
@@ -164,7 +175,7 @@ def run_reference(args):
     if rank != 0:
         return
     from odevec_b200 import workloads as W
-    wl = W.primordial(ncells=args.cpu_sample, seed=3, network=args.network)
+    wl = W.BUILDERS[args.workload](ncells=args.cpu_sample, seed=3, network=args.network)
     threads = host_threads()
     for _ in range(args.warmup):
         oracle_rate(wl, args.cpu_sample, threads)
@@ -177,7 +188,7 @@ def run_reference(args):
         "impl": "reference", "metric": METRIC, "value": value, "unit": "cells/s", "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * sum(times) / len(times),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": DATA,
-        "config": {"workload": WORKLOAD % args.ncells, "network": args.network,
+        "config": {"workload": workload_label(args, args.ncells), "network": args.network,
                    "sample_cells_per_step": args.cpu_sample},
         "cpu_baseline": {"value": value, "unit": "cells/s", "cores": threads, "kind": "port",
                          "sample": "%d of the workload's cells per step, oracle/ (C restatement of "
@@ -211,7 +222,7 @@ def run_product(args):
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         return float(t.item())
 
-    wl = W.primordial(ncells=args.ncells, seed=3 + rank, network=args.network)
+    wl = W.BUILDERS[args.workload](ncells=args.ncells, seed=3 + rank, network=args.network)
     N = wl.ncells
     y0 = torch.tensor(wl.y, device=dev)
     t0 = torch.tensor(wl.t0, device=dev)
@@ -228,9 +239,10 @@ def run_product(args):
         kw = {}
         if form == "plain_fp64":
             # the reference's loop structure ported one thread per cell: a grid
-            # of one cell per thread (no refill from the work queue), every
-            # Jacobian and step-size block run at once by the lanes that need
-            # it (no batching), two 128-thread blocks per SM
+            # of one thread per cell whose finished lanes take unstarted cells
+            # from the work queue on every trip, every Jacobian and step-size
+            # block run at once by the lanes that need it (no batching), two
+            # 128-thread blocks per SM, no lockstep, arrays thread-local
             kw = dict(jac_batch=1, ss_batch=1, max_wait=-1, staging=1, grid_blocks=(N + 127) // 128)
         ode = S.Odevec(wl.network, max_cells=N, RelativeTolerance=wl.rtol, AbsoluteTolerance=wl.atol,
                        MinimalTimestep=wl.dt_min, nvector=1, precision="fp64" if form == "plain_fp64" else form,
@@ -323,7 +335,8 @@ def run_product(args):
     r = res[head]
     peaks = fma_peaks(torch)
     achieved = r["flops_per_launch"] / (r["kernel_ms"] * 1e-3) / 1e12
-    tpc = traffic_per_cell()
+    tpc = traffic_per_cell() if args.workload == "PRIMORDIAL" else None
+    in_mb = N * (y0.shape[0] + 3) * 8 / 1e6  # species, t, dt, t_stop
     alg_bytes = N * (16 * 8 * 2 + 3 * 8 + 2 * 8 + 4)
     line = {
         "metric": METRIC,
@@ -338,8 +351,9 @@ def run_product(args):
         "vs_baseline": None,
         "dtype": "f64 state/residual/control, f32 LU" if head == "fp32_lu" else "f64",
         "data": DATA,
-        "config": {"workload": WORKLOAD % N, "network": args.network, "form": head,
-                   "l2": "inputs %.0f MB per GPU > 126 MB L2" % (N * 19 * 8 / 1e6),
+        "config": {"workload": workload_label(args, N), "network": args.network, "form": head,
+                   "l2": "inputs %.0f MB per GPU %s 126 MB L2" % (
+                       in_mb, ">" if in_mb > 126 else "<= (not flushed between steps)"),
                    "parallelism": "dp%d (independent cell shards, no exchange)" % world},
         "roofline": {"bound": "fp64", "achieved": achieved, "peak": peaks["fp64"], "unit": "TFLOP/s",
                      "frac": achieved / peaks["fp64"],
@@ -364,7 +378,7 @@ def run_product(args):
         line["fp32lu_over_plain_fp64"] = res["fp32_lu"]["value"] / res["plain_fp64"]["value"]
     if world == 1 and not args.no_cpu:
         threads = host_threads()
-        v, el, f = oracle_rate(W.primordial(ncells=args.cpu_sample, seed=3, network=args.network),
+        v, el, f = oracle_rate(W.BUILDERS[args.workload](ncells=args.cpu_sample, seed=3, network=args.network),
                                args.cpu_sample, threads)
         line["cpu_baseline"] = {"value": v, "unit": "cells/s", "cores": threads, "kind": "port",
                                 "sample": "%d cells of the same workload (%.1f s)" % (args.cpu_sample, el)}
