@@ -364,8 +364,8 @@ def run_product(args):
                      "peak_source": "FP64 FMA-chain probe on this GPU (odevec_probe_fma); "
                                     "MEASURED_PEAKS.json has no FP64 figure",
                      "fp64_share_of_flops": r["fp64_share"], "fp32_peak": peaks["fp32"]},
-        "e2e": {"value": r["e2e"], "unit": "cells/s", "h2d_bytes_per_step": N * (16 + 3) * 8,
-                "d2h_bytes_per_step": N * ((16 + 2) * 8 + 4)},
+        "e2e": {"value": r["e2e"], "unit": "cells/s", "h2d_bytes_per_step": N * (y0.shape[0] + 3) * 8,
+                "d2h_bytes_per_step": N * ((y0.shape[0] + 2) * 8 + 4)},
         "gpu_launches": args.steps * r["launches_per_step"],
         "clocks": {k: v for k, v in r["clocks"].items() if k != "samples"},
         "batch_latency_ms": {"p50": float(np.percentile(r["step_ms"], 50)),

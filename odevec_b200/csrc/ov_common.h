@@ -190,7 +190,7 @@ OV_HD static OV_INLINE double ov_pow(double x, double y)
    so each result is bit-identical to the branching function's; factors of
    1.0 stand in for the skipped scalings and are exact.  Without branches the
    compiler can interleave independent calls (the step-size selection needs
-   three powers at once). */
+   three powers at once, the PRIMORDIAL rate laws about forty). */
 OV_HD static OV_INLINE double ov_scale2_sel(double p, int k)
 {
     const int a = k > 1000 ? 1000 : (k < -1000 ? k + 1000 : k);
@@ -264,6 +264,11 @@ OV_HD static OV_INLINE double ov_log_sel(double x)
     v = x < 0.0 ? NAN : v;
     v = x != x ? x : v;
     return v;
+}
+
+OV_HD static OV_INLINE double ov_log10_sel(double x)
+{
+    return ov_log_sel(x) * OV_INV_LN10;
 }
 
 OV_HD static OV_INLINE double ov_pow_sel(double x, double y)

@@ -331,6 +331,18 @@ def test_ragged_sizes_bit_exact(gpu_lib, oracle, ncells):
         assert_bitwise(g, run_oracle(oracle, wl), "ncells %d staging %d" % (ncells, staging))
 
 
+def test_short_solves_more_cells_than_lanes_bit_exact(gpu_lib, oracle):
+    # about 15 trips per cell and two to three cells per lane: lanes go idle
+    # often and take new cells on every trip (staging 1) or only on every 16th
+    # trip (3, 9), until the work counter runs past the last cell
+    wl = W.primordial(ncells=120000, seed=17)
+    wl.t_stop[:] = 10.0 ** np.random.default_rng(17).uniform(-4.0, 0.0, wl.ncells)
+    o = run_oracle(oracle, wl)
+    assert np.all(o[3] == 0)
+    for staging in (1, 3, 9):
+        assert_bitwise(run_gpu(gpu_lib, wl, "fp64", staging=staging), o, "short solves staging %d" % staging)
+
+
 def test_empty_and_group_size_errors(gpu_lib):
     import torch
     S = gpu_lib
