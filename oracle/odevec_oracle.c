@@ -975,6 +975,13 @@ int ov_oracle_rates(double T, double* r)
     return 0;
 }
 
+/* k_j = small(y) + r_j for one PRIMORDIAL state (the per-call rate floor) */
+int ov_oracle_rates_k(const double* y, int neq, const double* r, double* k)
+{
+    ov_rates_primordial_k(y, neq, r, k);
+    return 0;
+}
+
 int ov_oracle_netinfo(const char* tag, int* info /* neq nnz nrea dense idx_tgas */, int* perm,
                       int* row_index, int* u_col_start, int* l_col_start)
 {

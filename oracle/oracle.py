@@ -28,6 +28,7 @@ def lib():
         L.ov_oracle_solve.restype = i32
         L.ov_oracle_eval.argtypes = [ctypes.c_char_p, P, P, d, d, P, P]
         L.ov_oracle_rates.argtypes = [d, P]
+        L.ov_oracle_rates_k.argtypes = [P, i32, P, P]
         L.ov_oracle_netinfo.argtypes = [ctypes.c_char_p, P, P, P, P, P]
         L.ov_oracle_num_nets.restype = i32
         L.ov_oracle_net_tag.restype = ctypes.c_char_p

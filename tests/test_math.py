@@ -85,3 +85,31 @@ def test_branch_free_functions_are_bit_identical(lib):
     for x in SPECIAL:
         for y in SPECIAL + [1.0 / k for k in range(1, 8)]:
             assert _same(lib.ov_oracle_pow_sel(float(x), float(y)), lib.ov_oracle_pow(float(x), float(y))), (x, y)
+
+
+def _rate_floor_reference(y):
+    # src/odevec_commons.F90:127-130: running maximum from y_1, clamped to 1
+    nmax = y[0]
+    for v in y[1:]:
+        nmax = v if v > nmax else nmax
+    nmax = nmax if nmax > 1.0 else 1.0
+    return 1e-40 / (nmax * nmax * nmax)
+
+
+def test_rate_floor_tree_maximum_matches_running_maximum(lib):
+    import ctypes
+    rng = np.random.default_rng(9)
+    r = np.zeros(38)
+    k = np.zeros(38)
+    P = lambda a: a.ctypes.data_as(ctypes.c_void_p)
+    for trial in range(3000):
+        y = 10.0 ** rng.uniform(-30, 8, 16)
+        y *= rng.choice([1.0, -1.0], 16, p=[0.8, 0.2])
+        for _ in range(rng.integers(0, 4)):
+            y[rng.integers(0, 16)] = rng.choice([np.nan, 0.0, -0.0, 1.0, np.inf, -np.inf, 0.5, 2.0])
+        if trial % 7 == 0:
+            y[0] = np.nan
+        y = np.ascontiguousarray(y)
+        lib.ov_oracle_rates_k(P(y), 16, P(r), P(k))
+        want = _rate_floor_reference(list(y))
+        assert _same(k[0], want), (y, k[0], want)
