@@ -76,11 +76,13 @@ typedef struct odevec_opts {
     int32_t group_size;       /* 1 or 32; 0: the variant's --nvector (1 if not 32) */
     int32_t precision;        /* OV_PREC_* */
     int32_t max_attempts;     /* cap on predictor attempts per cell or group; 0: 1000000 */
-    /* scheduling of per-cell control (group_size 1), no effect on results:
-       the Jacobian+LU and the step-size selection run for the waiting cells
-       of a warp together once jac_batch / ss_batch of its 32 cells wait, no
-       other cell can progress, or a cell has waited max_wait iterations.
-       0: defaults (24, 24, 8); 1, 1, -1 runs each cell's block at once. */
+    /* scheduling of per-cell control (group_size 1) on staging 1, no effect
+       on results: the Jacobian+LU and the step-size selection run for the
+       waiting cells of a warp together once jac_batch / ss_batch of its 32
+       cells wait, no other cell can progress, or a cell has waited max_wait
+       iterations.  0: defaults (24, 24, 8); 1, 1, -1 runs each cell's block
+       at once.  Stagings 2-11 ignore them: they run the two blocks on fixed
+       trips (every 4th trip each, the same trips in all warps of a block). */
     int32_t jac_batch;
     int32_t ss_batch;
     int32_t max_wait;

@@ -4,16 +4,18 @@ What it chooses, per network variant, precision form and GPU model:
 
 * the staging -- where a cell's Nordsieck history and LU live (thread-local
   arrays in registers / local memory, or shared memory), the block size
-  (cells per block: 128, 192 or 384 threads) and the blocks per SM, or one
-  warp per cell (staging 7, for the variants that have its tables);
-* the batching of the Jacobian and step-size blocks (jac_batch, ss_batch,
-  max_wait).
+  (cells per block: 128, 192, 256, 320 or 384 threads), the blocks per SM and
+  soft lockstep, or one warp per cell (staging 7, for the variants that have
+  its tables);
+* for staging 1, the batching of the Jacobian and step-size blocks
+  (jac_batch, ss_batch, max_wait); the other stagings run those blocks on
+  fixed trips.
 
 None of these settings changes a result (every cell runs the same operations whatever the interleaving;
 the GPU parity tests check this bit for bit), so tuning only moves time.
 
-The search times every compiled staging with every batch setting on a
-sample of the caller's cells (about fifty short solves).  Results go to a JSON table (``tuning.json`` beside this
+The search times every compiled staging (staging 1 with every batch
+setting) on a sample of the caller's cells (about fifty short solves).  Results go to a JSON table (``tuning.json`` beside this
 file) that InitOdevec consults for options left at 0 (automatic).
 
     python -m odevec_b200.autotune --network PRIMORDIAL_CSC_FF --precision fp32_lu
@@ -30,6 +32,10 @@ TABLE = os.path.join(HERE, "tuning.json")
 STAGINGS = (1, 2, 3, 4, 6, 7, 8, 9, 10, 11)
 FP32_STAGINGS = (5,)
 BATCHES = ((24, 24, 8), (16, 16, 4), (32, 32, 16), (8, 8, 4), (4, 4, 2), (2, 2, 1), (1, 1, -1))
+# the batch options act on staging 1 only; the other stagings run the Jacobian
+# and step-size blocks on fixed trips and are timed once
+BATCHED_STAGINGS = (1,)
+UNBATCHED = ((1, 1, -1),)
 FIELDS = ("staging", "jac_batch", "ss_batch", "max_wait")
 
 
@@ -77,14 +83,15 @@ def candidates(precision: str) -> List[int]:
 
 def search(time_config: Callable[[dict], Optional[float]], precision: str,
            batches=BATCHES) -> Tuple[dict, List[Tuple[dict, float]]]:
-    """Every compiled staging with every batch setting (the two interact:
-    soft lockstep is best without batching, thread-local stagings with it);
-    time_config(cfg) returns seconds, or None for a configuration that is
-    not compiled for the variant (then the staging is skipped)."""
+    """Every compiled staging, staging 1 with every batch setting (the
+    others schedule the Jacobian and step-size blocks on fixed trips and take
+    no batch options); time_config(cfg) returns seconds, or None for a
+    configuration that is not compiled for the variant (then the staging is
+    skipped)."""
     tried: List[Tuple[dict, float]] = []
     best, best_t = None, None
     for st in candidates(precision):
-        for b in batches:
+        for b in (batches if st in BATCHED_STAGINGS else UNBATCHED):
             cfg = {"staging": st, "jac_batch": b[0], "ss_batch": b[1], "max_wait": b[2]}
             t = time_config(cfg)
             if t is None:

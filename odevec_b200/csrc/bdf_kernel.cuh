@@ -16,9 +16,12 @@
  * in different phases still run the right-hand side and the solve together.
  * The two expensive and rarely needed blocks -- Jacobian + LU factorisation
  * and step-size/order selection -- exist once in the code; a lane that needs
- * one waits until enough lanes of its warp need it (jac_batch / ss_batch),
- * no lane can progress otherwise, or it has waited max_wait trips, and then
- * all waiting lanes run it together.  Waiting changes only the interleaving
+ * one waits, and all waiting lanes run it together: on staging 1 once enough
+ * lanes of its warp need it (jac_batch / ss_batch), no lane can progress
+ * otherwise, or it has waited max_wait trips; on the other stagings on fixed
+ * trips (StageCfg::PERIOD), the same trips in every warp of the block, so a
+ * trip runs at most one of the two and all warps run the same code.  Waiting
+ * changes only the interleaving
  * across lanes, never a cell's own sequence of operations: the arithmetic
  * per cell is that of src/odevec.F90 operation by operation, and with
  * --fmad=false it is bit-identical to the CPU oracle.
@@ -165,25 +168,29 @@ struct StageCfg;
    lanes take new cells on every REFILL-th trip of the cell loop only (the
    first trip included), so a warp sets up several cells at once instead of
    one every few trips, and the lockstep stagings set up cells in all their
-   warps in the same trip. */
+   warps in the same trip.  PERIOD > 1: the Jacobian + LU block runs on the
+   trips t with t % PERIOD == 1 and the step-size block on those with
+   t % PERIOD == 0 (or at once when no lane of the warp can progress
+   otherwise), the same trips in every warp; jac_batch / ss_batch / max_wait
+   apply with PERIOD = 1 only. */
 /* staging 1 keeps the straight port's refill on every trip */
-template <> struct StageCfg<1> { static constexpr int SHM = 0; static constexpr bool SOFT = false; static constexpr int BS = 128, MINB = 2, REFILL = 1; };
-template <> struct StageCfg<2> { static constexpr int SHM = 1; static constexpr bool SOFT = false; static constexpr int BS = 128, MINB = 1, REFILL = 16; };
-template <> struct StageCfg<3> { static constexpr int SHM = 0; static constexpr bool SOFT = false; static constexpr int BS = 128, MINB = 3, REFILL = 16; };
-template <> struct StageCfg<4> { static constexpr int SHM = 0; static constexpr bool SOFT = false; static constexpr int BS = 128, MINB = 4, REFILL = 16; };
-template <> struct StageCfg<5> { static constexpr int SHM = 1; static constexpr bool SOFT = false; static constexpr int BS = 192, MINB = 1, REFILL = 16; };
+template <> struct StageCfg<1> { static constexpr int SHM = 0; static constexpr bool SOFT = false; static constexpr int BS = 128, MINB = 2, REFILL = 1, PERIOD = 1; };
+template <> struct StageCfg<2> { static constexpr int SHM = 1; static constexpr bool SOFT = false; static constexpr int BS = 128, MINB = 1, REFILL = 16, PERIOD = 4; };
+template <> struct StageCfg<3> { static constexpr int SHM = 0; static constexpr bool SOFT = false; static constexpr int BS = 128, MINB = 3, REFILL = 16, PERIOD = 4; };
+template <> struct StageCfg<4> { static constexpr int SHM = 0; static constexpr bool SOFT = false; static constexpr int BS = 128, MINB = 4, REFILL = 16, PERIOD = 4; };
+template <> struct StageCfg<5> { static constexpr int SHM = 1; static constexpr bool SOFT = false; static constexpr int BS = 192, MINB = 1, REFILL = 16, PERIOD = 4; };
 /* as 3, the same register budget, in one block of 384 threads per SM */
-template <> struct StageCfg<6> { static constexpr int SHM = 0; static constexpr bool SOFT = false; static constexpr int BS = 384, MINB = 1, REFILL = 16; };
+template <> struct StageCfg<6> { static constexpr int SHM = 0; static constexpr bool SOFT = false; static constexpr int BS = 384, MINB = 1, REFILL = 16, PERIOD = 4; };
 /* as 6, with the block's warps held in soft lockstep (SoftSync) */
-template <> struct StageCfg<8> { static constexpr int SHM = 0; static constexpr bool SOFT = true;  static constexpr int BS = 384, MINB = 1, REFILL = 16; };
+template <> struct StageCfg<8> { static constexpr int SHM = 0; static constexpr bool SOFT = true;  static constexpr int BS = 384, MINB = 1, REFILL = 16, PERIOD = 4; };
 /* soft lockstep, one block of 256 threads per SM, the history in shared
    memory (the rest of L1 for the other per-cell arrays) */
-template <> struct StageCfg<9> { static constexpr int SHM = 2; static constexpr bool SOFT = true;  static constexpr int BS = 256, MINB = 1, REFILL = 16; };
+template <> struct StageCfg<9> { static constexpr int SHM = 2; static constexpr bool SOFT = true;  static constexpr int BS = 256, MINB = 1, REFILL = 16, PERIOD = 4; };
 /* as 9 with 320 threads (10 warps) per SM */
-template <> struct StageCfg<10> { static constexpr int SHM = 2; static constexpr bool SOFT = true;  static constexpr int BS = 320, MINB = 1, REFILL = 16; };
+template <> struct StageCfg<10> { static constexpr int SHM = 2; static constexpr bool SOFT = true;  static constexpr int BS = 320, MINB = 1, REFILL = 16, PERIOD = 4; };
 /* soft lockstep, one block of 192 threads per SM with history and LU in
    shared memory (fits with FP32 factors) */
-template <> struct StageCfg<11> { static constexpr int SHM = 1; static constexpr bool SOFT = true;  static constexpr int BS = 192, MINB = 1, REFILL = 16; };
+template <> struct StageCfg<11> { static constexpr int SHM = 1; static constexpr bool SOFT = true;  static constexpr int BS = 192, MINB = 1, REFILL = 16, PERIOD = 4; };
 
 /* Soft lockstep.  The warps of a block wait for each other at the top of
    every trip of the cell loop, so they run the same phase code at the same
@@ -960,8 +967,14 @@ __global__ void __launch_bounds__(StageCfg<STAGE>::BS, StageCfg<STAGE>::MINB) bd
             if (G == 1) {
                 const int waiting = warp_count(ph == PH_JACWAIT);
                 const int moving = warp_count(ph == PH_NEWTON || ph == PH_START || ph == PH_RESTART);
-                const bool aged = __any_sync(FULL, ph == PH_JACWAIT && c.wait >= A.max_wait);
-                run = waiting > 0 && (waiting >= A.jac_batch || moving == 0 || aged);
+                if constexpr (StageCfg<STAGE>::PERIOD > 1) {
+                    /* trip was counted up at the top of this trip */
+                    constexpr unsigned P = StageCfg<STAGE>::PERIOD;
+                    run = waiting > 0 && (trip % P == 1u % P || moving == 0);
+                } else {
+                    const bool aged = __any_sync(FULL, ph == PH_JACWAIT && c.wait >= A.max_wait);
+                    run = waiting > 0 && (waiting >= A.jac_batch || moving == 0 || aged);
+                }
             } else {
                 run = ph == PH_JACWAIT;
             }
@@ -1091,8 +1104,12 @@ __global__ void __launch_bounds__(StageCfg<STAGE>::BS, StageCfg<STAGE>::MINB) bd
             if (G == 1) {
                 const int waiting = warp_count(ph == PH_SSWAIT);
                 const int moving = warp_count(ph == PH_PRED || ph == PH_NEWTON || ph == PH_RESTART);
-                const bool aged = __any_sync(FULL, ph == PH_SSWAIT && c.wait >= A.max_wait);
-                run = waiting > 0 && (waiting >= A.ss_batch || moving == 0 || aged);
+                if constexpr (StageCfg<STAGE>::PERIOD > 1) {
+                    run = waiting > 0 && (trip % StageCfg<STAGE>::PERIOD == 0u || moving == 0);
+                } else {
+                    const bool aged = __any_sync(FULL, ph == PH_SSWAIT && c.wait >= A.max_wait);
+                    run = waiting > 0 && (waiting >= A.ss_batch || moving == 0 || aged);
+                }
             } else {
                 run = ph == PH_SSWAIT;
             }

@@ -17,13 +17,18 @@ def test_search_picks_fastest_and_skips_uncompiled():
         if base is None:
             return None
         if cfg["jac_batch"] == 16:
-            return base * 0.9
+            return base * 0.4
         return base
 
     best, tried = A.search(timer, "fp64")
-    assert best["staging"] == 6 and best["jac_batch"] == 16 and best["seconds"] == pytest.approx(1.35)
+    assert best["staging"] == 1 and best["jac_batch"] == 16 and best["seconds"] == pytest.approx(1.2)
     assert all(c["staging"] != 2 for c, _ in tried)
-    assert len(tried) == len(A.BATCHES) * (len(A.STAGINGS) - 1)
+    # batches are tried on staging 1 only; the others are timed once, unbatched
+    assert len(tried) == len(A.BATCHES) + (len(A.STAGINGS) - 2)
+    assert all((c["jac_batch"], c["ss_batch"], c["max_wait"]) == (1, 1, -1) for c, _ in tried if c["staging"] != 1)
+    cost[1] = 9.0
+    best, _ = A.search(timer, "fp64")
+    assert best["staging"] == 6 and best["seconds"] == pytest.approx(1.5)
     best32, _ = A.search(timer, "fp32_lu")
     assert best32["staging"] == 5  # FP32-only staging considered for fp32_lu
 
