@@ -18,10 +18,11 @@ struct LaunchArgs {
     double rtol, atol, dt_min;
     int32_t check_neg;
     int32_t max_attempts;
-    /* per-cell control (G = 1): the Jacobian+LU and the step-size selection
-       run for all waiting lanes of a warp at once when at least this many
-       lanes wait, when no lane of the warp can progress otherwise, or when a
-       lane has waited max_wait trips */
+    /* per-cell control (G = 1) on staging 1: the Jacobian+LU and the
+       step-size selection run for all waiting lanes of a warp at once when at
+       least this many lanes wait, when no lane of the warp can progress
+       otherwise, or when a lane has waited max_wait trips (the other
+       stagings run them on fixed trips, StageCfg::PERIOD) */
     int32_t jac_batch;
     int32_t ss_batch;
     int32_t max_wait;
