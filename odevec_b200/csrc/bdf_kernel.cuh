@@ -427,20 +427,24 @@ struct Cell {
 
     /* CalcStepSizeOrder (src/odevec.F90:547-618); returns dt_scale.  The
        literals 1.3, 1.2, 1.4 and 1.1 are single precision in the reference.
-       The three candidate factors are independent: all three are evaluated
-       (the unused ones are discarded) with the branch-free power, so their
-       dependency chains interleave instead of running one after another.
-       Each kept value is the same IEEE expression as in the reference. */
+       The three candidate factors are independent: with per-cell control all
+       three are evaluated (the unused ones are discarded) with the
+       branch-free power, so their dependency chains interleave instead of
+       running one after another; a lockstep group (whose order is uniform)
+       skips the unused norms and their shuffle reductions.  Each kept value
+       is the same IEEE expression as in the reference. */
     __device__ __forceinline__ double step_size_order()
     {
         const int order = q;
+        const bool want_down = G == 1 || order != 1;
+        const bool want_up = G == 1 || !(order == MAXQ || nuo);
         double d[ND];
 #pragma unroll
         for (int j = 0; j < ND; ++j)
             d[j] = en[j] - eno[j];
-        const double n_down = wnorm_ns(order) / tau(order, order - 1);
+        const double n_down = want_down ? wnorm_ns(order) / tau(order, order - 1) : 0.0;
         const double n_same = wnorm(en) / tau(order, order);
-        const double n_up = wnorm(d) / tau(order, order + 1);
+        const double n_up = want_up ? wnorm(d) / tau(order, order + 1) : 0.0;
         const double p_down = ov_pow_sel(n_down, c_inv[order]);
         const double p_same = ov_pow_sel(n_same, c_inv[order + 1]);
         const double p_up = ov_pow_sel(n_up, c_inv[order + 2]);
