@@ -223,3 +223,15 @@ def test_reciprocal_pivots_solve_the_same_system(example, order, pack):
 def test_reciprocal_pivots_rejects_a_pivot_read_after_it_is_final():
     with pytest.raises(ValueError, match="other than as a divisor"):
         pre_odevec.reciprocal_pivots(["a[1] = a[1] / a[0];", "a[2] = a[2] - a[0]*a[1];"], [])
+
+
+@pytest.mark.parametrize("example,order,pack,lum", [("PRIMORDIAL", "FF", "CSC", 1), ("ROBER", "None", "DENSE", 2),
+                                                    ("PRIMORDIAL", "None", "DENSE", 3)])
+def test_cuda_header_divides_only_through_pivot_helpers(example, order, pack, lum):
+    # every division of the emitted factorisation and solves goes through
+    # ov_divp, every pivot gets ov_pivot, so the FP32 LU uses reciprocals
+    s = pre_odevec.build_system(networks.load(example), order, pack, lu_method=lum)
+    text = pre_odevec.emit_cuda_header(s)
+    body = text[text.index("void lu_factor("):]
+    assert "ov_pivot<T>(" in body and "ov_divp<T>(" in body
+    assert not re.search(r"/ a\[\d+\]", body)
