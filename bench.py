@@ -5,14 +5,16 @@ Metric: PRIMORDIAL cells/s to t_end at rtol 1e-6 (the 16-species primordial
 network, 1,048,576 cells per GPU, per-cell temperature and t_end), reported
 for the FP32-LU/FP64-residual form (``value``) beside the FP64 form of the
 same kernel (bit-identical to the CPU oracle), the FP64 form with fused
-multiply-add, and a plain FP64 port (one cell per thread for the whole
-launch, no batching).  Launch options come from the autotuner's table
+multiply-add, and a plain FP64 port (a thread per cell that takes the next
+cell from the work queue on every trip, no batching, no lockstep).  Launch
+options come from the autotuner's table
 (odevec_b200/tuning.json).  One step = one complete solve of all cells from
 the initial state to their t_end; inputs are reset from a device copy before
 each step (159 MB of inputs, larger than the 126 MB L2).  ``e2e`` is the same
 solve through the C-ABI host entry with pinned host buffers.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl product|reference]
+                    [--workload PRIMORDIAL|ROBER|OREGO|SYN64 --network TAG]
 
 Multi-GPU (torchrun, one process per GPU): every rank integrates its own
 1,048,576 cells (weak scaling; cells are independent, no data exchange);
