@@ -342,7 +342,7 @@ def run_product(args):
     achieved = r["flops_per_launch"] / (r["kernel_ms"] * 1e-3) / 1e12
     tpc = traffic_per_cell() if args.workload == "PRIMORDIAL" else None
     in_mb = N * (y0.shape[0] + 3) * 8 / 1e6  # species, t, dt, t_stop
-    alg_bytes = N * (16 * 8 * 2 + 3 * 8 + 2 * 8 + 4)
+    alg_bytes = N * (y0.shape[0] * 8 * 2 + 3 * 8 + 2 * 8 + 4)
     line = {
         "metric": METRIC,
         "value": r["value"],

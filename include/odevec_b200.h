@@ -197,9 +197,13 @@ const char* odevec_last_error(void);
    that hands out cells) lives in a static device array of
    OV_NOALLOC_SCRATCH_BYTES, which every GPU that loads the library holds
    until the process exits; at most OV_NOALLOC_MAX_CELLS cells per call
-   (larger calls fail with OV_API_ETOOBIG).  The first call on a device looks
-   up that array's device address (cudaGetSymbolAddress) and caches it, so
-   make the first call on each device before any stream capture.  Every
+   (larger calls fail with OV_API_ETOOBIG).  The array has its own address in
+   every CUDA context (each device's primary context, and any context a
+   driver-API caller creates); the first call in a context looks that address
+   up (cudaGetSymbolAddress) and caches it under the context's unique ID
+   (cuCtxGetId), so a context destroyed by cudaDeviceReset or cuCtxDestroy
+   and made again gets a fresh lookup.  Make the first call in each context
+   before any stream capture.  Every
    call resets the counter to zero on `stream` before the launch; all calls
    share the one counter, so calls that overlap on the GPU (different
    streams, or different host threads) race and must be serialised by the

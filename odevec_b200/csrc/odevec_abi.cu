@@ -8,6 +8,7 @@
  * Errors never terminate the process: API misuse returns a negative code,
  * per-cell integration failures are status codes (the reference calls
  * `stop`, src/odevec.F90:114-124, 272-287, 380-390, 585-597). */
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include <cstdarg>
@@ -594,27 +595,89 @@ namespace {
    counter, the rest keeps the array on its own 256-byte line. */
 static __device__ __align__(256) unsigned long long ov_noalloc_scratch[OV_NOALLOC_SCRATCH_BYTES / 8];
 
-constexpr int kMaxDevices = 64;
+/* A __device__ variable has its own address in every CUDA context that
+   loads the library: one per device for the runtime's primary contexts, and
+   another for each context a driver-API caller creates.  A context that is
+   destroyed (cudaDeviceReset, cuCtxDestroy) takes its copy with it.  The
+   looked-up address is therefore cached per context, keyed by the context's
+   unique ID (cuCtxGetId: never reused within a process, unlike the handle),
+   so a reset or another context leads to a fresh lookup, never to a stale
+   address. */
+constexpr int kCacheSlots = 64;
+struct ScratchSlot {
+    unsigned long long ctx_id;
+    unsigned long long* ptr;
+};
 std::mutex g_noalloc_mutex;
-unsigned long long* g_noalloc_ptr[kMaxDevices] = {};
+ScratchSlot g_noalloc_cache[kCacheSlots] = {};
+int g_noalloc_next = 0;
+typedef CUresult (*ctx_get_current_fn)(CUcontext*);
+typedef CUresult (*ctx_get_id_fn)(CUcontext, unsigned long long*);
+ctx_get_current_fn g_ctx_get_current = nullptr;
+ctx_get_id_fn g_ctx_get_id = nullptr;
 
-/* Device address of the static scratch on the current device.  In host code
-   the name ov_noalloc_scratch is only a handle, so the address is looked up
-   once per device with that device current, and cached. */
-int32_t noalloc_scratch(int dev, unsigned long long** out)
+/* ID of the current context (the runtime's primary context of the current
+   device is made current first if the thread has none). */
+int32_t current_context_id(unsigned long long* id)
 {
-    if (dev < 0 || dev >= kMaxDevices)
-        return fail(OV_API_EINVAL, "odevec_solve_noalloc: device ordinal %d out of range", dev);
-    std::lock_guard<std::mutex> lock(g_noalloc_mutex);
-    if (!g_noalloc_ptr[dev]) {
-        void* p = nullptr;
-        cudaError_t e = cudaGetSymbolAddress(&p, ov_noalloc_scratch);
-        if (e != cudaSuccess || !p)
-            return fail(OV_API_ECUDA, "odevec_solve_noalloc: cudaGetSymbolAddress: %s",
-                        cudaGetErrorString(e));
-        g_noalloc_ptr[dev] = static_cast<unsigned long long*>(p);
+    if (!g_ctx_get_current || !g_ctx_get_id) {
+        void* f1 = nullptr;
+        void* f2 = nullptr;
+        cudaDriverEntryPointQueryResult q1 = cudaDriverEntryPointSymbolNotFound, q2 = q1;
+        cudaError_t e1 = cudaGetDriverEntryPoint("cuCtxGetCurrent", &f1, cudaEnableDefault, &q1);
+        cudaError_t e2 = cudaGetDriverEntryPoint("cuCtxGetId", &f2, cudaEnableDefault, &q2);
+        if (e1 != cudaSuccess || e2 != cudaSuccess || q1 != cudaDriverEntryPointSuccess ||
+            q2 != cudaDriverEntryPointSuccess || !f1 || !f2)
+            return fail(OV_API_ECUDA, "odevec_solve_noalloc: driver entry points cuCtxGetCurrent/cuCtxGetId "
+                        "unavailable (%s)", cudaGetErrorString(e1 != cudaSuccess ? e1 : e2));
+        g_ctx_get_current = reinterpret_cast<ctx_get_current_fn>(f1);
+        g_ctx_get_id = reinterpret_cast<ctx_get_id_fn>(f2);
     }
-    *out = g_noalloc_ptr[dev];
+    CUcontext ctx = nullptr;
+    if (g_ctx_get_current(&ctx) != CUDA_SUCCESS)
+        return fail(OV_API_ECUDA, "odevec_solve_noalloc: cuCtxGetCurrent failed");
+    if (!ctx) {
+        /* no context yet on this thread: cudaSetDevice makes the runtime's
+           primary context of the current device current */
+        int dev = 0;
+        cudaError_t e = cudaGetDevice(&dev);
+        if (e == cudaSuccess)
+            e = cudaSetDevice(dev);
+        if (e != cudaSuccess)
+            return fail(OV_API_ECUDA, "odevec_solve_noalloc: %s", cudaGetErrorString(e));
+        if (g_ctx_get_current(&ctx) != CUDA_SUCCESS || !ctx)
+            return fail(OV_API_ECUDA, "odevec_solve_noalloc: no current CUDA context");
+    }
+    if (g_ctx_get_id(ctx, id) != CUDA_SUCCESS)
+        return fail(OV_API_ECUDA, "odevec_solve_noalloc: cuCtxGetId failed");
+    return OV_API_OK;
+}
+
+/* Device address of the static scratch in the current context.  In host
+   code the name ov_noalloc_scratch is only a handle, so the address is
+   looked up with cudaGetSymbolAddress once per context and cached. */
+int32_t noalloc_scratch(unsigned long long** out)
+{
+    std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+    unsigned long long id = 0;
+    int32_t rc = current_context_id(&id);
+    if (rc)
+        return rc;
+    for (int i = 0; i < kCacheSlots; ++i) {
+        if (g_noalloc_cache[i].ptr && g_noalloc_cache[i].ctx_id == id) {
+            *out = g_noalloc_cache[i].ptr;
+            return OV_API_OK;
+        }
+    }
+    void* p = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&p, ov_noalloc_scratch);
+    if (e != cudaSuccess || !p)
+        return fail(OV_API_ECUDA, "odevec_solve_noalloc: cudaGetSymbolAddress: %s", cudaGetErrorString(e));
+    /* slots of destroyed contexts are never matched again (IDs are not
+       reused); they are overwritten in turn once all slots are taken */
+    g_noalloc_cache[g_noalloc_next] = ScratchSlot{id, static_cast<unsigned long long*>(p)};
+    g_noalloc_next = (g_noalloc_next + 1) % kCacheSlots;
+    *out = static_cast<unsigned long long*>(p);
     return OV_API_OK;
 }
 
@@ -644,17 +707,13 @@ extern "C" int32_t odevec_solve_noalloc(const char* network, const odevec_opts* 
     if (o.group_size == 32 && ncells % 32)
         return fail(OV_API_EINVAL, "group_size 32 needs ncells divisible by 32 (got %lld)",
                     (long long)ncells);
-    int dev = 0;
-    cudaError_t err = cudaGetDevice(&dev);
-    if (err != cudaSuccess)
-        return fail(OV_API_ECUDA, "odevec_solve_noalloc: %s", cudaGetErrorString(err));
     unsigned long long* counter = nullptr;
-    rc = noalloc_scratch(dev, &counter);
+    rc = noalloc_scratch(&counter);
     if (rc)
         return rc;
     cudaStream_t st = (cudaStream_t)stream;
     /* the scratch keeps the previous call's count: the counter must start at 0 */
-    err = cudaMemsetAsync(counter, 0, sizeof(unsigned long long), st);
+    cudaError_t err = cudaMemsetAsync(counter, 0, sizeof(unsigned long long), st);
     if (err != cudaSuccess)
         return fail(OV_API_ECUDA, "odevec_solve_noalloc: %s", cudaGetErrorString(err));
     ov::LaunchArgs a;

@@ -99,8 +99,9 @@ def test_scheduling_does_not_change_results(gpu_lib, precision):
     for batch in [(0, 0, 0), (32, 32, 1000), (5, 20, 2)]:
         g = run_gpu(gpu_lib, wl, precision, batch=batch)
         assert_bitwise(g, ref, "batch %s" % (batch,))
-    # every staging, the block-synchronous one (6) included, with the
-    # default batches and with per-cell blocks
+    # every staging (6: staging 3's thread-local kernel in one 384-thread
+    # block per SM; 8-11: soft lockstep), with the default batches and with
+    # per-cell blocks
     for staging in (1, 2, 3, 4, 6, 8, 9, 10) + ((5, 11) if precision == "fp32_lu" else ()):
         for batch in [(0, 0, 0), (1, 1, -1)]:
             g = run_gpu(gpu_lib, wl, precision, batch=batch, staging=staging)

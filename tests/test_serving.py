@@ -6,6 +6,7 @@ import numpy as np
 import pytest
 
 from odevec_b200 import serving as SV
+from oracle_backend import OracleBackend
 
 
 def small_stream(n=6, steps=3, seed=9):
@@ -14,7 +15,7 @@ def small_stream(n=6, steps=3, seed=9):
                           cells=(32, 96), dt_hydro=(1e2, 1e8), steps=steps, max_requests=n)
 
 
-class BudgetProbe(SV.OracleBackend):
+class BudgetProbe(OracleBackend):
     def __init__(self):
         super().__init__()
         self.live = 0.0
@@ -47,9 +48,9 @@ def test_scheduler_completes_all_steps_within_budget(oracle):
 
 def test_results_same_alone_and_in_mix(oracle):
     reqs = small_stream()
-    _, mixed = SV.Scheduler(SV.OracleBackend(), 1e12, slots=4).run(reqs, realtime=False)
+    _, mixed = SV.Scheduler(OracleBackend(), 1e12, slots=4).run(reqs, realtime=False)
     for r in reqs:
-        _, alone = SV.Scheduler(SV.OracleBackend(), 1e12, slots=1).run([r], realtime=False)
+        _, alone = SV.Scheduler(OracleBackend(), 1e12, slots=1).run([r], realtime=False)
         assert np.array_equal(alone[r.rid].y, mixed[r.rid].y)
         assert np.array_equal(alone[r.rid].status, mixed[r.rid].status)
 
@@ -70,7 +71,7 @@ def failing_request(steps=3):
 
 def test_failed_cell_is_reported_and_masked_out(oracle):
     r = failing_request()
-    _, res = SV.Scheduler(SV.OracleBackend(), 1e12, slots=1).run([r], realtime=False)
+    _, res = SV.Scheduler(OracleBackend(), 1e12, slots=1).run([r], realtime=False)
     assert list(res[0].status) == [0, 0, 3, 0] and res[0].failed == 1
     # the failed cell stays at its failure state (the diverged iterate, NaN
     # and inf here); the others continue as a request without it
@@ -78,7 +79,7 @@ def test_failed_cell_is_reported_and_masked_out(oracle):
     assert np.array_equal(res[0].y[:, 2], y1[:, 2], equal_nan=True)
     ok = [0, 1, 3]
     r3 = SV.Request(1, r.network, r.y0[:, ok].copy(), r.dt_hydro, r.steps, 0.0, r.rtol, r.atol, r.dt_min, r.dt_in)
-    _, res3 = SV.Scheduler(SV.OracleBackend(), 1e12, slots=1).run([r3], realtime=False)
+    _, res3 = SV.Scheduler(OracleBackend(), 1e12, slots=1).run([r3], realtime=False)
     assert np.array_equal(res[0].y[:, ok], res3[1].y)
     assert SV.summarize([SV.StepRecord(0, 0, 4, r.network, 0.0, 1.0)], res)["failed_cells"] == 1
 
@@ -87,7 +88,7 @@ def test_resident_steps_equal_oracle_continuation(oracle):
     # the scheduler's per-request result is the oracle's continuation over
     # the request's hydro steps
     r = small_stream(n=1)[0]
-    _, res = SV.Scheduler(SV.OracleBackend(), 1e12, slots=1).run([r], realtime=False)
+    _, res = SV.Scheduler(OracleBackend(), 1e12, slots=1).run([r], realtime=False)
     ws = oracle.workspace(r.network, r.ncells)
     y, t, dt = r.y0, np.zeros(r.ncells), np.full(r.ncells, r.dt_in)
     for k in range(r.steps):
@@ -99,7 +100,7 @@ def test_resident_steps_equal_oracle_continuation(oracle):
 def test_over_budget_request_rejected(oracle):
     reqs = small_stream(n=2)
     with pytest.raises(ValueError, match="budget"):
-        SV.Scheduler(SV.OracleBackend(), 16.0, slots=2).run(reqs, realtime=False)
+        SV.Scheduler(OracleBackend(), 16.0, slots=2).run(reqs, realtime=False)
 
 
 @pytest.mark.gpu
@@ -120,7 +121,7 @@ def test_gpu_results_same_alone_and_in_mix(gpu_lib):
 @pytest.mark.gpu
 def test_gpu_failed_cell_matches_oracle_backend(gpu_lib, oracle):
     r = failing_request()
-    _, ref = SV.Scheduler(SV.OracleBackend(), 1e12, slots=1).run([r], realtime=False)
+    _, ref = SV.Scheduler(OracleBackend(), 1e12, slots=1).run([r], realtime=False)
     _, got = SV.Scheduler(SV.GpuBackend("fp64"), 1e12, slots=1).run([r], realtime=False)
     assert np.array_equal(got[0].status, ref[0].status) and got[0].failed == 1
     assert np.array_equal(got[0].y, ref[0].y, equal_nan=True)

@@ -6,9 +6,10 @@ where cudaMalloc is not allowed); it keeps the kernel's only scratch, the
 counter that hands out cells, in a static device array shared by all calls.
 This test calls it twice in a row through the C ABI -- the second call must
 not see the first call's counter -- and checks both results against
-odevec_solve on the same inputs.  FP64 without fused multiply-add is
-compared bit for bit, as everywhere in the GPU tests; FP32-LU likewise,
-since both entry points run the same kernel.  The file is named to be
+odevec_solve on the same inputs, and that the second call leaves the
+device's free memory unchanged (nothing allocated).  FP64 without fused
+multiply-add is compared bit for bit, as everywhere in the GPU tests;
+FP32-LU likewise, since both entry points run the same kernel.  The file is named to be
 collected last, so a run that stops at its first failure has run every
 other test before it.
 """
@@ -30,7 +31,7 @@ def _noalloc_fn(S):
     return f
 
 
-def _solve(S, wl, precision, noalloc):
+def _solve(S, wl, precision, noalloc, check_free=False):
     import torch
     # the allocation-free entry point has no FP32-LU escalation: compare with
     # the regular entry point without it
@@ -47,9 +48,18 @@ def _solve(S, wl, precision, noalloc):
     stream = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
     if noalloc:
         opts = ode._opts()
-        rc = _noalloc_fn(S)(wl.network.encode(), ctypes.byref(opts), wl.ncells, ptr(y), ptr(t),
-                            ptr(dt), ptr(ts), None, ptr(status), ptr(stats), stream)
+        fn = _noalloc_fn(S)
+        # every input and output exists before the first reading of free memory
+        torch.cuda.synchronize()
+        free_before = torch.cuda.mem_get_info()[0]
+        rc = fn(wl.network.encode(), ctypes.byref(opts), wl.ncells, ptr(y), ptr(t),
+                ptr(dt), ptr(ts), None, ptr(status), ptr(stats), stream)
         assert rc == 0, S.lib().odevec_last_error().decode()
+        torch.cuda.synchronize()
+        free_after = torch.cuda.mem_get_info()[0]
+        if check_free:
+            assert free_after == free_before, \
+                "device free memory changed by %d bytes" % (free_before - free_after)
     else:
         S.InitOdevec(ode)
         try:
@@ -67,7 +77,9 @@ def test_noalloc_matches_regular_entry_twice(gpu_lib, precision):
     ref = _solve(gpu_lib, wl, precision, noalloc=False)
     assert np.all(ref[3] == 0)
     for call in range(2):
-        got = _solve(gpu_lib, wl, precision, noalloc=True)
+        # the first call may load the kernel's module (lazy loading) and look
+        # up the scratch address; the second must leave device memory as it was
+        got = _solve(gpu_lib, wl, precision, noalloc=True, check_free=call == 1)
         for name, a, b in zip(["y", "t", "dt", "status", "stats"], got, ref):
             assert np.array_equal(a, b), "call %d: %s differs" % (call + 1, name)
 
