@@ -162,7 +162,16 @@ int32_t odevec_solve_host(odevec_solver* s, int64_t ncells, double* y, double* t
    every successfully finished cell; resume = 1 continues each cell from its
    saved state to the new t_stop (the Jacobian and rate coefficients are
    recomputed, so the caller may change the temperature between calls; it
-   must not change the dynamic species).  Other arguments as odevec_solve. */
+   must not change the dynamic species).  resume = 2 starts fresh exactly as
+   odevec_solve, except that each cell's last Newton correction of the
+   previous call (en_old) is taken from the workspace: the reference's
+   solver object never resets this%en_old (src/odevec.F90:170-182, 464), and
+   a call whose first step restarts at order 1 after three error-test
+   failures reads it in CalcStepSizeOrder (:571).  A caller that makes its
+   first call with resume = 0 and every later call with resume = 2
+   reproduces a reference driver's repeated SolveODE calls on one solver
+   object (tests/rober.f90:57-62) bit for bit.  Other arguments as
+   odevec_solve. */
 int32_t odevec_workspace_doubles(const char* network, int64_t* per_cell);
 int32_t odevec_solve_resident(odevec_solver* s, int64_t ncells, double* y, double* t, double* dt,
                               const double* t_stop, const uint8_t* mask, int32_t* status,

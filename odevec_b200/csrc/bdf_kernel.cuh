@@ -670,7 +670,9 @@ struct Cell {
         }
         s = s + fz_add;
         const double mx = group_max<G>(msk ? s : -HUGE_VAL);
-        const double d = sqrt(tol / (1.0 / (W0 * W0) + mx / N));
+        /* W0**(-2.0): a real exponent other than -1, 0, 1 or 2 is a pow() call
+           in the reference's compiled Fortran, not 1/(W0*W0) */
+        const double d = sqrt(tol / (ov_pow(W0, -2.0) + mx / N));
         const double span = fabs(tstop - t);
         return d < span ? d : span;
     }
@@ -902,7 +904,7 @@ __global__ void __launch_bounds__(StageCfg<STAGE>::BS, StageCfg<STAGE>::MINB) bd
                 if (skip) {
                     c.t = c.tstop; /* src/odevec.F90:187-191 */
                     ph = PH_DONE;
-                } else if (A.resume) {
+                } else if (A.resume == 1) {
                     /* continuation: the saved history, step, order and
                        weights; the state is the saved y_NS(0); rates and
                        Jacobian are recomputed (the caller may have changed
@@ -926,6 +928,14 @@ __global__ void __launch_bounds__(StageCfg<STAGE>::BS, StageCfg<STAGE>::MINB) bd
                         ph = PH_DONE;
                     }
                 } else {
+                    if (A.resume == 2) {
+                        /* a fresh SolveODE that keeps the previous call's
+                           last correction vector, as the reference's solver
+                           object does (this%en_old is never reset) */
+#pragma unroll
+                        for (int j = 0; j < ND; ++j)
+                            c.eno[j] = A.ws[((int64_t)(MAXQ + 1) * ND + j) * ncells + cell];
+                    }
                     if (Net::NREA > 0)
                         Net::rates_T(c.y, c.rT);
 #pragma unroll

@@ -354,8 +354,9 @@ int32_t odevec_solve_resident(odevec_solver* s, int64_t ncells, double* y, doubl
 {
     if (!workspace)
         return fail(OV_API_EINVAL, "odevec_solve_resident: workspace is null");
-    return solve_impl(s, ncells, y, t, dt, t_stop, mask, status, stats, workspace, resume ? 1 : 0,
-                      stream);
+    if (resume < 0 || resume > 2)
+        return fail(OV_API_EINVAL, "odevec_solve_resident: resume must be 0, 1 or 2 (got %d)", resume);
+    return solve_impl(s, ncells, y, t, dt, t_stop, mask, status, stats, workspace, resume, stream);
 }
 
 static int32_t solve_impl(odevec_solver* s, int64_t ncells, double* y, double* t, double* dt,

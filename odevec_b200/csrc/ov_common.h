@@ -299,4 +299,19 @@ template <>
 OV_HD OV_INLINE float ov_divp<float>(float x, float p) { return x * p; }
 #endif
 
+/* Host builds of the CPU oracle with OV_LIBM defined call the C library's
+   exp, log, log10 and pow instead, as the reference's Fortran does, so that
+   the oracle can be compared bit for bit with runs of the reference's own
+   solver module.  Device code never sees this. */
+#if defined(OV_LIBM) && !defined(__CUDACC__)
+#define ov_exp(x) exp(x)
+#define ov_log(x) log(x)
+#define ov_log10(x) log10(x)
+#define ov_pow(x, y) pow((x), (y))
+#define ov_exp_sel(x) exp(x)
+#define ov_log_sel(x) log(x)
+#define ov_log10_sel(x) log10(x)
+#define ov_pow_sel(x, y) pow((x), (y))
+#endif
+
 #endif /* OV_COMMON_H */

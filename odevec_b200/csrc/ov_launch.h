@@ -30,7 +30,9 @@ struct LaunchArgs {
     /* resident integrator state (continuation across calls): ws = null for
        none; otherwise ws holds ws_doubles(ND) doubles per cell, [field][cell],
        written at the end of every successful solve and, with resume = 1,
-       read at the start instead of a fresh start */
+       read at the start instead of a fresh start; with resume = 2 the start
+       is fresh but takes en_old (the previous call's last correction) from
+       it, as the reference's solver object keeps this%en_old between calls */
     double* ws;
     int32_t resume;
     /* if non-null, the kernel returns at once unless *run_if != 0 (a count

@@ -482,7 +482,9 @@ struct WCell {
         double s = ordered_sum(p);
         s = s + fz_add;
         const double mx = group_max<1>(msk ? s : -HUGE_VAL);
-        const double d = sqrt(tol / (1.0 / (W0 * W0) + mx / N));
+        /* W0**(-2.0): a real exponent other than -1, 0, 1 or 2 is a pow() call
+           in the reference's compiled Fortran, not 1/(W0*W0) */
+        const double d = sqrt(tol / (ov_pow(W0, -2.0) + mx / N));
         const double span = fabs(tstop - t);
         return d < span ? d : span;
     }
@@ -551,7 +553,7 @@ struct WCell {
             return;
         }
         double f[NS], den[NS];
-        if (A.resume) {
+        if (A.resume == 1) {
             load_state(A.ws, ncells, cell);
             double v[NS];
 #pragma unroll
@@ -568,6 +570,14 @@ struct WCell {
             }
             told = t;
         } else {
+            if (A.resume == 2) {
+                /* the previous call's last correction vector (this%en_old) */
+                const int f0 = (MAXQ + 1) * ND;
+#pragma unroll
+                for (int m = 0; m < NS; ++m)
+                    if (own(m))
+                        eno[m] = A.ws[((int64_t)f0 + lane + 32 * m) * ncells + cell];
+            }
 #pragma unroll
             for (int m = 0; m < NS; ++m)
                 yns[0][m] = own(m) ? yv[sp[m]] : 0.0;

@@ -214,25 +214,31 @@ def orego_schedule(ncells: int = 4096, network: str = "OREGO_CSC_CMK", t_end: fl
 def primordial_schedule(ncells: int = 8192, network: str = "PRIMORDIAL_CSC_FF", tgas: float = 1000.0) -> Schedule:
     """tests/primordial.f90:43-92: mass fractions (H 0.75615, He 0.24375,
     e- 4.46406e-8, H+ 8.1967e-5, H2 1.5123e-6, traces 1e-40, the rest 1e-20)
-    normalised per cell, rho = 1e-10 g/cm^3, t_stop = 1e8, 2e8, ... up to
-    1e10, dt carried from 2.2954626201190183e-26, rtol 1e-4, atol 1e-20,
-    dt_min 1e-20.  The reference's rate function fixes Tgas at 1000 K; here
-    the temperature row passes through the conversion and holds tgas."""
+    normalised per cell by their sum taken in index order, rho = 1e-10 g/cm^3,
+    t_stop = 1e8, 2e8, ... up to 1e10, dt carried from
+    2.2954626201190183E-026, rtol 1e-4, atol 1e-20, dt_min 1e-20.  Every
+    real literal of the driver without a d exponent (the fractions, 1e-20,
+    rho's 1e-10, the first dt, the loop bound 1e10) is single precision.
+    The reference's rate function fixes Tgas at 1000 K; here the temperature
+    row passes through the conversion and holds tgas."""
     from .networks import PRIMORDIAL_SPECIES as SP
     x = np.full((16, ncells), _f32(1e-20))
     vals = {"H": 0.75615, "E": 4.46406e-8, "H+": 8.1967e-5, "D": 1.0e-40, "D+": 1.0e-40, "HE": 0.24375,
             "HE+": 1.0e-40, "H2+": 1.0e-40, "H2": 1.5123e-6, "HD": 1.0e-40, "H-": 1.0e-40, "HE++": 1.0e-40}
     for name, v in vals.items():
         x[SP.index(name)] = _f32(v)
-    x[:12] = x[:12] / x[:12].sum(axis=0)
+    total = x[0].copy()
+    for j in range(1, 12):          # sum(x(i,:)) accumulates in index order
+        total = total + x[j]
+    x[:12] = x[:12] / total
     x[12:] = 0.0
     x[SP.index("Tgas")] = tgas
     ts, t = [], 0.0
     while t < _f32(1e10):
         t = t + 1e8
         ts.append(t)
-    return Schedule(network, x, 0.0, 2.2954626201190183e-26, ts, 1e-4, 1e-20, 1e-20,
-                    rho=np.full(ncells, 1e-10))
+    return Schedule(network, x, 0.0, _f32(2.2954626201190183e-26), ts, 1e-4, 1e-20, 1e-20,
+                    rho=np.full(ncells, _f32(1e-10)))
 
 
 def run_schedule(sch: Schedule, precision: str = "fp64", graph: bool = False, chunk: int = 64, ode=None):

@@ -256,7 +256,14 @@ def SolveODE(ode: Odevec, time, dt, t_stop, y, Mask=None, stream=None, want_stat
     ``(time, dt)`` after the solve (``time == t_stop``).  ``Mask``: optional
     per-cell booleans.  Per-cell status and statistics are left in
     ``ode.status`` / ``ode.stats``.
+
+    ``workspace`` (from :func:`Workspace`) keeps each cell's integrator state
+    between calls.  ``resume``: False/0 starts fresh and saves the state;
+    True/1 continues from the saved state; ``"en_old"``/2 starts fresh but
+    keeps the previous call's last Newton correction, as the reference's
+    solver object does between SolveODE calls (this%en_old is never reset).
     """
+    resume_code = {False: 0, True: 1, 2: 2, "en_old": 2}[resume]
     h = ode.handle
     is_torch = False
     try:
@@ -292,7 +299,7 @@ def SolveODE(ode: Odevec, time, dt, t_stop, y, Mask=None, stream=None, want_stat
                     raise ValueError("workspace too small: use Workspace(ode, ncells)")
                 _check(lib().odevec_solve_resident(h, ncells, ptr(y), ptr(t), ptr(d), ptr(ts), ptr(m),
                                                    ptr(status), ptr(stats), ptr(workspace),
-                                                   1 if resume else 0,
+                                                   resume_code,
                                                    ctypes.c_void_p(st.cuda_stream)))
         ode.status, ode.stats = status, stats
         if ode.raise_on_failure:

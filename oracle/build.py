@@ -11,25 +11,30 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 SRC = os.path.join(HERE, "odevec_oracle.c")
 LIB = os.path.join(HERE, "libodevec_oracle.so")
+LIB_LIBM = os.path.join(HERE, "libodevec_oracle_libm.so")
 
 
-def build(force: bool = False, verbose: bool = False) -> str:
+def build(force: bool = False, verbose: bool = False, libm: bool = False) -> str:
+    """libm: the variant whose exp/log/log10/pow are the C library's (-DOV_LIBM),
+    compared bit for bit with runs of the reference's own solver module."""
+    lib = LIB_LIBM if libm else LIB
     deps = [SRC, os.path.join(HERE, "..", "include", "odevec_b200.h")]
     gen = os.path.join(HERE, "..", "odevec_b200", "csrc")
     for root, _, files in os.walk(gen):
         deps += [os.path.join(root, f) for f in files if f.endswith((".h", ".inc"))]
-    if (not force and os.path.exists(LIB)
-            and os.path.getmtime(LIB) >= max(os.path.getmtime(d) for d in deps)):
-        return LIB
+    if (not force and os.path.exists(lib)
+            and os.path.getmtime(lib) >= max(os.path.getmtime(d) for d in deps)):
+        return lib
     cmd = ["gcc", "-std=gnu11", "-O2", "-ffp-contract=off", "-fno-fast-math", "-fPIC", "-shared",
-           "-fopenmp", "-Wall", "-Wno-unused-function", "-Wno-unused-variable", "-o", LIB + ".tmp",
-           SRC, "-lm"]
+           "-fopenmp", "-Wall", "-Wno-unused-function", "-Wno-unused-variable", "-o", lib + ".tmp",
+           SRC, "-lm"] + (["-DOV_LIBM"] if libm else [])
     if verbose:
         print(" ".join(cmd))
     subprocess.run(cmd, check=True)
-    os.replace(LIB + ".tmp", LIB)
-    return LIB
+    os.replace(lib + ".tmp", lib)
+    return lib
 
 
 if __name__ == "__main__":
     print(build(force="--force" in sys.argv, verbose=True))
+    print(build(force="--force" in sys.argv, verbose=True, libm=True))

@@ -705,7 +705,9 @@ static double initial_step_size(ode_t* o, double time, double t_stop, const doub
         if (s > mx)
             mx = s;
     }
-    double dt = sqrt(tol / (1.0 / (W0 * W0) + mx / n));
+    /* W0**(-2.0) (:231, :233): gfortran keeps a real exponent other than -1,
+       0, 1 or 2 as a pow() call, which is not 1/(W0*W0) in the last bit */
+    double dt = sqrt(tol / (ov_pow(W0, -2.0) + mx / n));
     const double span = fabs(t_stop - time);
     return dt < span ? dt : span;
 }
@@ -922,9 +924,11 @@ int ov_oracle_solve(const char* tag, int64_t ncells, int G, double rtol, double 
             memset(o.en_old, 0, sizeof(double) * N);
             double time = t[c0], h = dt[c0];
             double* w = ws ? ws + (size_t)g * ws_group_doubles(n, G) : NULL;
+            if (resume == 2 && w) /* the reference keeps this%en_old between calls */
+                memcpy(o.en_old, w + N * (MAXORDER + 1), sizeof(double) * N);
             if (bad)
                 o.status = OV_ERR_GROUP_MISMATCH;
-            else if (resume && w)
+            else if (resume == 1 && w)
                 resume_group(&o, &time, &h, t_stop[c0], o.ytmp, w);
             else
                 solve_group(&o, &time, &h, t_stop[c0], o.ytmp, w);
