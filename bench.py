@@ -60,6 +60,10 @@ def parse():
     p.add_argument("--accuracy-cells", type=int, default=256)
     p.add_argument("--no-cpu", action="store_true")
     p.add_argument("--no-configs", action="store_true", help="skip the ROBER/OREGO/SYN64 lines")
+    p.add_argument("--serving-duration", type=float, default=8.0,
+                   help="seconds of Poisson arrivals in the serving block (0: no serving block)")
+    p.add_argument("--serving-rate", type=float, default=1.0, help="mean arrivals per second")
+    p.add_argument("--serving-seed", type=int, default=5)
     return p.parse_args()
 
 
@@ -156,14 +160,37 @@ def traffic_per_cell():
     return None
 
 
-def oracle_rate(wl, ncells, threads):
+def oracle_rate(wl, ncells, threads, fast=True):
+    """cells/s of the CPU restatement of the reference (oracle/) on the first
+    ncells cells: fast = the -O3 -march=native build with contraction, else
+    the parity build (-O2, no contraction, bit-identical to the GPU fp64 form)"""
     from oracle import oracle as O
     sub = slice(0, ncells)
+    O.lib(fast=fast)            # build / load outside the timed region
     t0 = time.perf_counter()
     _, _, _, st, _ = O.solve(wl.network, wl.y[:, sub], wl.t0[sub], wl.dt0[sub], wl.t_stop[sub], wl.rtol,
-                             wl.atol, wl.dt_min, group=wl.group, nthreads=threads)
+                             wl.atol, wl.dt_min, group=wl.group, nthreads=threads, fast=fast)
     el = time.perf_counter() - t0
     return ncells / el, el, int((st != 0).sum())
+
+
+def cpu_model():
+    from oracle import build as OB
+    return OB.cpu_model()
+
+
+def cpu_baseline(wl, ncells, threads):
+    """the reported CPU baseline: the -O3 build timed on ncells cells, the
+    parity build beside it"""
+    v, el, f = oracle_rate(wl, ncells, threads, fast=True)
+    vp, elp, _ = oracle_rate(wl, ncells, threads, fast=False)
+    return {"value": v, "unit": "cells/s", "cores": threads, "kind": "port_O3",
+            "cpu_model": cpu_model(),
+            "sample": "%d cells of the same workload (%.1f s), oracle/ C restatement of src/odevec.F90 "
+                      "built -O3 -march=native, OpenMP over cells" % (ncells, el),
+            "failed_cells": f,
+            "parity_build": {"value": vp, "kind": "port", "sample_s": elp,
+                             "build": "-O2 -ffp-contract=off (bit-identical to the GPU fp64 form)"}}
 
 
 def host_threads():
@@ -187,17 +214,21 @@ def run_reference(args):
         _, el, _ = oracle_rate(wl, args.cpu_sample, threads)
         times.append(el)
     value = args.cpu_sample * len(times) / sum(times)
+    vp, elp, _ = oracle_rate(wl, args.cpu_sample, threads, fast=False)
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": "cells/s", "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * sum(times) / len(times),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": DATA,
         "config": {"workload": workload_label(args, args.ncells), "network": args.network,
                    "sample_cells_per_step": args.cpu_sample},
-        "cpu_baseline": {"value": value, "unit": "cells/s", "cores": threads, "kind": "port",
+        "cpu_baseline": {"value": value, "unit": "cells/s", "cores": threads, "kind": "port_O3",
+                         "cpu_model": cpu_model(),
                          "sample": "%d of the workload's cells per step, oracle/ (C restatement of "
-                                   "src/odevec.F90), %s, OpenMP over cells" % (
+                                   "src/odevec.F90) built -O3 -march=native, %s, OpenMP over cells" % (
                                        args.cpu_sample, "per-cell control" if wl.group == 1 else
-                                       "lockstep groups of %d" % wl.group)},
+                                       "lockstep groups of %d" % wl.group),
+                         "parity_build": {"value": vp, "kind": "port", "sample_s": elp,
+                                          "build": "-O2 -ffp-contract=off"}},
         "e2e": {"value": value, "unit": "cells/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -363,6 +394,10 @@ def run_product(args):
         "roofline": {"bound": "fp64", "achieved": achieved, "peak": peaks["fp64"], "unit": "TFLOP/s",
                      "frac": achieved / peaks["fp64"],
                      "traffic": None if tpc is None else tpc * N,
+                     "traffic_source": None if tpc is None else
+                     "not measured in this run: DRAM bytes per cell of the solve kernel from the ncu "
+                     "capture in profiles/bdf_kernel_primordial_ncu.txt (262,144 cells), times the "
+                     "cells of one launch",
                      "algorithmic_flops_per_launch": r["flops_per_launch"],
                      "algorithmic_bytes_per_launch": alg_bytes,
                      "achieved_hbm_gbs": alg_bytes / (r["kernel_ms"] * 1e-3) / 1e9,
@@ -382,36 +417,63 @@ def run_product(args):
     if "plain_fp64" in res and "fp32_lu" in res:
         line["fp32lu_over_plain_fp64"] = res["fp32_lu"]["value"] / res["plain_fp64"]["value"]
     if world == 1 and not args.no_cpu:
-        threads = host_threads()
-        v, el, f = oracle_rate(W.BUILDERS[args.workload](ncells=args.cpu_sample, seed=3, network=args.network),
-                               args.cpu_sample, threads)
-        line["cpu_baseline"] = {"value": v, "unit": "cells/s", "cores": threads, "kind": "port",
-                                "sample": "%d cells of the same workload (%.1f s)" % (args.cpu_sample, el)}
+        line["cpu_baseline"] = cpu_baseline(
+            W.BUILDERS[args.workload](ncells=args.cpu_sample, seed=3, network=args.network),
+            args.cpu_sample, host_threads())
     if world == 1 and args.accuracy_cells > 0 and args.workload == "PRIMORDIAL":
         line["accuracy"] = accuracy(args, wl, S, torch)
     if world == 1 and not args.no_configs:
-        line["other_configs"] = other_configs(args, torch, S, W)
+        line["other_configs"] = other_configs(args, torch, S, W, peaks)
+    if world == 1 and args.serving_duration > 0:
+        line["serving"] = serving_block(args)
+        iso = line["serving"].get("isolated", {})
+        line["latency_ms"] = {"p50": line["serving"]["mix"]["p50_ms"], "p99": line["serving"]["mix"]["p99_ms"],
+                              "isolated_p99": iso.get("p99_ms"),
+                              "p99_over_isolated_p99": iso.get("mix_p99_over_isolated_p99"),
+                              "what": "hydro-step latency of the serving stream (serving block)"}
     print(json.dumps(line), flush=True)
     if world > 1:
         dist.destroy_process_group()
 
 
+def _rel_err(g, ref, mask):
+    rel = np.abs(g[mask] - ref[mask]) / np.abs(ref[mask])
+    return rel
+
+
 def accuracy(args, wl, S, torch):
-    """Max relative error of each form at rtol 1e-6 against the oracle at
-    rtol 1e-12 (species above atol/rtol), on a sample of cells."""
+    """Errors of each form at rtol 1e-6 against the oracle at rtol 1e-12 on a
+    sample of cells, and where they come from: per species, per abundance
+    relative to n_H, under three floors (species above atol/rtol, above atol,
+    above 1e-12 n_H), the worst cells, the oracle's own convergence (rtol
+    1e-12 against 1e-13) and an rtol sweep of the FP64 form."""
     from oracle import oracle as O
+    from odevec_b200 import networks as NW
+    from odevec_b200 import workloads as WL
     n = args.accuracy_cells
     sub = slice(0, n)
-    ref, _, _, st, _ = O.solve(wl.network, wl.y[:, sub], wl.t0[sub], wl.dt0[sub], wl.t_stop[sub], 1e-12,
-                               1e-26, wl.dt_min, group=1, nthreads=host_threads(), fix_restart=True)
+    thr = host_threads()
+
+    def oracle_at(rtol, fix=True):
+        y, _, _, st, _ = O.solve(wl.network, wl.y[:, sub], wl.t0[sub], wl.dt0[sub], wl.t_stop[sub], rtol,
+                                 rtol * 1e-14, wl.dt_min, group=1, nthreads=thr, fix_restart=fix)
+        return y, int((st != 0).sum())
+    ref, f12 = oracle_at(1e-12)
+    ref13, f13 = oracle_at(1e-13)
+    nh = WL.primordial_invariants(wl.y[:, sub])[0]      # hydrogen nuclei per cell (constant)
+    names = list(NW.PRIMORDIAL_SPECIES[:12])
+    floors = {"above_atol_over_rtol": np.abs(ref[:12]) > wl.atol / wl.rtol,
+              "above_atol": np.abs(ref[:12]) > wl.atol,
+              "above_1e-12_nH": np.abs(ref[:12]) > 1e-12 * nh[None, :]}
+    selfc = _rel_err(ref[:12], ref13[:12], floors["above_atol_over_rtol"])
     out = {"oracle_rtol": 1e-12, "oracle_fix_restart": True, "cells": n,
-           "oracle_failures": int((st != 0).sum())}
-    # plain_fp64 schedules the fp64 form differently; its results are the same
-    runs = [(f, False) for f in args.forms.split(",") if f != "plain_fp64"] + [("fp32_lu", True),
-                                                                            ("fp64", True)]
-    got = {}
-    for form, fix in runs:
-        ode = S.Odevec(wl.network, RelativeTolerance=wl.rtol, AbsoluteTolerance=wl.atol,
+           "oracle_failures": f12, "oracle_self_convergence": {
+               "what": "oracle at rtol 1e-12 against rtol 1e-13, species above 1e-14",
+               "max_rel": float(selfc.max()), "p99_rel": float(np.percentile(selfc, 99)),
+               "failures_1e-13": f13}}
+
+    def solve(form, rtol, fix):
+        ode = S.Odevec(wl.network, RelativeTolerance=rtol, AbsoluteTolerance=wl.atol,
                        MinimalTimestep=wl.dt_min, nvector=1, precision=form, raise_on_failure=False,
                        fix_restart=fix)
         S.InitOdevec(ode)
@@ -419,30 +481,76 @@ def accuracy(args, wl, S, torch):
         S.SolveODE(ode, torch.tensor(wl.t0[sub], device="cuda"), torch.tensor(wl.dt0[sub], device="cuda"),
                    torch.tensor(wl.t_stop[sub], device="cuda"), y)
         g = y.cpu().numpy()
-        got[(form, fix)] = g
         S.CloseOdevec(ode)
-        m = np.abs(ref[:12]) > wl.atol / wl.rtol
-        rel = np.abs(g[:12][m] - ref[:12][m]) / np.abs(ref[:12][m])
-        out[form + ("+fix_restart" if fix else "")] = {
-            "max_rel_err": float(rel.max()), "median_rel_err": float(np.median(rel)),
-            "p99_rel_err": float(np.percentile(rel, 99)), "max_over_rtol": float(rel.max() / wl.rtol)}
+        return g
+    forms = [f for f in args.forms.split(",") if f != "plain_fp64"]
+    got = {}
+    for form in forms:
+        for fix in (False, True):
+            g = solve(form, wl.rtol, fix)
+            got[(form, fix)] = g
+            blk = {}
+            for fname, m in floors.items():
+                rel = _rel_err(g[:12], ref[:12], m)
+                blk[fname] = {"max_rel_err": float(rel.max()), "p99_rel_err": float(np.percentile(rel, 99)),
+                              "median_rel_err": float(np.median(rel)), "max_over_rtol": float(rel.max() / wl.rtol)}
+            out[form + ("+fix_restart" if fix else "")] = blk
+    # where the largest errors live (the FP32-LU form as the reference restarts)
+    g = got[(forms[0], False)]
+    m = floors["above_atol_over_rtol"]
+    err = np.where(m, np.abs(g[:12] - ref[:12]) / np.maximum(np.abs(ref[:12]), 1e-300), 0.0)
+    out["by_species"] = {names[j]: {"max_rel_err": float(err[j].max()),
+                                    "cells_above_10rtol": int((err[j] > 10 * wl.rtol).sum())}
+                         for j in range(12)}
+    ab = np.abs(ref[:12]) / nh[None, :]
+    bins = [(0, 1e-14), (1e-14, 1e-10), (1e-10, 1e-6), (1e-6, 1e-2), (1e-2, 10.0)]
+    out["by_abundance_over_nH"] = {"%.0e..%.0e" % (lo, hi): {
+        "max_rel_err": float(err[(ab >= lo) & (ab < hi) & m].max()) if np.any((ab >= lo) & (ab < hi) & m) else None,
+        "entries": int(np.sum((ab >= lo) & (ab < hi) & m))} for lo, hi in bins}
+    worst = np.argsort(err.ravel())[::-1][:5]
+    out["worst"] = [{"cell": int(k % n), "species": names[k // n], "rel_err": float(err.ravel()[k]),
+                     "abundance_over_nH": float(ab.ravel()[k]), "t_end": float(wl.t_stop[k % n]),
+                     "T": float(wl.y[14, k % n])} for k in worst]
+    # the global error's scaling: the FP64 form at tighter tolerances
+    sweep = {}
+    for rt in (1e-6, 1e-7, 1e-8):
+        g = solve("fp64", rt, True)
+        rel = _rel_err(g[:12], ref[:12], np.abs(ref[:12]) > wl.atol / rt)
+        sweep["%.0e" % rt] = {"max_rel_err": float(rel.max()), "max_over_rtol": float(rel.max() / rt),
+                              "p99_rel_err": float(np.percentile(rel, 99))}
+    out["rtol_sweep_fp64_fix_restart"] = sweep
     # what the FP32 factors add: FP32-LU against the FP64 path at the same rtol
     if ("fp32_lu", False) in got and ("fp64", False) in got:
         a, b = got[("fp32_lu", False)][:12], got[("fp64", False)][:12]
-        m = np.abs(b) > wl.atol / wl.rtol
-        rel = np.abs(a[m] - b[m]) / np.abs(b[m])
+        rel = _rel_err(a, b, np.abs(b) > wl.atol / wl.rtol)
         out["fp32_lu_vs_fp64_same_rtol"] = {"max_rel_err": float(rel.max()), "median_rel_err": float(np.median(rel)),
                                             "max_over_rtol": float(rel.max() / wl.rtol)}
     return out
 
 
-def other_configs(args, torch, S, W):
+def serving_block(args):
+    """A bounded serving run: Poisson arrivals of ROBER, PRIMORDIAL and SYN64
+    requests (1k..256k cells, 50 hydro steps each, dt 1e6..1e11 s, 120 GB
+    budget) at a rate near the device's capacity, FP32-LU form, and every
+    request run again alone; step latencies p50/p99 in the mix and alone."""
+    from odevec_b200 import serving as SV
+    t0 = time.perf_counter()
+    out = SV.measure(rate=args.serving_rate, duration=args.serving_duration, steps=50,
+                     precisions=("fp32_lu",), seed=args.serving_seed, isolated=True)[0]
+    out["wall_s"] = time.perf_counter() - t0
+    out.pop("per_network", None)
+    return out
+
+
+def other_configs(args, torch, S, W, peaks):
     """cells/s of the other configurations (FP64 and FP32-LU), one timed
-    solve each after one untimed one, inputs reset from a device copy."""
+    solve each after one untimed one, inputs reset from a device copy, with
+    the FP64 roofline of the kernel and the CPU baseline on a sample."""
+    from odevec_b200 import metrics
     out = {}
-    cases = [("ROBER", W.rober(ncells=4096)), ("OREGO", W.orego(ncells=65536)),
-             ("SYN64", W.syn64(ncells=262144))]
-    for name, wl in cases:
+    cases = [("ROBER", W.rober(ncells=4096), 4096), ("OREGO", W.orego(ncells=65536), 16384),
+             ("SYN64", W.syn64(ncells=262144), 1024)]
+    for name, wl, cpu_n in cases:
         row = {"network": wl.network, "cells": wl.ncells, "group": wl.group}
         for form in ("fp64", "fp32_lu"):
             ode = S.Odevec(wl.network, RelativeTolerance=wl.rtol, AbsoluteTolerance=wl.atol,
@@ -466,10 +574,19 @@ def other_configs(args, torch, S, W):
                     stats = ode.stats.cpu().numpy()
                     fails = int((ode.status != 0).sum().item())
                 ms = e0.elapsed_time(e1)
+            flops = float(metrics.flops_per_cell(wl.network, stats).sum())
+            ach = flops / (ms * 1e-3) / 1e12
             row[form] = {"cells_per_s": wl.ncells / (ms * 1e-3), "ms": ms, "failed_cells": fails,
-                         "mean_newton_iters": float(stats[:, 4].mean()), "mean_steps": float(stats[:, 0].mean())}
+                         "mean_newton_iters": float(stats[:, 4].mean()), "mean_steps": float(stats[:, 0].mean()),
+                         "roofline": {"bound": "fp64", "achieved": ach, "peak": peaks["fp64"],
+                                      "unit": "TFLOP/s", "frac": ach / peaks["fp64"],
+                                      "algorithmic_flops_per_launch": flops,
+                                      "fp64_share_of_flops": metrics.fp64_fraction(wl.network, stats,
+                                                                                    form == "fp32_lu")}}
             S.CloseOdevec(ode)
         row["fp32lu_over_fp64"] = row["fp32_lu"]["cells_per_s"] / row["fp64"]["cells_per_s"]
+        if not args.no_cpu:
+            row["cpu_baseline"] = cpu_baseline(wl, min(cpu_n, wl.ncells), host_threads())
         out[name] = row
     return out
 

@@ -191,6 +191,9 @@ template <> struct StageCfg<10> { static constexpr int SHM = 2; static constexpr
 /* soft lockstep, one block of 192 threads per SM with history and LU in
    shared memory (fits with FP32 factors) */
 template <> struct StageCfg<11> { static constexpr int SHM = 1; static constexpr bool SOFT = true;  static constexpr int BS = 192, MINB = 1, REFILL = 16, PERIOD = 4; };
+/* as 9 with 384 threads (12 warps) per SM: the history of 384 cells fills
+   the shared memory (221 KB for 12 species) */
+template <> struct StageCfg<12> { static constexpr int SHM = 2; static constexpr bool SOFT = true;  static constexpr int BS = 384, MINB = 1, REFILL = 16, PERIOD = 4; };
 
 /* Soft lockstep.  The warps of a block wait for each other at the top of
    every trip of the cell loop, so they run the same phase code at the same
@@ -286,7 +289,9 @@ struct Cell {
     double y[N];
     typename Staging<Net, LUT, SHM, BS>::LU a; /* packed LU of the iteration matrix */
     double rT[NR];
-    double sc[SCALED ? ND : 1], isc[SCALED ? ND : 1];
+    /* FP32 LU: the scale of species j is 2^sce[j] (kept as an exponent, the
+       factors are formed only while the Jacobian and the solve run) */
+    short sce[SCALED ? ND : 1];
 
     double t, h, told, tstop, crate, jchg, cerr, tint;
     double fz_add; /* 0, or NaN when a frozen species has a non-finite error weight */
@@ -545,6 +550,7 @@ struct Cell {
     /* GetJac + LUDecompose (src/odevec.F90:301-315) */
     __device__ __forceinline__ void jacobian_lu()
     {
+        double sc[SCALED ? ND : 1], isc[SCALED ? ND : 1];
         if constexpr (SCALED) {
             /* scale by powers of two close to the error weights (exact in
                FP64), then round to FP32 */
@@ -553,12 +559,13 @@ struct Cell {
                 int e = (int)((ov_d2bits(w2[j]) >> 52) & 0x7ff) - 1023;
                 int hexp = e >= 0 ? e / 2 : -((-e + 1) / 2);
                 hexp = hexp > 480 ? 480 : (hexp < -480 ? -480 : hexp);
+                sce[j] = (short)hexp;
                 sc[j] = ov_pow2i(hexp);
                 isc[j] = ov_pow2i(-hexp);
             }
         }
         if constexpr (Net::LU_METHOD == 3) {
-            fd_jacobian();
+            fd_jacobian(sc, isc);
         } else {
             double k[NR];
             Net::rates_k(y, rT, k);
@@ -578,7 +585,7 @@ struct Cell {
        whatever their off-diagonal values, so they never reach a solution.
        Every array index is a compile-time constant (the perturbed column
        is selected, not indexed), so the state stays in registers. */
-    __device__ __forceinline__ void fd_jacobian()
+    __device__ __forceinline__ void fd_jacobian(const double* sc, const double* isc)
     {
         const double uround = 2.2204460492503131e-16;  /* 2^-52 */
         const double srur = 1.4901161193847656e-08;    /* 2^-26 */
@@ -643,10 +650,17 @@ struct Cell {
 #pragma unroll
         for (int j = 0; j < ND; ++j)
             res[j] = h * f[Net::dyn(j)] - (yns[1][j] + en[j]);
-        if constexpr (SCALED)
+        if constexpr (SCALED) {
+            double sc[ND], isc[ND];
+#pragma unroll
+            for (int j = 0; j < ND; ++j) {
+                sc[j] = ov_pow2i(sce[j]);
+                isc[j] = ov_pow2i(-sce[j]);
+            }
             Net::template lu_solve<LUT>(a, res, den, sc, isc);
-        else
+        } else {
             Net::template lu_solve<LUT>(a, res, den, nullptr, nullptr);
+        }
         const double l0 = lcoef(q, 0);
 #pragma unroll
         for (int j = 0; j < ND; ++j) {
@@ -888,6 +902,14 @@ __global__ void __launch_bounds__(StageCfg<STAGE>::BS, StageCfg<STAGE>::MINB) bd
 #pragma unroll
             for (int j = 0; j < ND; ++j)
                 c.eno[j] = 0.0;
+            if constexpr (Net::HC_FD) {
+                /* the heating/cooling Jacobian leaves entries of cells with a
+                   non-positive species as the storage holds them: zero at
+                   the start, as the reference's InitOdevec leaves its LU */
+#pragma unroll
+                for (int kk = 0; kk < C::NNZ; ++kk)
+                    c.a[kk] = (LUT)0;
+            }
             write_y = false;
             bool skip = !group_any<G>(c.msk);
             if (G == 32) {
@@ -1227,6 +1249,14 @@ constexpr bool hist_fits()
     return Staging<Net, double, 2, BS>::smem_bytes <= 200 * 1024;
 }
 
+/* the history alone within the 227 KB a block may hold (less the soft
+   lockstep words) */
+template <class Net, int BS>
+constexpr bool hist_fits_max()
+{
+    return Staging<Net, double, 2, BS>::smem_bytes <= 226 * 1024;
+}
+
 }  // namespace OV_MODE_NS
 }  // namespace ov
 
@@ -1240,9 +1270,9 @@ constexpr bool hist_fits()
    constant-coefficient CSC variants); 8 = as 6 in soft lockstep; 9, 10 =
    soft lockstep in one block of 256 or 320 with the history in shared
    memory; 11 = soft lockstep in one block of 192 with history and LU in
-   shared memory (where they fit).  With per-cell control stagings 2-11
-   refill idle lanes on every 16th trip, staging 1 on every trip.  Stages
-   2-11 exist for per-cell control (G = 1). */
+   shared memory (where they fit); 12 = as 9 in one block of 384.  With
+   per-cell control stagings 2-12 refill idle lanes on every 16th trip,
+   staging 1 on every trip.  Stages 2-12 exist for per-cell control (G = 1). */
 #define OV_STAGE_CASE(NET, LU, ST)                                                               \
     if (stage == ST)                                                                             \
         return launch<NET, 1, LU, ST>(a, block, grid, s);
@@ -1265,6 +1295,9 @@ constexpr bool hist_fits()
             }                                                                                    \
             if constexpr (hist_fits<NET, 320>()) {                                               \
                 OV_STAGE_CASE(NET, double, 10)                                                   \
+            }                                                                                    \
+            if constexpr (hist_fits_max<NET, 384>()) {                                           \
+                OV_STAGE_CASE(NET, double, 12)                                                   \
             }                                                                                    \
             if constexpr (shm_fits<NET, double, 192>()) {                                        \
                 OV_STAGE_CASE(NET, double, 11)                                                   \
@@ -1290,6 +1323,9 @@ constexpr bool hist_fits()
                 }                                                                                \
                 if constexpr (hist_fits<NET, 320>()) {                                           \
                     OV_STAGE_CASE(NET, float, 10)                                                \
+                }                                                                                \
+                if constexpr (hist_fits_max<NET, 384>()) {                                       \
+                    OV_STAGE_CASE(NET, float, 12)                                                \
                 }                                                                                \
                 if constexpr (shm_fits<NET, float, 192>()) {                                     \
                     OV_STAGE_CASE(NET, float, 11)                                                \

@@ -31,6 +31,7 @@ OV_HD static OV_INLINE void ov_orego_dense_none_rhs(const double* OV_RESTRICT y,
   f[2] = 0.161*y[0] - 0.161*y[2];
 }
 
+/* P at the pattern positions, CSC storage order. */
 OV_HD static OV_INLINE void ov_orego_dense_none_jac(const double* OV_RESTRICT y, const double* OV_RESTRICT k, double beta, double dt, double* OV_RESTRICT a)
 {
   (void)y; (void)k; (void)beta; (void)dt; (void)a;

@@ -15,6 +15,10 @@ struct ov_net_orego_dense_none_lu2 {
   static constexpr bool DENSE = true;
   /* 1: symbolic Jacobian + numeric LU, 2: symbolic LU, 3: difference quotients */
   static constexpr int LU_METHOD = 2;
+  /* the Tgas row is the heating/cooling term (--heatcool=1); HC_FD: GetJac writes
+     its difference quotients and leaves some entries as the storage holds them */
+  static constexpr bool HEATCOOL = false;
+  static constexpr bool HC_FD = false;
   static constexpr const char* TAG = "OREGO_DENSE_NONE_LU2";
   /* dynamic species (solver state index -> species) and frozen ones */
   OV_HD static constexpr int dyn(int i) { return i == 0 ? 0 : (i == 1 ? 1 : (2)); }

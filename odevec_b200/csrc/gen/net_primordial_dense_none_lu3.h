@@ -44,6 +44,7 @@ OV_HD static OV_INLINE void ov_primordial_dense_none_lu3_rhs(const double* OV_RE
   f[15] = 0.0;
 }
 
+/* P at the pattern positions, CSC storage order. */
 OV_HD static OV_INLINE void ov_primordial_dense_none_lu3_jac(const double* OV_RESTRICT y, const double* OV_RESTRICT k, double beta, double dt, double* OV_RESTRICT a)
 {
   (void)y; (void)k; (void)beta; (void)dt; (void)a;

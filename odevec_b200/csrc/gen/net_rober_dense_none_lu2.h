@@ -31,6 +31,7 @@ OV_HD static OV_INLINE void ov_rober_dense_none_lu2_rhs(const double* OV_RESTRIC
   f[2] = 30000000.0*((y[1])*(y[1]));
 }
 
+/* P at the pattern positions, CSC storage order. */
 OV_HD static OV_INLINE void ov_rober_dense_none_lu2_jac(const double* OV_RESTRICT y, const double* OV_RESTRICT k, double beta, double dt, double* OV_RESTRICT a)
 {
   (void)y; (void)k; (void)beta; (void)dt; (void)a;

@@ -15,6 +15,10 @@ struct ov_net_rober_dense_none_lu3 {
   static constexpr bool DENSE = true;
   /* 1: symbolic Jacobian + numeric LU, 2: symbolic LU, 3: difference quotients */
   static constexpr int LU_METHOD = 3;
+  /* the Tgas row is the heating/cooling term (--heatcool=1); HC_FD: GetJac writes
+     its difference quotients and leaves some entries as the storage holds them */
+  static constexpr bool HEATCOOL = false;
+  static constexpr bool HC_FD = false;
   OV_HD static constexpr int pidx(int i, int j) { return j * ND + i; }
   static constexpr const char* TAG = "ROBER_DENSE_NONE_LU3";
   /* dynamic species (solver state index -> species) and frozen ones */

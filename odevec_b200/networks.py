@@ -52,6 +52,20 @@ class Network:
     # that is not a species abundance (temperature, counters)
     masses: Optional[List[float]] = None
     imasses: Optional[List[float]] = None
+    # --heatcool=1: the gas-temperature row (index neq-2, KROME's layout:
+    # chemical species, CR, g, Tgas, dummy) is the heating/cooling term of
+    # this header (ov_hc_heating, ov_hc_cooling, ov_hc_gamma, OV_HC_BOLTZMANN,
+    # OV_HC_NMOLS) instead of the dump's expression
+    heatcool_header: Optional[str] = None
+
+    @property
+    def heatcool(self) -> bool:
+        return self.heatcool_header is not None
+
+    @property
+    def nmols(self) -> int:
+        """chemical species (KROME's nmols): all but CR, g, Tgas and dummy"""
+        return self.neq - 4
 
 
 def state_symbols(neq: int) -> List[sp.Symbol]:
@@ -196,6 +210,27 @@ def load_krome_dump(path: str, name: str = "KROME") -> Network:
         raise ValueError("KROME dump %s: rhs has symbols other than y: %s"
                          % (path, sorted(map(str, free))))
     return Network(name, neq, nrea, y, rhs)
+
+
+def enable_heatcool(net: Network, header: str) -> Network:
+    """Makes the gas temperature (state entry neq-2) follow the heating and
+    cooling functions of `header` (pre_odevec.py:148-190, 556-561).  The rate
+    coefficients of a network with a temperature-dependent rate model are
+    computed once per solve from the initial temperature, so such a network
+    cannot take a temperature equation."""
+    if net.neq < 5:
+        raise SystemExit("# Error: --heatcool=1 needs the KROME species layout (chemical species, CR, g, "
+                         "Tgas, dummy): at least 5 species")
+    if net.rates:
+        raise SystemExit("# Error: --heatcool=1 needs rate coefficients that do not depend on the "
+                         "temperature (a KROME dump); %s computes its rates from Tgas once per solve"
+                         % net.name)
+    if sp.sympify(net.rhs[net.neq - 2]) != 0:
+        raise SystemExit("# Error: --heatcool=1 replaces the Tgas row (species %d), which must be 0 in the "
+                         "network" % (net.neq - 1))
+    net.heatcool_header = header
+    net.idx_tgas = net.neq - 2
+    return net
 
 
 def load(example: str, kromefile: Optional[str] = None) -> Network:

@@ -185,6 +185,14 @@ def build_system(net: networks.Network, ordering: str = "None", packaging: str =
         # the solve applies the permutation to the residual
         raise SystemExit("# Error: --LUmethod=3 needs --ordering=None")
     n = net.neq
+    if net.heatcool:
+        if lu_method == 2:
+            raise SystemExit("# Error: --heatcool=1 with --LUmethod=2: the symbolic factors would "
+                             "ignore the temperature equation; use --LUmethod=1 or 3")
+        if packaging == "DENSE" and lu_method == 1 and ordering not in (None, "None", "NONE", ""):
+            # the difference quotients are written at species positions
+            # (pre_odevec.py:148-170)
+            raise SystemExit("# Error: --heatcool=1 with DENSE packaging needs --ordering=None")
     jac = net.rhs.jacobian(net.y)
     dt, beta = sp.symbols("dt beta")
     P = sp.SparseMatrix(sp.eye(n) - dt * beta * jac)
@@ -201,6 +209,12 @@ def build_system(net: networks.Network, ordering: str = "None", packaging: str =
         for j in range(n):
             P_order[i, j] = P[perm[i], perm[j]]
     pat = _pattern_of(sp.SparseMatrix(P_order))
+    if heatcool_fd(net, packaging, lu_method):
+        # the Tgas row over the chemical species and the whole Tgas column
+        # are difference quotients (ordering None: storage = species order)
+        T = net.neq - 2
+        pat[T, :net.nmols] = True
+        pat[:, T] = True
     lu_exprs = None
     if lu_method == 3:
         # the difference quotients fill every entry: the rate coefficients of
@@ -369,6 +383,8 @@ def emit_c_header(sysm: System) -> str:
     L.append('#include "../ov_common.h"')
     if net.rates:
         L.append('#include "../rates_%s.h"' % net.rates)
+    if net.heatcool:
+        L.append('#include "../%s"' % os.path.basename(net.heatcool_header))
     L.append("")
     L.append("#define OV_%s_NEQ %d" % (cid.upper(), n))
     L.append("#define OV_%s_NNZ %d" % (cid.upper(), nnz))
@@ -397,24 +413,39 @@ def emit_c_header(sysm: System) -> str:
     arr("u_col_start", sysm.u_col_start)
     arr("l_col_start", sysm.l_col_start)
     L.append("")
+    if net.heatcool:
+        L += _hc_function(cid, net)
+        L.append("")
     L.append("OV_HD static OV_INLINE void ov_%s_rhs(const double* OV_RESTRICT y, "
              "const double* OV_RESTRICT k, double* OV_RESTRICT f)" % cid)
     L.append("{")
     L.append("  (void)k;")
     for i in range(n):
-        L.append("  f[%d] = %s;" % (i, _cexpr(net.rhs[i], pr)))
+        if net.heatcool and i == n - 2:
+            L.append("  f[%d] = ov_%s_hc(y, y[%d], y);  /* heating/cooling */" % (i, cid, i))
+        else:
+            L.append("  f[%d] = %s;" % (i, _cexpr(net.rhs[i], pr)))
     L.append("}")
     L.append("")
+    hc_note = (" With heating/cooling difference quotients, entries the reference leaves"
+               " unwritten keep a[]'s content." if heatcool_fd(net, sysm.packaging, sysm.lu_method) else "")
+    L.append("/* P at the pattern positions, CSC storage order.%s */" % hc_note)
     L.append("OV_HD static OV_INLINE void ov_%s_jac(const double* OV_RESTRICT y, "
              "const double* OV_RESTRICT k, double beta, double dt, double* OV_RESTRICT a)" % cid)
     L.append("{")
     L.append("  (void)y; (void)k; (void)beta; (void)dt; (void)a;")
     src = _jac_source(sysm)
-    for j in range(n):
-        for kk in range(sysm.u_col_start[j], sysm.u_col_start[j + 1]):
-            i = sysm.row_index[kk]
-            if src is not None:
-                L.append("  a[%d] = %s;  /* (%d,%d) */" % (kk, _cexpr(src[i, j], pr), i, j))
+    if heatcool_fd(net, sysm.packaging, sysm.lu_method):
+        items = [((sysm.row_index[kk], j), kk) for j in range(n)
+                 for kk in range(sysm.u_col_start[j], sysm.u_col_start[j + 1])]
+        L += _hc_jac_lines(sysm, cid, items, lambda kk, i, j, e: "a[%d] = %s;  /* (%d,%d) */" % (kk, e, i, j),
+                           "  ", lambda i, j: _cexpr(src[i, j], pr))
+    else:
+        for j in range(n):
+            for kk in range(sysm.u_col_start[j], sysm.u_col_start[j + 1]):
+                i = sysm.row_index[kk]
+                if src is not None:
+                    L.append("  a[%d] = %s;  /* (%d,%d) */" % (kk, _cexpr(src[i, j], pr), i, j))
     L.append("}")
     L.append("")
     L.append("#endif")
@@ -520,11 +551,93 @@ def frozen_species(sysm: System) -> List[int]:
 def _frozen_of(net: networks.Network) -> List[int]:
     n = net.neq
     J = net.rhs.jacobian(net.y)
+    # with --heatcool=1 the temperature has a right-hand side that depends on
+    # the chemical species and on itself
+    live = set(range(net.nmols)) | {n - 2} if net.heatcool else set()
     out = []
     for i in range(n):
+        if i in live:
+            continue
         if sp.sympify(net.rhs[i]) == 0 and all(sp.sympify(J[r, i]) == 0 for r in range(n)):
             out.append(i)
     return out
+
+
+def heatcool_fd(net: networks.Network, packaging: str, lu_method: int) -> bool:
+    """whether GetJac writes the heating/cooling difference quotients: DENSE
+    packaging with the symbolic Jacobian (pre_odevec.py:146-170); CSC
+    packaging keeps the symbolic entries, where the Tgas row is that of the
+    network without the heating/cooling term (pre_odevec.py:173-180)"""
+    return net.heatcool and packaging.upper() == "DENSE" and lu_method == 1
+
+
+def _hc_function(cid: str, net: networks.Network) -> List[str]:
+    """the gas-temperature right-hand side (pre_odevec.py:556-558):
+    ((heating - cooling) * (gamma - 1)) / k_B / sum of the chemical species,
+    the sum taken in index order from 0 as gfortran's sum(.., dim=2)"""
+    L = ["/* dTgas/dt: heating/cooling term of the temperature row; yv is the state",
+         "   heating and cooling see, Tgas their temperature, ys the state whose",
+         "   chemical species are summed and whose gamma is taken */",
+         "OV_HD static OV_INLINE double ov_%s_hc(const double* OV_RESTRICT yv, double Tgas, "
+         "const double* OV_RESTRICT ys)" % cid, "{", "  double s = 0.0;"]
+    for j in range(net.nmols):
+        L.append("  s = s + ys[%d];" % j)
+    L.append("  return (ov_hc_heating(yv, Tgas) - ov_hc_cooling(yv, Tgas)) * (ov_hc_gamma(ys) - 1.0) "
+             "/ OV_HC_BOLTZMANN / s;")
+    L.append("}")
+    return L
+
+
+def _hc_jac_lines(sysm: "System", cid: str, pos_items, store, indent: str, symbolic) -> List[str]:
+    """GetJac with the heating/cooling difference quotients
+    (pre_odevec.py:146-170), column by column as the reference writes it:
+    the Tgas row of each chemical species column j is
+    -(beta*dt*(hc(y + dy_j e_j) - hc(y)))/dy_j with dy_j = y_j*1e-2, written
+    only where dy_j > 0 (elsewhere the entry keeps what the matrix storage
+    holds); the Tgas column is -(beta*dt*(f_i(yy)/dy_T)) for every row i, 1
+    added on the diagonal, where yy is the state of the last species column
+    (its species still perturbed) with y_T + dy_T, dy_T = y_T*1e-2 -- f(yy)
+    itself, not f(yy) - f(y).  pos_items: ((i, j), kk) in storage order;
+    store(kk, i, j, expr) -> line or None; symbolic(i, j) -> expr string."""
+    net = sysm.net
+    n, T = net.neq, net.neq - 2
+    L = [indent + "const double hc_dy0 = ov_%s_hc(y, y[%d], y);" % (cid, T),
+         indent + "double hc_yy[%d];" % n]
+    col_T = [(i, kk) for (i, j), kk in pos_items if j == T]
+    done_T = False
+    for (i, j), kk in pos_items:
+        if j == T:
+            if done_T:
+                continue
+            done_T = True
+            L.append(indent + "{ /* Tgas column */")
+            L.append(indent + "  const double dyy = y[%d]*1e-2;" % T)
+            L.append(indent + "  hc_yy[%d] = y[%d] + dyy;" % (T, T))
+            L.append(indent + "  double dy[%d];" % n)
+            L.append(indent + "  ov_%s_rhs(hc_yy, k, dy);" % cid)
+            for r, kr in col_T:
+                v = "-(beta*dt*(dy[%d]/dyy))" % r
+                if r == T:
+                    v = "1.0 + (%s)" % v
+                ln = store(kr, r, T, v)
+                if ln:
+                    L.append(indent + "  " + ln)
+            L.append(indent + "}")
+        elif i == T and j < net.nmols:
+            L.append(indent + "{ /* Tgas row, column %d */" % j)
+            L.append(indent + "  for (int m = 0; m < %d; ++m) hc_yy[m] = y[m];" % n)
+            L.append(indent + "  const double dyy = y[%d]*1e-2;" % j)
+            L.append(indent + "  hc_yy[%d] = y[%d] + dyy;" % (j, j))
+            L.append(indent + "  const double dy1 = ov_%s_hc(hc_yy, y[%d], y);" % (cid, T))
+            ln = store(kk, i, j, "-(beta*dt*(dy1 - hc_dy0)/dyy)")
+            if ln:
+                L.append(indent + "  if (dyy > 0.0) " + ln)
+            L.append(indent + "}")
+        else:
+            ln = store(kk, i, j, symbolic(i, j))
+            if ln:
+                L.append(indent + ln)
+    return L
 
 
 def _reduced(sysm: System):
@@ -594,6 +707,24 @@ def _remap_a(line: str, kmap: Dict[int, int]) -> str:
     return re.sub(r"a\[(\d+)\]", lambda m: "a[%d]" % kmap[int(m.group(1))], line)
 
 
+def _reduce_lines(lines: List[str], kmap: Dict[int, int]) -> List[str]:
+    """The factorisation restricted to the dynamic block: a statement that
+    writes an entry of a frozen species' row (the heating/cooling Tgas column
+    reaches those rows) is left out -- such a row holds the identity's
+    pivot, so nothing it computes reaches a dynamic entry; a statement that
+    writes a dynamic entry must read dynamic entries only."""
+    out = []
+    for ln in lines:
+        idx = [int(v) for v in re.findall(r"a\[(\d+)\]", ln)]
+        if all(i in kmap for i in idx):
+            out.append(_remap_a(ln, kmap))
+        elif idx and idx[0] not in kmap:
+            continue
+        else:
+            raise ValueError("dynamic entry computed from a frozen one: %s" % ln)
+    return out
+
+
 def emit_cuda_header(sysm: System) -> str:
     net = sysm.net
     cid = _cid(sysm.tag)
@@ -632,6 +763,11 @@ def emit_cuda_header(sysm: System) -> str:
     L.append("  static constexpr bool DENSE = %s;" % ("true" if sysm.packaging == "DENSE" else "false"))
     L.append("  /* 1: symbolic Jacobian + numeric LU, 2: symbolic LU, 3: difference quotients */")
     L.append("  static constexpr int LU_METHOD = %d;" % sysm.lu_method)
+    L.append("  /* the Tgas row is the heating/cooling term (--heatcool=1); HC_FD: GetJac writes")
+    L.append("     its difference quotients and leaves some entries as the storage holds them */")
+    L.append("  static constexpr bool HEATCOOL = %s;" % ("true" if net.heatcool else "false"))
+    L.append("  static constexpr bool HC_FD = %s;" % (
+        "true" if heatcool_fd(net, sysm.packaging, sysm.lu_method) else "false"))
     if sysm.lu_method == 3:
         # full pattern, species order: packed index of solver-state entry (i, j)
         for (i, j), kk in pos.items():
@@ -660,9 +796,16 @@ def emit_cuda_header(sysm: System) -> str:
     L.append("  template <class T, class A> OV_HD static OV_INLINE void jac(const double* OV_RESTRICT y, "
              "const double* OV_RESTRICT k, double beta, double dt, A a) {")
     L.append("    (void)y; (void)k; (void)beta; (void)dt; (void)a;")
-    for (i, j), kk in sorted(pos.items(), key=lambda t: t[1]):
-        if kk in kmap and src is not None:
-            L.append("    a[%d] = (T)(%s);" % (kmap[kk], _cexpr(src[i, j], pr)))
+    hcfd = heatcool_fd(net, sysm.packaging, sysm.lu_method)
+    items = sorted(pos.items(), key=lambda t: t[1])
+    if hcfd:
+        L += _hc_jac_lines(sysm, cid, items,
+                           lambda kk, i, j, e: ("a[%d] = (T)(%s);" % (kmap[kk], e)) if kk in kmap else None,
+                           "    ", lambda i, j: _cexpr(src[i, j], pr))
+    else:
+        for (i, j), kk in items:
+            if kk in kmap and src is not None:
+                L.append("    a[%d] = (T)(%s);" % (kmap[kk], _cexpr(src[i, j], pr)))
     L.append("  }")
     L.append("  /* a = D P D^-1 rounded to T, D = diag(sc) over solver-state indices */")
     L.append("  template <class T, class A> OV_HD static OV_INLINE void store_scaled(const double* OV_RESTRICT P, "
@@ -678,14 +821,20 @@ def emit_cuda_header(sysm: System) -> str:
              "const double* OV_RESTRICT k, double beta, double dt, A a, "
              "const double* OV_RESTRICT sc, const double* OV_RESTRICT isc) {")
     L.append("    (void)y; (void)k; (void)beta; (void)dt; (void)a; (void)sc; (void)isc;")
-    for (i, j), kk in sorted(pos.items(), key=lambda t: t[1]):
-        if kk in kmap and src is not None:
-            L.append("    a[%d] = (T)((%s)*sc[%d]*isc[%d]);" % (kmap[kk], _cexpr(src[i, j], pr),
-                                                             dpos[sysm.perm[i]], dpos[sysm.perm[j]]))
+    if hcfd:
+        L += _hc_jac_lines(sysm, cid, items,
+                           lambda kk, i, j, e: ("a[%d] = (T)((%s)*sc[%d]*isc[%d]);" % (
+                               kmap[kk], e, dpos[sysm.perm[i]], dpos[sysm.perm[j]])) if kk in kmap else None,
+                           "    ", lambda i, j: _cexpr(src[i, j], pr))
+    else:
+        for (i, j), kk in items:
+            if kk in kmap and src is not None:
+                L.append("    a[%d] = (T)((%s)*sc[%d]*isc[%d]);" % (kmap[kk], _cexpr(src[i, j], pr),
+                                                                 dpos[sysm.perm[i]], dpos[sysm.perm[j]]))
     L.append("  }")
     L.append("  /* in-place numeric LU of the packed dynamic block a[0..NNZ-1]; A is a")
     L.append("     pointer or an accessor whose operator[] yields T& */")
-    f_lines, s_lines = reciprocal_pivots([_remap_a(l, kmap) for l in _lu_factor_lines(sysm)],
+    f_lines, s_lines = reciprocal_pivots(_reduce_lines(_lu_factor_lines(sysm), kmap),
                                          [_remap_a(l, kmap) for l in _lu_solve_lines(sysm, dpos=dpos)])
     L.append("  template <class T, class A> OV_HD static OV_INLINE void lu_factor(A a) {")
     L.append("    (void)a;")
@@ -812,7 +961,11 @@ def parse_args(argv=None):
     p.add_argument("--dt_min", default=1e-10, help="default minimal time step")
     p.add_argument("--nvector", type=int, required=True,
                    help="default lockstep group size (1 = per-cell control, 32 = one warp)")
-    p.add_argument("--heatcool", type=int, default=0)
+    p.add_argument("--heatcool", type=int, default=0,
+                   help="1: the Tgas row (species neq-1 of a KROME layout) follows heating and cooling")
+    p.add_argument("--heatcool_header", default=None,
+                   help="header in odevec_b200/csrc defining ov_hc_heating, ov_hc_cooling, ov_hc_gamma, "
+                        "OV_HC_BOLTZMANN and OV_HC_NMOLS for --heatcool=1")
     p.add_argument("--equilibrium_H", type=int, default=0)
     p.add_argument("--ordering", default="None", help="CMK | INVERT | FF | None")
     p.add_argument("--packaging", default="DENSE", help="DENSE | CSC")
@@ -827,9 +980,9 @@ def main(argv=None) -> System:
     args = parse_args(argv)
     if args.krome_setupfile is not None:
         args.example = "KROME"
-    if args.heatcool:
-        raise SystemExit("# Error: --heatcool=1 needs KROME's heating/cooling functions, "
-                         "which this build does not provide")
+    if args.heatcool and not args.heatcool_header:
+        raise SystemExit("# Error: --heatcool=1 needs --heatcool_header=<file> with the heating and "
+                         "cooling functions (KROME's heating/cooling are not part of this build)")
     if args.equilibrium_H == 1 and args.packaging != "DENSE":   # pre_odevec.py:455-460
         raise SystemExit("args.equilibrium_H is only allowed with DENSE packaging.")
     if args.equilibrium_H == 1 and args.ordering != "None":
@@ -841,6 +994,11 @@ def main(argv=None) -> System:
     net = networks.load(args.example, args.krome_setupfile)
     if args.name:
         net.name = args.name
+    if args.heatcool:
+        hdr = os.path.join(os.path.dirname(GEN_DIR), os.path.basename(args.heatcool_header))
+        if not os.path.exists(hdr):
+            raise SystemExit("# Error: heating/cooling header %s not found (it must be in odevec_b200/csrc)" % hdr)
+        networks.enable_heatcool(net, hdr)
     sysm = build_system(net, args.ordering, args.packaging, args.lu_pattern, args.nvector,
                         float(args.dt_min), args.LUmethod)
     n = net.neq

@@ -289,6 +289,63 @@ def make_stream(seed: int = 5, rate: float = 200.0, duration: float = 1.0,
     return out
 
 
+def measure(rate: float = 200.0, duration: float = 0.25, steps: int = 50, cells=(1000, 262144),
+            dt_hydro=(1e6, 1e11), networks=("ROBER_DENSE_NONE", "PRIMORDIAL_CSC_FF", "SYN64_CSC_CMK"),
+            precisions=("fp32_lu", "fp64"), budget: float = 120e9, slots: int = 16, seed: int = 5,
+            isolated: bool = False, fair_share: bool = True) -> List[dict]:
+    """Runs a Poisson request stream through the scheduler on the GPU, per
+    precision form; with isolated, every request is run again alone and the
+    mix's step latencies are compared with the isolated ones."""
+    reqs = make_stream(seed, rate, duration, tuple(networks), tuple(cells), tuple(dt_hydro), steps)
+    outs = []
+    for prec in precisions:
+        be = GpuBackend(prec, fair_share=fair_share)
+        # warm-up: one small request per network (module load, first launches)
+        warm = [Request(10**6 + i, r.network, r.y0[:, :64].copy(), r.dt_hydro, 1, 0.0, r.rtol, r.atol,
+                        r.dt_min, r.dt_in) for i, r in enumerate({r.network: r for r in reqs}.values())]
+        Scheduler(be, budget, slots).run(warm, realtime=False)
+        recs, res = Scheduler(be, budget, slots).run(reqs, realtime=True)
+        mix = summarize(recs, res)
+        offered = sum(r.ncells * r.steps for r in reqs) / duration
+        out = {"form": prec, "requests": len(reqs), "rate": rate, "steps": steps,
+               "cells": list(cells), "dt_hydro": list(dt_hydro), "seed": seed,
+               "budget_gb": budget / 1e9, "slots": slots, "fair_share": fair_share,
+               "mix": mix,
+               # offered load: cell-steps asked for per second of arrivals, against
+               # the cell-steps per second the device delivered in the mix
+               "offered_cell_steps_per_s": offered, "load_factor": offered / mix["cells_per_s"]}
+        by_net = {}
+        for r in recs:
+            by_net.setdefault(r.network, []).append(r)
+        out["per_network"] = {k: summarize(v, res) for k, v in by_net.items()}
+        if isolated:
+            iso = {}
+            iso_res = {}
+            for r in reqs:
+                rr, rs = Scheduler(be, budget, 1).run([dataclasses.replace(r, arrival=0.0)], realtime=False)
+                iso_res.update(rs)
+                for x in rr:
+                    iso[(x.rid, x.step)] = x.latency
+            ratio = np.array([x.latency / iso[(x.rid, x.step)] for x in recs])
+            iso_l = np.array(list(iso.values()))
+            sratio = np.array([x.service / iso[(x.rid, x.step)] for x in recs])
+            lat_mix = np.array([x.latency for x in recs])
+            # each request's result alone and in the mix
+            same = all(np.array_equal(res[k].y, iso_res[k].y, equal_nan=True) and
+                       np.array_equal(res[k].status, iso_res[k].status) for k in res)
+            out["isolated"] = {"p50_ms": 1e3 * float(np.percentile(iso_l, 50)),
+                               "p99_ms": 1e3 * float(np.percentile(iso_l, 99)),
+                               "mix_over_isolated_p50": float(np.percentile(ratio, 50)),
+                               "mix_over_isolated_p99": float(np.percentile(ratio, 99)),
+                               "mix_p99_over_isolated_p99": float(np.percentile(lat_mix, 99)
+                                                                  / np.percentile(iso_l, 99)),
+                               "service_over_isolated_p50": float(np.percentile(sratio, 50)),
+                               "service_over_isolated_p99": float(np.percentile(sratio, 99)),
+                               "results_same_alone_and_in_mix": bool(same)}
+        outs.append(out)
+    return outs
+
+
 def main(argv=None):
     """Serving measurement: python -m odevec_b200.serving [options]; prints one
     JSON line per precision form."""
@@ -311,46 +368,9 @@ def main(argv=None):
     p.add_argument("--no-fair-share", action="store_true",
                    help="every launch may take the whole device (no 1/k block share, one stream priority)")
     a = p.parse_args(argv)
-    reqs = make_stream(a.seed, a.rate, a.duration, tuple(a.networks.split(",")), (a.min_cells, a.max_cells),
-                       (a.dt_min, a.dt_max), a.steps)
-    for prec in a.precisions.split(","):
-        be = GpuBackend(prec, fair_share=not a.no_fair_share)
-        # warm-up: one small request per network (module load, first launches)
-        warm = [Request(10**6 + i, r.network, r.y0[:, :64].copy(), r.dt_hydro, 1, 0.0, r.rtol, r.atol,
-                        r.dt_min, r.dt_in) for i, r in enumerate({r.network: r for r in reqs}.values())]
-        Scheduler(be, a.budget, a.slots).run(warm, realtime=False)
-        recs, res = Scheduler(be, a.budget, a.slots).run(reqs, realtime=True)
-        mix = summarize(recs, res)
-        offered = sum(r.ncells * r.steps for r in reqs) / a.duration
-        out = {"form": prec, "requests": len(reqs), "rate": a.rate, "steps": a.steps,
-               "cells": [a.min_cells, a.max_cells], "dt_hydro": [a.dt_min, a.dt_max],
-               "budget_gb": a.budget / 1e9, "slots": a.slots, "fair_share": not a.no_fair_share,
-               "mix": mix,
-               # offered load: cell-steps asked for per second of arrivals, against
-               # the cell-steps per second the device delivered in the mix
-               "offered_cell_steps_per_s": offered, "load_factor": offered / mix["cells_per_s"]}
-        by_net = {}
-        for r in recs:
-            by_net.setdefault(r.network, []).append(r)
-        out["per_network"] = {k: summarize(v, res) for k, v in by_net.items()}
-        if a.isolated:
-            iso = {}
-            for r in reqs:
-                rr, _ = Scheduler(be, a.budget, 1).run([dataclasses.replace(r, arrival=0.0)], realtime=False)
-                for x in rr:
-                    iso[(x.rid, x.step)] = x.latency
-            ratio = np.array([x.latency / iso[(x.rid, x.step)] for x in recs])
-            iso_l = np.array(list(iso.values()))
-            sratio = np.array([x.service / iso[(x.rid, x.step)] for x in recs])
-            lat_mix = np.array([x.latency for x in recs])
-            out["isolated"] = {"p50_ms": 1e3 * float(np.percentile(iso_l, 50)),
-                               "p99_ms": 1e3 * float(np.percentile(iso_l, 99)),
-                               "mix_over_isolated_p50": float(np.percentile(ratio, 50)),
-                               "mix_over_isolated_p99": float(np.percentile(ratio, 99)),
-                               "mix_p99_over_isolated_p99": float(np.percentile(lat_mix, 99)
-                                                                  / np.percentile(iso_l, 99)),
-                               "service_over_isolated_p50": float(np.percentile(sratio, 50)),
-                               "service_over_isolated_p99": float(np.percentile(sratio, 99))}
+    for out in measure(a.rate, a.duration, a.steps, (a.min_cells, a.max_cells), (a.dt_min, a.dt_max),
+                       a.networks.split(","), a.precisions.split(","), a.budget, a.slots, a.seed,
+                       a.isolated, not a.no_fair_share):
         print(json.dumps(out), flush=True)
 
 

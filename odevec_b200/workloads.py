@@ -18,6 +18,8 @@ with the shapes, sizes and value distributions of the configurations below.
                driver (tests/primordial.f90:73).
 * SYN64      - abundances log-uniform 1e-20..1; t_end 1e10 s; rtol 1e-5,
                atol 1e-25.
+* HCTOY      - the heating/cooling test network: n_H 1..1e4, Tgas
+               100..1e4 K, t_end 1e8..1e11 s; rtol 1e-6, atol 1e-20.
 """
 from __future__ import annotations
 
@@ -113,4 +115,24 @@ def syn64(ncells: int = 262144, seed: int = 4, network: str = "SYN64_CSC_CMK") -
                     np.full(ncells, 1e10), 1e-5, 1e-25, 1e-20, 1, seed)
 
 
-BUILDERS = {"ROBER": rober, "OREGO": orego, "PRIMORDIAL": primordial, "SYN64": syn64}
+def hctoy(ncells: int = 65536, seed: int = 6, network: str = "HCTOY_DENSE_NONE") -> Workload:
+    """The heating/cooling test network (E, H+, H, H2, HE, CR, g, Tgas,
+    dummy): log-uniform n_H 1..1e4 cm^-3, ionisation fraction 1e-4..1e-1, H2
+    fraction 1e-6..1e-1, He/H 0.08, Tgas 100..1e4 K, t_end log-uniform
+    1e8..1e11 s; rtol 1e-6, atol 1e-20."""
+    rng = np.random.default_rng(seed)
+    lu = lambda lo, hi: 10.0 ** rng.uniform(np.log10(lo), np.log10(hi), ncells)
+    nH = lu(1.0, 1e4)
+    y = np.zeros((9, ncells))
+    y[1] = lu(1e-4, 1e-1) * nH
+    y[0] = y[1]
+    y[3] = lu(1e-6, 1e-1) * nH
+    y[2] = nH - y[1] - 2.0 * y[3]
+    y[4] = 0.08 * nH
+    y[7] = lu(100.0, 1e4)
+    t_stop = lu(1e8, 1e11)
+    return Workload("HCTOY", network, y, np.zeros(ncells), np.full(ncells, 1e-10), t_stop,
+                    1e-6, 1e-20, 1e-20, 1, seed)
+
+
+BUILDERS = {"ROBER": rober, "OREGO": orego, "PRIMORDIAL": primordial, "SYN64": syn64, "HCTOY": hctoy}

@@ -14,10 +14,42 @@ LIB = os.path.join(HERE, "libodevec_oracle.so")
 LIB_LIBM = os.path.join(HERE, "libodevec_oracle_libm.so")
 
 
-def build(force: bool = False, verbose: bool = False, libm: bool = False) -> str:
+def cpu_model() -> str:
+    try:
+        for line in open("/proc/cpuinfo"):
+            if line.startswith("model name"):
+                return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
+
+
+def _cpu_tag() -> str:
+    """identifies the host CPU (model and instruction-set flags) so that a
+    -march=native build is never loaded on another kind of CPU"""
+    import hashlib
+    flags = ""
+    try:
+        for line in open("/proc/cpuinfo"):
+            if line.startswith("flags"):
+                flags = line
+                break
+    except OSError:
+        pass
+    return hashlib.sha1((cpu_model() + flags).encode()).hexdigest()[:10]
+
+
+def fast_lib_path() -> str:
+    return os.path.join(HERE, "libodevec_oracle_fast_%s.so" % _cpu_tag())
+
+
+def build(force: bool = False, verbose: bool = False, libm: bool = False, fast: bool = False) -> str:
     """libm: the variant whose exp/log/log10/pow are the C library's (-DOV_LIBM),
-    compared bit for bit with runs of the reference's own solver module."""
-    lib = LIB_LIBM if libm else LIB
+    compared bit for bit with runs of the reference's own solver module.
+    fast: the CPU baseline's build, -O3 -march=native with floating-point
+    contraction allowed (not bit-identical to the GPU kernels); built on the
+    host that loads it."""
+    lib = LIB_LIBM if libm else (fast_lib_path() if fast else LIB)
     deps = [SRC, os.path.join(HERE, "..", "include", "odevec_b200.h")]
     gen = os.path.join(HERE, "..", "odevec_b200", "csrc")
     for root, _, files in os.walk(gen):
@@ -25,7 +57,8 @@ def build(force: bool = False, verbose: bool = False, libm: bool = False) -> str
     if (not force and os.path.exists(lib)
             and os.path.getmtime(lib) >= max(os.path.getmtime(d) for d in deps)):
         return lib
-    cmd = ["gcc", "-std=gnu11", "-O2", "-ffp-contract=off", "-fno-fast-math", "-fPIC", "-shared",
+    opt = ["-O3", "-march=native", "-ffp-contract=fast"] if fast else ["-O2", "-ffp-contract=off"]
+    cmd = ["gcc", "-std=gnu11"] + opt + ["-fno-fast-math", "-fPIC", "-shared",
            "-fopenmp", "-Wall", "-Wno-unused-function", "-Wno-unused-variable", "-o", lib + ".tmp",
            SRC, "-lm"] + (["-DOV_LIBM"] if libm else [])
     if verbose:

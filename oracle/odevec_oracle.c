@@ -171,6 +171,14 @@ static void get_jac(ode_t* o, double beta, const double* y, double dt)
             yc[j] = y[j * G + i];
         if (nr)
             ov_rates_primordial_k(yc, n, o->rT + (size_t)i * nr, kc);
+        if (o->net->dense) {
+            /* entries the generated routine leaves unwritten (the heating/
+               cooling difference quotients of a species <= 0) keep what the
+               matrix holds, as the reference's GetJac writes into this%LU */
+            for (int c = 0; c < n; ++c)
+                for (int kk = o->net->u_col_start[c]; kk < o->net->u_col_start[c + 1]; ++kk)
+                    a[kk] = o->LU[((size_t)o->net->row_index[kk] * n + c) * G + i];
+        }
         o->net->jac(yc, kc, beta, dt, a);
         if (o->net->dense) {
             for (int r = 0; r < n; ++r)

@@ -14,12 +14,14 @@ OV_NSTATS = 8
 _libs = {}
 
 
-def lib(libm: bool = False):
+def lib(libm: bool = False, fast: bool = False):
     """The oracle library; libm=True: the variant calling the C library's
     exp/log/log10/pow (as the reference's Fortran does) instead of the
-    library's own, for bit-for-bit comparison with the reference's solver."""
-    if libm not in _libs:
-        path = _build.build(libm=libm)
+    library's own, for bit-for-bit comparison with the reference's solver;
+    fast=True: the -O3 -march=native build timed as the CPU baseline."""
+    key = (libm, fast)
+    if key not in _libs:
+        path = _build.build(libm=libm, fast=fast)
         L = ctypes.CDLL(path)
         d, i64, i32 = ctypes.c_double, ctypes.c_int64, ctypes.c_int
         P = ctypes.c_void_p
@@ -43,8 +45,8 @@ def lib(libm: bool = False):
             getattr(L, f).restype = d
         L.ov_oracle_convert.argtypes = [ctypes.c_char_p, i64, i32, P, P, P]
         L.ov_oracle_convert.restype = i32
-        _libs[libm] = L
-    return _libs[libm]
+        _libs[key] = L
+    return _libs[key]
 
 
 def _p(a):
@@ -74,13 +76,14 @@ def tags():
 
 def solve(tag, y, t, dt, t_stop, rtol, atol, dt_min, group=1, check_negatives=False,
           mask=None, max_attempts=1000000, nthreads=0, fix_restart=False, ws=None, resume=False,
-          libm=False):
+          libm=False, fast=False):
     """SolveODE on all cells.  y: (neq, ncells) float64, modified copy returned
     with t, dt, status, stats.  ws: a workspace from workspace() to save the
     integrator state into (and, with resume, to continue from); resume
     "en_old" (or 2): a fresh start keeping the previous call's last Newton
     correction from ws, as the reference's solver object does.  libm: the
-    oracle variant with the C library's exp/log/log10/pow."""
+    oracle variant with the C library's exp/log/log10/pow; fast: the -O3
+    -march=native build (CPU baseline timing only)."""
     y = np.ascontiguousarray(y, dtype=np.float64).copy()
     ncells = y.shape[1]
     t = np.ascontiguousarray(np.broadcast_to(t, (ncells,)), dtype=np.float64).copy()
@@ -89,7 +92,7 @@ def solve(tag, y, t, dt, t_stop, rtol, atol, dt_min, group=1, check_negatives=Fa
     m = None if mask is None else np.ascontiguousarray(mask, dtype=np.uint8)
     status = np.zeros(ncells, np.int32)
     stats = np.zeros((ncells, OV_NSTATS), np.int32)
-    rc = lib(libm).ov_oracle_solve(tag.encode(), ncells, group, rtol, atol, dt_min,
+    rc = lib(libm, fast).ov_oracle_solve(tag.encode(), ncells, group, rtol, atol, dt_min,
                                int(bool(check_negatives)), int(bool(fix_restart)), max_attempts,
                                _p(y), _p(t), _p(dt),
                                _p(t_stop), _p(m), _p(status), _p(stats), nthreads, _p(ws),

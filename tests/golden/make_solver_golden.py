@@ -37,6 +37,7 @@ source.  Usage: ``python tests/golden/make_solver_golden.py [REF] [case ...]``.
 """
 import json
 import os
+import re
 import shutil
 import subprocess
 import sys
@@ -149,18 +150,93 @@ def primordial_bench_cells(n, seed):
 
 # --------------------------------------------------------------------- driver
 class Case:
-    def __init__(self, name, tag, ex, pack, order, lum, nvector, runs, defines=(), check_neg=False):
+    def __init__(self, name, tag, ex, pack, order, lum, nvector, runs, defines=(), check_neg=False,
+                 krome=None):
         self.name, self.tag, self.ex, self.pack, self.order = name, tag, ex, pack, order
         self.lum, self.nvector, self.runs, self.defines = lum, nvector, runs, defines
         self.check_neg = check_neg
+        self.krome = krome      # KROME dump for --heatcool=1 cases
+
+
+# heating and cooling of the HCTOY test network as Fortran functions with
+# KROME's interfaces (heating(n, Tgas, k, nH2dust), cooling(n, Tgas)); the
+# same laws, in the same operation order, as odevec_b200/csrc/heatcool_hctoy.h
+HCTOY_FORTRAN = """
+module hctoy_heatcool
+contains
+  function heating(y, Tgas, k, nh2dust)
+    implicit none
+    double precision, dimension(:,:) :: y, k
+    double precision, dimension(:) :: Tgas, nh2dust
+    double precision, dimension(size(y,1)) :: heating
+    heating = 1.0d-25*(y(:,3) + y(:,4) + y(:,5))
+  end function heating
+  function cooling(y, Tgas)
+    implicit none
+    double precision, dimension(:,:) :: y
+    double precision, dimension(:) :: Tgas
+    double precision, dimension(size(y,1)) :: cooling
+    cooling = 1.0d-23*y(:,1)*y(:,2)*sqrt(Tgas) + 2.0d-24*y(:,4)*Tgas
+  end function cooling
+end module hctoy_heatcool
+"""
+
+
+def krome_shim(commons, neq):
+    """The reference's --heatcool=1 output is a fragment for KROME's build
+    (pre_odevec.py:148-190, 556-561): it calls KROME's heating/cooling and
+    uses krome_gamma, boltzmann_erg, nmols, Tgas, nH2dust, yy, dyy, dy, dy0,
+    dy1 without declaring them, leaves #KROME_ placeholders for KROME's
+    preprocessor, and its template has no #ODEVEC_DY0 line to compute dy0.
+    This supplies that context the way KROME does and changes nothing the
+    reference wrote: the placeholders are dropped (no quench, no floor);
+    krome_gamma -> 5/3, boltzmann_erg -> 1.380648d-16, nmols -> neq-4;
+    Tgas = y(:,neq-1) and nH2dust = 0 at the entry of GetRHS and GetJac; the
+    scratch arrays are declared in GetJac, and dy0 = the heating/cooling term
+    of y (the reference's own Tgas right-hand side) before the Jacobian."""
+    c = commons.replace("#KROME_coolingQuench #KROME_coolfloor", "")
+    c = c.replace("krome_gamma(:)", "(5d0/3d0)").replace("boltzmann_erg", "1.380648d-16")
+    c = c.replace("y(:,1:nmols)", "y(:,1:%d)" % (neq - 4))
+    # the generated Tgas right-hand side, joined, as the dy0 statement
+    joined = re.sub(r"&\s*\n\s*", "", c)
+    m = re.search(r"rhs\(:,%d\) = (.*)\n" % (neq - 1), joined)
+    dy0 = "      dy0(:) = " + m.group(1).strip() + "\n"
+    out = []
+    sub = None
+    for line in c.split("\n"):
+        ms = re.match(r"\s*subroutine\s+(\w+)", line, re.I)
+        if ms:
+            sub = ms.group(1).lower()
+        st = line.strip().lower()
+        if sub in ("getrhs", "getjac") and st == "#ifdef have_coefficients":
+            out.append("    double precision, dimension(this%nvector) :: Tgas, nH2dust")
+            if sub == "getjac":
+                out.append("    double precision, dimension(this%nvector) :: dyy, dy0, dy1")
+                out.append("    double precision, dimension(this%nvector,this%neq) :: yy, dy")
+        out.append(line)
+        if sub in ("getrhs", "getjac") and st == "#endif":
+            out.append("      Tgas(:) = y(:,%d)" % (neq - 1))
+            out.append("      nH2dust(:) = 0d0")
+            if sub == "getjac":
+                out.append(dy0.rstrip("\n"))
+            sub = None
+    return "\n".join(out)
 
 
 def translate_case(work, case):
-    cmd = [sys.executable, "pre_odevec.py", "--nvector=%d" % case.nvector, "--example=%s" % case.ex,
-           "--packaging=%s" % case.pack, "--ordering=%s" % case.order, "--LUmethod=%d" % case.lum]
+    if case.krome:
+        cmd = [sys.executable, "pre_odevec.py", "--nvector=%d" % case.nvector,
+               "--krome_setupfile=%s" % case.krome, "--heatcool=1",
+               "--packaging=%s" % case.pack, "--ordering=%s" % case.order, "--LUmethod=%d" % case.lum]
+    else:
+        cmd = [sys.executable, "pre_odevec.py", "--nvector=%d" % case.nvector, "--example=%s" % case.ex,
+               "--packaging=%s" % case.pack, "--ordering=%s" % case.order, "--LUmethod=%d" % case.lum]
     subprocess.run(cmd, cwd=work, capture_output=True, text=True, check=True)
     b = os.path.join(work, "build")
     srcs = [open(os.path.join(b, "odevec.f90")).read(), open(os.path.join(b, "odevec_commons.f90")).read()]
+    if case.krome:
+        neq = int(re.search(r"integer :: neq=(\d+)", srcs[0]).group(1))
+        srcs = [srcs[0], HCTOY_FORTRAN, krome_shim(srcs[1], neq)]
     _, ns = F.translate(srcs, defines=case.defines, probes=PROBES)
     return ns
 
@@ -300,6 +376,16 @@ def cases():
                   bench[2:4], defines=("HAVE_COEFFICIENTS",)))
     C.append(Case("primordial_lu3", "PRIMORDIAL_DENSE_NONE_LU3", "PRIMORDIAL", "DENSE", "None", 3, 1,
                   bench[4:6], defines=("HAVE_COEFFICIENTS",)))
+    # --heatcool=1: the heating/cooling test network's cells, single solves
+    # and a ladder of hydro steps with dt carried
+    from odevec_b200 import workloads as W
+    wl = W.hctoy(ncells=6, seed=41)
+    hc = [{"y0": wl.y[:, i:i + 1], "t0": 0.0, "dt0": wl.dt0[i], "t_stops": [wl.t_stop[i]], "dt_reset": None,
+           "rtol": wl.rtol, "atol": wl.atol, "dt_min": wl.dt_min} for i in range(4)]
+    hc.append({"y0": wl.y[:, 4:5], "t0": 0.0, "dt0": 1e-10, "t_stops": [np.float64(1e9) * (k + 1) for k in range(20)],
+               "dt_reset": None, "rtol": wl.rtol, "atol": wl.atol, "dt_min": wl.dt_min})
+    dump = os.path.join(os.path.dirname(os.path.dirname(HERE)), "odevec_b200", "data", "hctoy_krome.py")
+    C.append(Case("hctoy_heatcool", "HCTOY_DENSE_NONE", "KROME", "DENSE", "None", 1, 1, hc, krome=dump))
     return C
 
 

@@ -75,6 +75,8 @@ CASES = [
     ("ROBER", dict(ncells=256), "ROBER_DENSE_NONE_LU3", 32),
     ("ROBER", dict(ncells=256), "ROBER_DENSE_NONE_LU3", 1),
     ("PRIMORDIAL", dict(ncells=256), "PRIMORDIAL_DENSE_NONE_LU3", 1),
+    # --heatcool=1: the heating/cooling temperature row and its difference quotients
+    ("HCTOY", dict(ncells=512), "HCTOY_DENSE_NONE", 1),
 ]
 
 
@@ -123,15 +125,16 @@ def _relerr(a, b, floor):
 @pytest.mark.parametrize("precision", ["fp64_fma", "fp32_lu"])
 def test_fast_forms_within_tolerance(gpu_lib, oracle, precision):
     # FMA changes roundings and FP32-LU the Newton iterates, so step
-    # sequences differ; both must stay within 100*rtol of the exact form for
-    # species above 1e-12 of the cell's hydrogen density
+    # sequences differ; both must stay within 10*rtol of the exact FP64 form
+    # at the same tolerance (the FP32 factors' share is measured at about
+    # 0.1*rtol), for species above 1e-12 of the cell's largest abundance
     wl = W.primordial(ncells=1024)
     g = run_gpu(gpu_lib, wl, precision)
     o = run_oracle(oracle, wl)
     assert np.all(g[3] == 0)
     floor = 1e-12 * np.max(wl.y[:12], axis=0)
     err = np.max([_relerr(g[0][s], o[0][s], floor) for s in range(12)])
-    assert err < 100 * wl.rtol, err
+    assert err < 10 * wl.rtol, err
 
 
 def test_mask_semantics(gpu_lib, oracle):

@@ -141,6 +141,8 @@ def test_cli_writes_variant(tmp_path):
     (["--packaging=CSR"], "CSR packaging is not supported"),
     (["--packaging=XYZ"], "This format is not known"),
     (["--heatcool=1"], "heating/cooling"),
+    (["--heatcool=1", "--heatcool_header=heatcool_hctoy.h"], "KROME species layout"),
+    (["--heatcool=1", "--heatcool_header=no_such_header.h"], "not found"),
     (["--LUmethod=2", "--packaging=CSC"], "LUmethod=2 needs --packaging=DENSE"),
     (["--LUmethod=3", "--packaging=CSC"], "not supported with sparse matrices"),
     (["--LUmethod=3", "--ordering=CMK"], "LUmethod=3 needs --ordering=None"),
@@ -235,3 +237,31 @@ def test_cuda_header_divides_only_through_pivot_helpers(example, order, pack, lu
     body = text[text.index("void lu_factor("):]
     assert "ov_pivot<T>(" in body and "ov_divp<T>(" in body
     assert not re.search(r"/ a\[\d+\]", body)
+
+
+def test_heatcool_structure():
+    """--heatcool=1 (pre_odevec.py:146-190): the Tgas row becomes the
+    heating/cooling term, GetJac fills the Tgas row over the chemical species
+    and the whole Tgas column with difference quotients (DENSE), the
+    temperature and every chemical species stay in the solver state, and a
+    network whose rates depend on the temperature is refused."""
+    hdr = os.path.join(os.path.dirname(HERE), "odevec_b200", "csrc", "heatcool_hctoy.h")
+    dump = os.path.join(os.path.dirname(HERE), "odevec_b200", "data", "hctoy_krome.py")
+    net = networks.enable_heatcool(networks.load_krome_dump(dump, "HCTOY"), hdr)
+    s = pre_odevec.build_system(net, "None", "DENSE")
+    T = net.neq - 2
+    assert net.idx_tgas == T and net.nmols == 5
+    assert all(s.lu_pat[T, j] for j in range(net.nmols)) and all(s.lu_pat[:, T])
+    assert pre_odevec.frozen_species(s) == [5, 6, 8]
+    h = pre_odevec.emit_c_header(s)
+    assert "f[7] = ov_hctoy_dense_none_hc(y, y[7], y);" in h
+    assert h.count("if (dyy > 0.0)") == net.nmols and "ov_hctoy_dense_none_rhs(hc_yy, k, dy);" in h
+    cu = pre_odevec.emit_cuda_header(s)
+    assert "static constexpr bool HC_FD = true;" in cu
+    # CSC packaging keeps the symbolic P (pre_odevec.py:173-180): no difference quotients
+    c = pre_odevec.emit_c_header(pre_odevec.build_system(net, "CMK", "CSC"))
+    assert "dyy" not in c and "ov_hctoy_csc_cmk_hc(y, y[7], y)" in c
+    with pytest.raises(SystemExit, match="ordering=None"):
+        pre_odevec.build_system(net, "CMK", "DENSE")
+    with pytest.raises(SystemExit, match="temperature"):
+        networks.enable_heatcool(networks.load("PRIMORDIAL"), hdr)

@@ -130,7 +130,7 @@ def test_fixture_coverage():
     tags = {c["tag"] for c in CASES.values()}
     for tag in ("ROBER_DENSE_NONE", "ROBER_CSC_NONE", "ROBER_DENSE_NONE_LU2", "ROBER_DENSE_NONE_LU3",
                 "OREGO_DENSE_NONE", "OREGO_CSC_CMK", "OREGO_DENSE_NONE_LU2", "PRIMORDIAL_CSC_FF",
-                "PRIMORDIAL_CSC_CMK", "PRIMORDIAL_DENSE_NONE", "PRIMORDIAL_DENSE_NONE_LU3"):
+                "PRIMORDIAL_CSC_CMK", "PRIMORDIAL_DENSE_NONE", "PRIMORDIAL_DENSE_NONE_LU3", "HCTOY_DENSE_NONE"):
         assert tag in tags, tag
     assert any(c["check_negatives"] for c in CASES.values())
     assert any("mask" in call for c in CASES.values() for r in c["runs"] for call in r["calls"])
