@@ -197,6 +197,34 @@ int32_t odevec_close(odevec_solver* s);
 /* message of the last failed call on this thread */
 const char* odevec_last_error(void);
 
+/* Several solves of different network variants in one kernel launch; no
+   counterpart in the reference, which integrates one network per SolveODE.
+   Each job is one odevec_solve_resident call (workspace and resume as
+   there; workspace may be null with resume = 0): its own solver (distinct
+   across jobs), cells and arrays.  All jobs must use the same precision
+   form and per-cell control (group_size 1); the launch uses one compiled
+   multi-network kernel whose set of variants holds every job's network
+   (OV_API_EUNSUPPORTED if none does).  The kernel gives each job a share of
+   the blocks in proportion to its cells, and a block whose job has no cells
+   left takes cells of the others, so the networks share the device for the
+   whole launch.  Failed FP32-LU cells are not solved again (see
+   no_escalation).  Asynchronous on stream. */
+#define OV_MULTI_MAX_JOBS 8
+typedef struct odevec_job {
+    odevec_solver* solver;
+    int64_t ncells;
+    double* y;
+    double* t;
+    double* dt;
+    const double* t_stop;
+    const uint8_t* mask;
+    int32_t* status;
+    int32_t* stats;
+    double* workspace;
+    int32_t resume;
+} odevec_job;
+int32_t odevec_solve_many(const odevec_job* jobs, int32_t njobs, void* stream);
+
 /* SolveODE on device arrays without allocating anything.  No counterpart in
    the reference.  For callers that cannot call cudaMalloc -- a host code
    that passes its own device arrays from a region where device allocation

@@ -44,6 +44,29 @@ def variants():
 
 PREC_CODE = {"fp64": 0, "fp64_fma": 1, "fp32_lu": 2}
 
+# variant sets compiled into one multi-network kernel each (odevec_solve_many):
+# the serving mix of ROBER, PRIMORDIAL and the 64-species network
+MULTI_SETS = [("serving", ["rober_dense_none", "primordial_csc_ff", "syn64_csc_cmk"])]
+
+
+def multi_sets():
+    have = {cid for cid, _ in variants()}
+    tags = dict(variants())
+    return [(sid, cids, [tags[c] for c in cids]) for sid, cids in MULTI_SETS if all(c in have for c in cids)]
+
+
+def write_multi_registry() -> str:
+    """gen/multi.inc: OV_MULTI(sid, "TAG", ...) per compiled set"""
+    lines = ["/* Generated by odevec_b200/build.py: the multi-network kernel sets. */"]
+    for sid, _, tags in multi_sets():
+        lines.append("OV_MULTI(%s, %s)" % (sid, ", ".join('"%s"' % t for t in tags)))
+    path = os.path.join(GEN, "multi.inc")
+    text = "\n".join(lines) + "\n"
+    if not os.path.exists(path) or open(path).read() != text:
+        with open(path, "w") as fh:
+            fh.write(text)
+    return path
+
 
 def write_tuning_table() -> str:
     """gen/tuning.inc: the autotuner's table (odevec_b200/tuning.json) as C,
@@ -123,6 +146,24 @@ def build(force: bool = False, jobs: int = 0, verbose: bool = False) -> str:
             objs.append(obj)
             if force or not os.path.exists(obj) or not os.path.exists(stamp) or open(stamp).read() != key:
                 tasks.append((src, obj, flags, obj + ".log", stamp, key))
+    for sid, cids, _ in multi_sets():
+        for mode, flags in MODES.items():
+            src = os.path.join(BUILD, "multi_%s_%s.cu" % (sid, mode))
+            text = ("/* generated by odevec_b200/build.py */\n#define OV_MODE_NS %s\n"
+                    '#include "bdf_kernel.cuh"\n' % mode
+                    + "".join('#include "gen/net_%s.cuh"\n' % c for c in cids)
+                    + "OV_DEFINE_MULTI(%s, %d, %s)\n" % (sid, 1 if mode == "fma" else 0,
+                                                        ", ".join("ov_net_%s" % c for c in cids)))
+            if not os.path.exists(src) or open(src).read() != text:
+                with open(src, "w") as fh:
+                    fh.write(text)
+            deps = hdrs + [os.path.join(GEN, "net_%s.%s" % (c, ext)) for c in cids for ext in ("h", "cuh")]
+            key = _hash_files(deps + [src], " ".join(COMMON + flags))
+            obj = os.path.join(BUILD, "multi_%s_%s.o" % (sid, mode))
+            stamp = obj + ".key"
+            objs.append(obj)
+            if force or not os.path.exists(obj) or not os.path.exists(stamp) or open(stamp).read() != key:
+                tasks.append((src, obj, flags, obj + ".log", stamp, key))
     probe_src = os.path.join(CSRC, "ov_probe.cu")
     probe_obj = os.path.join(BUILD, "ov_probe.o")
     pkey = _hash_files(hdrs + [probe_src], " ".join(COMMON))
@@ -133,8 +174,9 @@ def build(force: bool = False, jobs: int = 0, verbose: bool = False) -> str:
     abi_src = os.path.join(CSRC, "odevec_abi.cu")
     abi_obj = os.path.join(BUILD, "odevec_abi.o")
     tune_inc = write_tuning_table()
+    multi_inc = write_multi_registry()
     key = _hash_files(hdrs + [abi_src, os.path.join(GEN, "registry.inc"),
-                              os.path.join(GEN, "includes_c.inc"), tune_inc] +
+                              os.path.join(GEN, "includes_c.inc"), tune_inc, multi_inc] +
                       [os.path.join(GEN, "net_%s.h" % c) for c, _ in variants()], " ".join(COMMON))
     if force or not os.path.exists(abi_obj) or not os.path.exists(abi_obj + ".key") or \
             open(abi_obj + ".key").read() != key:

@@ -786,8 +786,11 @@ struct Cell {
 __device__ __forceinline__ int warp_count(bool b) { return __popc(__ballot_sync(FULL, b)); }
 
 
+/* The persistent cell loop of one network variant: the body of bdf_kernel,
+   also run by the multi-network kernel for each of its jobs in turn.  A
+   warp leaves it once the job's work counter has no cells left for it. */
 template <class Net, int G, class LUT, int STAGE>
-__global__ void __launch_bounds__(StageCfg<STAGE>::BS, StageCfg<STAGE>::MINB) bdf_kernel(const LaunchArgs A)
+__device__ __forceinline__ void bdf_run(const LaunchArgs& A)
 {
     constexpr int SHM = StageCfg<STAGE>::SHM;
     constexpr int BS = StageCfg<STAGE>::BS;
@@ -1198,7 +1201,77 @@ __global__ void __launch_bounds__(StageCfg<STAGE>::BS, StageCfg<STAGE>::MINB) bd
     }
 }
 
-/* Launch helper: persistent grid of (SMs x resident blocks) unless given. */
+template <class Net, int G, class LUT, int STAGE>
+__global__ void __launch_bounds__(StageCfg<STAGE>::BS, StageCfg<STAGE>::MINB)
+    bdf_kernel(const __grid_constant__ LaunchArgs A)
+{
+    bdf_run<Net, G, LUT, STAGE>(A);
+}
+
+/* ---- several networks in one launch ---------------------------------- */
+constexpr int MULTI_STAGE = 3; /* thread-local arrays, three 128-thread blocks per SM */
+
+template <class LUT, class... Nets>
+struct MultiDispatch {
+    __device__ __forceinline__ static void run(int, const LaunchArgs&) {}
+};
+template <class LUT, class Net0, class... Rest>
+struct MultiDispatch<LUT, Net0, Rest...> {
+    __device__ __forceinline__ static void run(int idx, const LaunchArgs& A)
+    {
+        if (idx == 0)
+            bdf_run<Net0, 1, LUT, MULTI_STAGE>(A);
+        else
+            MultiDispatch<LUT, Rest...>::run(idx - 1, A);
+    }
+};
+
+template <class LUT, class... Nets>
+__global__ void __launch_bounds__(StageCfg<MULTI_STAGE>::BS, StageCfg<MULTI_STAGE>::MINB)
+    bdf_multi_kernel(const __grid_constant__ MultiArgs P)
+{
+    int first = 0;
+    while (first + 1 < P.njobs && (int)blockIdx.x >= P.block_start[first + 1])
+        ++first;
+    for (int k = 0; k < P.njobs; ++k) {
+        const int j = (first + k) % P.njobs;
+        MultiDispatch<LUT, Nets...>::run(P.net[j], P.job[j]);
+    }
+}
+
+/* Launches the multi-network kernel on P (block ranges filled in here in
+   proportion to the jobs' cells, at least one block per job). */
+template <class LUT, class... Nets>
+cudaError_t launch_multi(MultiArgs& P, cudaStream_t stream)
+{
+    using Cfg = StageCfg<MULTI_STAGE>;
+    auto kern = bdf_multi_kernel<LUT, Nets...>;
+    static int cached_grid = 0;
+    if (cached_grid == 0) {
+        int dev = 0, sms = 0, per_sm = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, Cfg::BS, 0);
+        cached_grid = sms * (per_sm > 0 ? per_sm : 1);
+    }
+    int64_t total = 0;
+    for (int j = 0; j < P.njobs; ++j)
+        total += P.job[j].ncells;
+    int grid = cached_grid;
+    if (grid < P.njobs)
+        grid = P.njobs;
+    int start = 0;
+    for (int j = 0; j < P.njobs; ++j) {
+        P.block_start[j] = start;
+        int nb = total > 0 ? (int)((double)grid * (double)P.job[j].ncells / (double)total) : 0;
+        if (nb < 1)
+            nb = 1;
+        start += nb;
+    }
+    P.block_start[P.njobs] = start;
+    kern<<<start, Cfg::BS, 0, stream>>>(P);
+    return cudaGetLastError();
+}
 template <class Net, int G, class LUT, int STAGE>
 cudaError_t launch(const LaunchArgs& a, int block, int grid, cudaStream_t stream)
 {
@@ -1276,6 +1349,25 @@ constexpr bool hist_fits_max()
 #define OV_STAGE_CASE(NET, LU, ST)                                                               \
     if (stage == ST)                                                                             \
         return launch<NET, 1, LU, ST>(a, block, grid, s);
+
+/* Defines the multi-network launcher of one set of variants in the current
+   mode: launch_multi_<sid>(P, lu, stream), lu 0 = FP64 LU, 1 = FP32 LU (fma
+   mode only). */
+#define OV_DEFINE_MULTI(sid, FP32, ...)                                                          \
+    namespace ov {                                                                               \
+    namespace OV_MODE_NS {                                                                       \
+    cudaError_t launch_multi_##sid(MultiArgs& P, int lu, cudaStream_t s)                          \
+    {                                                                                            \
+        if (lu == 0)                                                                             \
+            return launch_multi<double, __VA_ARGS__>(P, s);                                      \
+        if constexpr (FP32) {                                                                    \
+            if (lu == 1)                                                                         \
+                return launch_multi<float, __VA_ARGS__>(P, s);                                   \
+        }                                                                                        \
+        return cudaErrorNotSupported;                                                            \
+    }                                                                                            \
+    }                                                                                            \
+    }
 
 #define OV_DEFINE_LAUNCHER(cid, FP32)                                                            \
     namespace ov {                                                                               \

@@ -34,6 +34,20 @@
 #include "gen/registry.inc"
 #undef OV_NET
 
+/* multi-network launchers, one per compiled set and arithmetic mode
+   (multi_<sid>_<mode>.cu) */
+#define OV_MULTI(sid, ...)                                                                     \
+    namespace ov {                                                                             \
+    namespace exact {                                                                          \
+    cudaError_t launch_multi_##sid(MultiArgs&, int, cudaStream_t);                             \
+    }                                                                                          \
+    namespace fma {                                                                            \
+    cudaError_t launch_multi_##sid(MultiArgs&, int, cudaStream_t);                             \
+    }                                                                                          \
+    }
+#include "gen/multi.inc"
+#undef OV_MULTI
+
 namespace {
 
 struct NetEntry {
@@ -54,6 +68,21 @@ const NetEntry g_nets[] = {
 };
 #undef OV_NET
 constexpr int g_nnets = (int)(sizeof g_nets / sizeof g_nets[0]);
+
+/* the sets of variants a multi-network kernel is compiled for */
+#define OV_MULTI(sid, ...) const char* const g_multi_tags_##sid[] = {__VA_ARGS__, nullptr};
+#include "gen/multi.inc"
+#undef OV_MULTI
+struct MultiEntry {
+    const char* const* tags;
+    ov::multi_fn exact;
+    ov::multi_fn fma;
+};
+#define OV_MULTI(sid, ...) {g_multi_tags_##sid, ov::exact::launch_multi_##sid, ov::fma::launch_multi_##sid},
+const MultiEntry g_multi[] = {
+#include "gen/multi.inc"
+    {nullptr, nullptr, nullptr}};
+#undef OV_MULTI
 
 /* tuned launch options per (variant, precision, group size, GPU model),
    generated from the autotuner's table (odevec_b200/autotune.py) */
@@ -749,5 +778,106 @@ extern "C" int32_t odevec_solve_noalloc(const char* network, const odevec_opts* 
                     o.group_size, o.precision);
     if (err != cudaSuccess)
         return fail(OV_API_ECUDA, "odevec_solve_noalloc launch: %s", cudaGetErrorString(err));
+    return OV_API_OK;
+}
+
+/* ------------------------------------------------------------------------
+ * Several networks in one launch.
+ * ------------------------------------------------------------------------ */
+extern "C" int32_t odevec_solve_many(const odevec_job* jobs, int32_t njobs, void* stream)
+{
+    if (!jobs || njobs < 1 || njobs > OV_MULTI_MAX_JOBS)
+        return fail(OV_API_EINVAL, "odevec_solve_many: 1..%d jobs (got %d)", OV_MULTI_MAX_JOBS, njobs);
+    int prec = -1;
+    int live[OV_MULTI_MAX_JOBS];
+    int nlive = 0;
+    for (int j = 0; j < njobs; ++j) {
+        const odevec_job& J = jobs[j];
+        if (!J.solver)
+            return fail(OV_API_EINVAL, "odevec_solve_many: job %d has no solver", j);
+        if (J.ncells < 0)
+            return fail(OV_API_EINVAL, "odevec_solve_many: job %d: ncells < 0", j);
+        for (int i = 0; i < j; ++i)
+            if (jobs[i].solver == J.solver)
+                return fail(OV_API_EINVAL, "odevec_solve_many: jobs %d and %d share a solver", i, j);
+        const odevec_opts& o = J.solver->opts;
+        if (o.group_size != 1)
+            return fail(OV_API_EUNSUPPORTED, "odevec_solve_many: job %d: group_size %d (per-cell control only)",
+                        j, o.group_size);
+        if (prec >= 0 && o.precision != prec)
+            return fail(OV_API_EINVAL, "odevec_solve_many: jobs of different precision forms");
+        prec = o.precision;
+        if (J.ncells == 0)
+            continue;
+        if (!J.y || !J.t || !J.dt || !J.t_stop)
+            return fail(OV_API_EINVAL, "odevec_solve_many: job %d: y, t, dt and t_stop are required", j);
+        if (J.resume && !J.workspace)
+            return fail(OV_API_EINVAL, "odevec_solve_many: job %d: resume needs a workspace", j);
+        if (J.resume < 0 || J.resume > 2)
+            return fail(OV_API_EINVAL, "odevec_solve_many: job %d: resume must be 0, 1 or 2", j);
+        live[nlive++] = j;
+    }
+    if (nlive == 0)
+        return OV_API_OK;
+    /* a compiled set that holds every job's network */
+    const MultiEntry* m = g_multi;
+    int idx[OV_MULTI_MAX_JOBS];
+    for (; m->tags; ++m) {
+        bool all = true;
+        for (int q = 0; q < nlive && all; ++q) {
+            const char* tag = g_nets[jobs[live[q]].solver->net].tag;
+            idx[q] = -1;
+            for (int k = 0; m->tags[k]; ++k)
+                if (std::strcmp(m->tags[k], tag) == 0)
+                    idx[q] = k;
+            all = idx[q] >= 0;
+        }
+        if (all)
+            break;
+    }
+    if (!m->tags)
+        return fail(OV_API_EUNSUPPORTED, "odevec_solve_many: no multi-network kernel compiled for this set of "
+                    "networks (see odevec_b200/build.py MULTI_SETS)");
+    cudaStream_t st = (cudaStream_t)stream;
+    ov::MultiArgs P;
+    std::memset(&P, 0, sizeof P);
+    P.njobs = nlive;
+    for (int q = 0; q < nlive; ++q) {
+        const odevec_job& J = jobs[live[q]];
+        const odevec_opts& o = J.solver->opts;
+        ov::LaunchArgs& a = P.job[q];
+        a.ncells = J.ncells;
+        a.y = J.y;
+        a.t = J.t;
+        a.dt = J.dt;
+        a.t_stop = J.t_stop;
+        a.mask = J.mask;
+        a.status = J.status;
+        a.stats = J.stats;
+        a.queue = J.solver->d_queue;
+        a.rtol = o.rtol;
+        a.atol = o.atol;
+        a.dt_min = o.dt_min;
+        a.check_neg = o.check_negatives ? 1 : 0;
+        a.max_attempts = o.max_attempts;
+        a.jac_batch = o.jac_batch;
+        a.ss_batch = o.ss_batch;
+        a.max_wait = o.max_wait;
+        a.fix_restart = o.fix_restart ? 1 : 0;
+        a.ws = J.workspace;
+        a.resume = J.resume;
+        a.run_if = nullptr;
+        P.net[q] = idx[q];
+        cudaError_t err = cudaMemsetAsync(J.solver->d_queue, 0, sizeof(unsigned long long), st);
+        if (err != cudaSuccess)
+            return fail(OV_API_ECUDA, "odevec_solve_many: %s", cudaGetErrorString(err));
+    }
+    const int lu = prec == OV_PREC_FP32_LU ? 1 : 0;
+    ov::multi_fn fn = prec == OV_PREC_FP64 ? m->exact : m->fma;
+    cudaError_t err = fn(P, lu, st);
+    if (err == cudaErrorNotSupported)
+        return fail(OV_API_EUNSUPPORTED, "odevec_solve_many: precision %d not compiled", prec);
+    if (err != cudaSuccess)
+        return fail(OV_API_ECUDA, "odevec_solve_many launch: %s", cudaGetErrorString(err));
     return OV_API_OK;
 }

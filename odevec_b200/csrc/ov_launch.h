@@ -40,6 +40,20 @@ struct LaunchArgs {
     const unsigned long long* run_if;
 };
 
+/* Several solves of different networks in one launch (the multi-network
+   kernel): job j's launch arguments, the index of its network in the
+   kernel's network list, and its first block; a block starts with the job
+   whose block range holds it and then drains the other jobs' work counters
+   in turn, so blocks whose job is done help the others. */
+constexpr int MULTI_MAX_JOBS = 8;
+struct MultiArgs {
+    LaunchArgs job[MULTI_MAX_JOBS];
+    int32_t net[MULTI_MAX_JOBS];
+    int32_t block_start[MULTI_MAX_JOBS + 1];
+    int32_t njobs;
+};
+typedef cudaError_t (*multi_fn)(MultiArgs& P, int lu, cudaStream_t stream);
+
 /* doubles per cell of the resident workspace: history y_NS(0:5), en_old,
    error weights, and 12 scalars (internal time, step, control state) */
 __host__ __device__ constexpr int ws_doubles(int nd) { return 6 * nd + 2 * nd + 12; }

@@ -65,6 +65,14 @@ class _Opts(ctypes.Structure):
                 ("fix_restart", ctypes.c_int32), ("no_escalation", ctypes.c_int32)]
 
 
+class _Job(ctypes.Structure):
+    """odevec_job (include/odevec_b200.h)"""
+    _fields_ = [("solver", ctypes.c_void_p), ("ncells", ctypes.c_int64), ("y", ctypes.c_void_p),
+                ("t", ctypes.c_void_p), ("dt", ctypes.c_void_p), ("t_stop", ctypes.c_void_p),
+                ("mask", ctypes.c_void_p), ("status", ctypes.c_void_p), ("stats", ctypes.c_void_p),
+                ("workspace", ctypes.c_void_p), ("resume", ctypes.c_int32)]
+
+
 _lib = None
 
 
@@ -99,6 +107,8 @@ def lib():
         L.odevec_convert.argtypes = [ctypes.c_char_p, i64, i32, P, P, P, P]
         L.odevec_convert.restype = i32
         L.odevec_last_error.restype = ctypes.c_char_p
+        L.odevec_solve_many.argtypes = [ctypes.POINTER(_Job), i32, P]
+        L.odevec_solve_many.restype = i32
         _lib = L
     return _lib
 
@@ -122,7 +132,7 @@ def network_info(tag):
 
 # resident blocks per SM of each staging (block size x blocks: the launch
 # shape the kernel is compiled for; 0 = the library's automatic choice, 3)
-BLOCKS_PER_SM = {0: 3, 1: 2, 2: 1, 3: 3, 4: 4, 5: 1, 6: 1, 7: 3, 8: 1, 9: 1, 10: 1, 11: 1}
+BLOCKS_PER_SM = {0: 3, 1: 2, 2: 1, 3: 3, 4: 4, 5: 1, 6: 1, 7: 3, 8: 1, 9: 1, 10: 1, 11: 1, 12: 1}
 
 
 class Odevec:
