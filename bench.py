@@ -56,6 +56,8 @@ def parse():
                    help="fp32_lu | fp64 | fp64_fma | plain_fp64 (FP64, a thread per cell, refilled from "
                         "the work queue on every trip, Jacobian and step-size blocks run where a cell "
                         "needs them)")
+    p.add_argument("--staging", type=int, default=0,
+                   help="launch shape of the timed forms (0: the tuning table's; see odevec_opts.staging)")
     p.add_argument("--cpu-sample", type=int, default=65536)
     p.add_argument("--accuracy-cells", type=int, default=256)
     p.add_argument("--no-cpu", action="store_true")
@@ -280,6 +282,8 @@ def run_product(args):
             # block run at once by the lanes that need it (no batching), two
             # 128-thread blocks per SM, no lockstep, arrays thread-local
             kw = dict(jac_batch=1, ss_batch=1, max_wait=-1, staging=1, grid_blocks=(N + 127) // 128)
+        if args.staging and form != "plain_fp64":
+            kw = dict(staging=args.staging)
         ode = S.Odevec(wl.network, max_cells=N, RelativeTolerance=wl.rtol, AbsoluteTolerance=wl.atol,
                        MinimalTimestep=wl.dt_min, nvector=wl.group, precision="fp64" if form == "plain_fp64" else form,
                        raise_on_failure=False, **kw)
@@ -388,6 +392,7 @@ def run_product(args):
         "dtype": "f64 state/residual/control, f32 LU" if head == "fp32_lu" else "f64",
         "data": DATA,
         "config": {"workload": workload_label(args, N), "network": args.network, "form": head,
+                   "staging": args.staging or "tuning table",
                    "l2": "inputs %.0f MB per GPU %s 126 MB L2" % (
                        in_mb, ">" if in_mb > 126 else "<= (not flushed between steps)"),
                    "parallelism": "dp%d (independent cell shards, no exchange)" % world},

@@ -177,6 +177,19 @@ int32_t odevec_solve_resident(odevec_solver* s, int64_t ncells, double* y, doubl
                               const double* t_stop, const uint8_t* mask, int32_t* status,
                               int32_t* stats, double* workspace, int32_t resume, void* stream);
 
+/* odevec_solve_resident on a range of cells of larger arrays, no
+   counterpart in the reference: the caller passes y + c0, t + c0, dt + c0,
+   t_stop + c0, mask + c0, status + c0, stats + c0 * OV_NSTATS and
+   workspace + c0 (workspace may be null with resume = 0) for cells
+   [c0, c0 + ncells), and stride = the arrays' full cell count (the row
+   stride of y and of the workspace, >= ncells).  Lets a caller cut one large
+   solve into several shorter launches, e.g. a serving loop that keeps short
+   requests from waiting behind one long launch; results are those of the
+   whole solve. */
+int32_t odevec_solve_range(odevec_solver* s, int64_t ncells, int64_t stride, double* y, double* t,
+                           double* dt, const double* t_stop, const uint8_t* mask, int32_t* status,
+                           int32_t* stats, double* workspace, int32_t resume, void* stream);
+
 /* The operator-split caller's format (tests/primordial.f90:79-87, 113-140):
    the hydro code keeps mass fractions x and the gas density rho (g/cm^3) per
    cell; the network integrates number densities n (1/cm^3).  direction

@@ -299,16 +299,23 @@ struct Cell {
     bool ujac, nuo, first, msk, fz_neg;
     int status, attempts, steps, ltef, convf, newt, jacs, ppass;
 
-    /* WeightedNorm1 (src/odevec.F90:669-684) over the solver state */
-    __device__ __forceinline__ double wnorm(const double* e) const
+    /* WeightedNorm1 (src/odevec.F90:669-684) over the solver state; the
+       lane's own sum of squares is left in s_lane */
+    __device__ __forceinline__ double wnorm(const double* e, double& s_lane) const
     {
         double s = 0.0;
 #pragma unroll
         for (int j = 0; j < ND; ++j)
             s = s + e[j] * e[j] * w2[j];
         s = s + fz_add;
+        s_lane = s;
         double v = msk ? sqrt(s / N) : -HUGE_VAL;
         return group_max<G>(v);
+    }
+    __device__ __forceinline__ double wnorm(const double* e) const
+    {
+        double s;
+        return wnorm(e, s);
     }
 
     /* WeightedNorm2 of y_NS(:,:,col) for a runtime column */
@@ -498,7 +505,8 @@ struct Cell {
     /* CheckConvergence (src/odevec.F90:622-665), den in d */
     __device__ __forceinline__ void check_convergence(const double* d, bool& failed, bool& converged)
     {
-        const double err = wnorm(d);
+        double s_lane;
+        const double err = wnorm(d, s_lane);
         double rate_tmp = 0.0;
         if (it != 0) {
             rate_tmp = err / cerr;
@@ -506,10 +514,16 @@ struct Cell {
         }
         const double r15 = 1.5 * crate;
         const double crit = err * (1.0 < r15 ? 1.0 : r15) / conv_divisor(q);
-        bool nan = fz_add != fz_add;
+        /* a NaN in den or in the weights (src/odevec.F90:645) makes its
+           term and so the lane's sum of squares NaN: the entries are only
+           scanned when that sum is NaN */
+        bool nan = false;
+        if (s_lane != s_lane) {
+            nan = fz_add != fz_add;
 #pragma unroll
-        for (int j = 0; j < ND; ++j)
-            nan |= (d[j] != d[j]) | (w2[j] != w2[j]);
+            for (int j = 0; j < ND; ++j)
+                nan |= (d[j] != d[j]) | (w2[j] != w2[j]);
+        }
         if (group_any<G>(nan)) {
             failed = true;
             return;
@@ -729,7 +743,7 @@ struct Cell {
         return PH_DONE;
     }
 
-    /* resident workspace: [field][cell] with stride ncells */
+    /* resident workspace: [field][cell] with the launch's row stride */
     __device__ __forceinline__ void save_state(double* ws, int64_t n, int64_t cell) const
     {
         int f = 0;
@@ -799,6 +813,7 @@ __device__ __forceinline__ void bdf_run(const LaunchArgs& A)
     constexpr int ND = C::ND;
     const int lane = threadIdx.x & 31;
     const int64_t ncells = A.ncells;
+    const int64_t stride = A.stride;
     if (A.run_if && *A.run_if == 0)
         return;
 
@@ -876,7 +891,7 @@ __device__ __forceinline__ void bdf_run(const LaunchArgs& A)
         if (ph == PH_START) {
 #pragma unroll
             for (int j = 0; j < N; ++j)
-                c.y[j] = A.y[(int64_t)j * ncells + cell];
+                c.y[j] = A.y[(int64_t)j * stride + cell];
             c.t = A.t[cell];
             c.h = A.dt[cell];
             c.tstop = A.t_stop[cell];
@@ -934,7 +949,7 @@ __device__ __forceinline__ void bdf_run(const LaunchArgs& A)
                        weights; the state is the saved y_NS(0); rates and
                        Jacobian are recomputed (the caller may have changed
                        the temperature) */
-                    c.load_state(A.ws, ncells, cell);
+                    c.load_state(A.ws, stride, cell);
 #pragma unroll
                     for (int j = 0; j < ND; ++j)
                         if (c.msk)
@@ -959,7 +974,7 @@ __device__ __forceinline__ void bdf_run(const LaunchArgs& A)
                            object does (this%en_old is never reset) */
 #pragma unroll
                         for (int j = 0; j < ND; ++j)
-                            c.eno[j] = A.ws[((int64_t)(MAXQ + 1) * ND + j) * ncells + cell];
+                            c.eno[j] = A.ws[((int64_t)(MAXQ + 1) * ND + j) * stride + cell];
                     }
                     if (Net::NREA > 0)
                         Net::rates_T(c.y, c.rT);
@@ -1174,11 +1189,11 @@ __device__ __forceinline__ void bdf_run(const LaunchArgs& A)
         if (ph == PH_DONE) {
             const bool ok = c.status == OV_OK;
             if (A.ws && ok && write_y)
-                c.save_state(A.ws, ncells, cell);
+                c.save_state(A.ws, stride, cell);
             if ((!ok || write_y) && c.msk) {
 #pragma unroll
                 for (int j = 0; j < ND; ++j)
-                    A.y[(int64_t)Net::dyn(j) * ncells + cell] = c.y[Net::dyn(j)];
+                    A.y[(int64_t)Net::dyn(j) * stride + cell] = c.y[Net::dyn(j)];
             }
             A.t[cell] = c.t;
             if (c.status != OV_ERR_GROUP_MISMATCH)

@@ -199,18 +199,19 @@ __global__ void __launch_bounds__(256) ov_convert(int64_t ncells, int direction,
     }
 }
 
-__global__ void ov_escalate(int64_t ncells, int neq, double* y, double* t, double* dt,
+__global__ void ov_escalate(int64_t ncells, int64_t stride, int neq, double* y, double* t, double* dt,
                             const double* y_in, const double* t_in, const double* dt_in,
                             const int32_t* status, const uint8_t* mask, uint8_t* retry,
                             unsigned long long* nfail)
 {
+    /* y rows have the launch's stride, the saved inputs y_in are packed */
     for (int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; c < ncells;
          c += (int64_t)gridDim.x * blockDim.x) {
         const bool bad = status[c] != OV_OK && (!mask || mask[c]);
         retry[c] = bad ? 1 : 0;
         if (bad) {
             for (int s = 0; s < neq; ++s)
-                y[(int64_t)s * ncells + c] = y_in[(int64_t)s * ncells + c];
+                y[(int64_t)s * stride + c] = y_in[(int64_t)s * ncells + c];
             t[c] = t_in[c];
             dt[c] = dt_in[c];
             atomicAdd(nfail, 1ull);
@@ -355,15 +356,15 @@ int32_t odevec_set_options(odevec_solver* s, const odevec_opts* opts)
     return OV_API_OK;
 }
 
-static int32_t solve_impl(odevec_solver* s, int64_t ncells, double* y, double* t, double* dt,
-                          const double* t_stop, const uint8_t* mask, int32_t* status, int32_t* stats,
-                          double* ws, int32_t resume, void* stream);
+static int32_t solve_impl(odevec_solver* s, int64_t ncells, int64_t stride, double* y, double* t,
+                          double* dt, const double* t_stop, const uint8_t* mask, int32_t* status,
+                          int32_t* stats, double* ws, int32_t resume, void* stream);
 
 int32_t odevec_solve(odevec_solver* s, int64_t ncells, double* y, double* t, double* dt,
                      const double* t_stop, const uint8_t* mask, int32_t* status, int32_t* stats,
                      void* stream)
 {
-    return solve_impl(s, ncells, y, t, dt, t_stop, mask, status, stats, nullptr, 0, stream);
+    return solve_impl(s, ncells, ncells, y, t, dt, t_stop, mask, status, stats, nullptr, 0, stream);
 }
 
 int32_t odevec_workspace_doubles(const char* network, int64_t* per_cell)
@@ -385,17 +386,30 @@ int32_t odevec_solve_resident(odevec_solver* s, int64_t ncells, double* y, doubl
         return fail(OV_API_EINVAL, "odevec_solve_resident: workspace is null");
     if (resume < 0 || resume > 2)
         return fail(OV_API_EINVAL, "odevec_solve_resident: resume must be 0, 1 or 2 (got %d)", resume);
-    return solve_impl(s, ncells, y, t, dt, t_stop, mask, status, stats, workspace, resume, stream);
+    return solve_impl(s, ncells, ncells, y, t, dt, t_stop, mask, status, stats, workspace, resume, stream);
 }
 
-static int32_t solve_impl(odevec_solver* s, int64_t ncells, double* y, double* t, double* dt,
-                          const double* t_stop, const uint8_t* mask, int32_t* status, int32_t* stats,
-                          double* ws, int32_t resume, void* stream)
+int32_t odevec_solve_range(odevec_solver* s, int64_t ncells, int64_t stride, double* y, double* t, double* dt,
+                           const double* t_stop, const uint8_t* mask, int32_t* status, int32_t* stats,
+                           double* workspace, int32_t resume, void* stream)
+{
+    if (resume < 0 || resume > 2)
+        return fail(OV_API_EINVAL, "odevec_solve_range: resume must be 0, 1 or 2 (got %d)", resume);
+    if (resume && !workspace)
+        return fail(OV_API_EINVAL, "odevec_solve_range: resume needs a workspace");
+    return solve_impl(s, ncells, stride, y, t, dt, t_stop, mask, status, stats, workspace, resume, stream);
+}
+
+static int32_t solve_impl(odevec_solver* s, int64_t ncells, int64_t stride, double* y, double* t,
+                          double* dt, const double* t_stop, const uint8_t* mask, int32_t* status,
+                          int32_t* stats, double* ws, int32_t resume, void* stream)
 {
     if (!s)
         return fail(OV_API_EINVAL, "solver is null");
     if (ncells < 0)
         return fail(OV_API_EINVAL, "ncells < 0");
+    if (stride < ncells)
+        return fail(OV_API_EINVAL, "stride %lld < ncells %lld", (long long)stride, (long long)ncells);
     if (ncells == 0)
         return OV_API_OK;
     if (!y || !t || !dt || !t_stop)
@@ -407,6 +421,7 @@ static int32_t solve_impl(odevec_solver* s, int64_t ncells, double* y, double* t
     const NetEntry& e = g_nets[s->net];
     ov::LaunchArgs a;
     a.ncells = ncells;
+    a.stride = stride;
     a.y = y;
     a.t = t;
     a.dt = dt;
@@ -457,7 +472,10 @@ static int32_t solve_impl(odevec_solver* s, int64_t ncells, double* y, double* t
             s->fb_cells = ncells;
         }
         const size_t n = (size_t)ncells;
-        err = cudaMemcpyAsync(s->fb_y, y, sizeof(double) * n * neq, cudaMemcpyDeviceToDevice, st);
+        err = stride == ncells
+                  ? cudaMemcpyAsync(s->fb_y, y, sizeof(double) * n * neq, cudaMemcpyDeviceToDevice, st)
+                  : cudaMemcpy2DAsync(s->fb_y, sizeof(double) * n, y, sizeof(double) * (size_t)stride,
+                                      sizeof(double) * n, neq, cudaMemcpyDeviceToDevice, st);
         if (err == cudaSuccess) err = cudaMemcpyAsync(s->fb_t, t, sizeof(double) * n, cudaMemcpyDeviceToDevice, st);
         if (err == cudaSuccess) err = cudaMemcpyAsync(s->fb_dt, dt, sizeof(double) * n, cudaMemcpyDeviceToDevice, st);
         if (err == cudaSuccess) err = cudaMemsetAsync(s->d_queue + 1, 0, sizeof(unsigned long long), st);
@@ -470,7 +488,7 @@ static int32_t solve_impl(odevec_solver* s, int64_t ncells, double* y, double* t
     if (escalate && err == cudaSuccess) {
         int blocks = 0;
         cudaDeviceGetAttribute(&blocks, cudaDevAttrMultiProcessorCount, s->device);
-        ov_escalate<<<blocks * 4, 256, 0, st>>>(ncells, neq, y, t, dt, s->fb_y, s->fb_t, s->fb_dt,
+        ov_escalate<<<blocks * 4, 256, 0, st>>>(ncells, stride, neq, y, t, dt, s->fb_y, s->fb_t, s->fb_dt,
                                                 a.status, mask, s->fb_mask, s->d_queue + 1);
         err = cudaGetLastError();
         if (err == cudaSuccess) {
@@ -748,6 +766,7 @@ extern "C" int32_t odevec_solve_noalloc(const char* network, const odevec_opts* 
         return fail(OV_API_ECUDA, "odevec_solve_noalloc: %s", cudaGetErrorString(err));
     ov::LaunchArgs a;
     a.ncells = ncells;
+    a.stride = ncells;
     a.y = y;
     a.t = t;
     a.dt = dt;
@@ -847,6 +866,7 @@ extern "C" int32_t odevec_solve_many(const odevec_job* jobs, int32_t njobs, void
         const odevec_opts& o = J.solver->opts;
         ov::LaunchArgs& a = P.job[q];
         a.ncells = J.ncells;
+        a.stride = J.ncells;
         a.y = J.y;
         a.t = J.t;
         a.dt = J.dt;

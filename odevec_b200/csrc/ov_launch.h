@@ -7,7 +7,10 @@ namespace ov {
 
 struct LaunchArgs {
     int64_t ncells;
-    double* y;             /* [neq][ncells] */
+    /* row stride of y and ws in cells (>= ncells): the full arrays' cell
+       count when a launch covers a range of their cells */
+    int64_t stride;
+    double* y;             /* [neq][stride] */
     double* t;             /* [ncells] */
     double* dt;            /* [ncells] */
     const double* t_stop;  /* [ncells] */

@@ -554,7 +554,7 @@ struct WCell {
         }
         double f[NS], den[NS];
         if (A.resume == 1) {
-            load_state(A.ws, ncells, cell);
+            load_state(A.ws, A.stride, cell);
             double v[NS];
 #pragma unroll
             for (int m = 0; m < NS; ++m)
@@ -576,7 +576,7 @@ struct WCell {
 #pragma unroll
                 for (int m = 0; m < NS; ++m)
                     if (own(m))
-                        eno[m] = A.ws[((int64_t)f0 + lane + 32 * m) * ncells + cell];
+                        eno[m] = A.ws[((int64_t)f0 + lane + 32 * m) * A.stride + cell];
             }
 #pragma unroll
             for (int m = 0; m < NS; ++m)
@@ -769,7 +769,7 @@ __global__ void __launch_bounds__(256, 3) wpc_kernel(const LaunchArgs A)
             break;
         __syncwarp();
         for (int s = lane; s < N; s += 32)
-            c.yv[s] = A.y[(int64_t)s * ncells + cell];
+            c.yv[s] = A.y[(int64_t)s * A.stride + cell];
         __syncwarp();
         c.t = A.t[cell];
         c.h = A.dt[cell];
@@ -804,13 +804,13 @@ __global__ void __launch_bounds__(256, 3) wpc_kernel(const LaunchArgs A)
         /* store (the thread kernel's phase DONE) */
         const bool ok = c.status == OV_OK;
         if (A.ws && ok && write_y)
-            c.save_state(A.ws, ncells, cell);
+            c.save_state(A.ws, A.stride, cell);
         __syncwarp();
         if ((!ok || write_y) && c.msk) {
 #pragma unroll
             for (int m = 0; m < NS; ++m)
                 if (c.own(m))
-                    A.y[(int64_t)c.sp[m] * ncells + cell] = c.yv[c.sp[m]];
+                    A.y[(int64_t)c.sp[m] * A.stride + cell] = c.yv[c.sp[m]];
         }
         if (lane == 0) {
             A.t[cell] = c.t;

@@ -180,7 +180,7 @@ class GpuBackend:
     CUDA stream; launches are asynchronous and completion is an event."""
 
     def __init__(self, precision: str = "fp32_lu", device: str = "cuda", fair_share: bool = True,
-                 small_cells: int = 16384, staging: int = 3):
+                 small_cells: int = 16384, staging: int = 3, chunk_cells: int = 0):
         import torch
         from . import solver as S
         self.S = S
@@ -194,6 +194,10 @@ class GpuBackend:
         # block per SM holding its shared memory) would leave SMs to a single
         # request and most of the device idle under many small requests.
         self.staging = staging
+        # chunk_cells > 0: a step of a larger request is launched as ranges of
+        # at most this many cells, one after another on its stream, so that a
+        # short request arriving meanwhile waits for one range, not the step
+        self.chunk_cells = chunk_cells
         self.sms = torch.cuda.get_device_properties(device).multi_processor_count
 
     def _solver(self, r: Request):
@@ -239,9 +243,20 @@ class GpuBackend:
             h["ts"].fill_(r.dt_hydro * (step + 1))
             if step > 0:
                 h["mask"].copy_(h["failed"] == 0)
-            self.S.SolveODE(h["ode"], h["t"], h["dt"], h["ts"], h["y"], Mask=h["mask"], stream=h["stream"],
-                            want_stats=False, workspace=h["ws"], resume=step > 0)
-            st = h["ode"].status
+            if self.chunk_cells and r.ncells > self.chunk_cells:
+                if "status" not in h:
+                    h["status"] = torch.empty(r.ncells, dtype=torch.int32, device=self.device)
+                ode = h["ode"]
+                for c0 in range(0, r.ncells, self.chunk_cells):
+                    c1 = min(r.ncells, c0 + self.chunk_cells)
+                    self.S.SolveODERange(ode, c0, c1, h["t"], h["dt"], h["ts"], h["y"], h["status"],
+                                         Mask=h["mask"], stream=h["stream"], workspace=h["ws"],
+                                         resume=step > 0)
+                st = h["status"]
+            else:
+                self.S.SolveODE(h["ode"], h["t"], h["dt"], h["ts"], h["y"], Mask=h["mask"], stream=h["stream"],
+                                want_stats=False, workspace=h["ws"], resume=step > 0)
+                st = h["ode"].status
             torch.where(h["failed"] != 0, h["failed"], st, out=h["failed"])
             ev = torch.cuda.Event()
             ev.record(h["stream"])
@@ -292,14 +307,14 @@ def make_stream(seed: int = 5, rate: float = 200.0, duration: float = 1.0,
 def measure(rate: float = 200.0, duration: float = 0.25, steps: int = 50, cells=(1000, 262144),
             dt_hydro=(1e6, 1e11), networks=("ROBER_DENSE_NONE", "PRIMORDIAL_CSC_FF", "SYN64_CSC_CMK"),
             precisions=("fp32_lu", "fp64"), budget: float = 120e9, slots: int = 16, seed: int = 5,
-            isolated: bool = False, fair_share: bool = True) -> List[dict]:
+            isolated: bool = False, fair_share: bool = True, chunk_cells: int = 0) -> List[dict]:
     """Runs a Poisson request stream through the scheduler on the GPU, per
     precision form; with isolated, every request is run again alone and the
     mix's step latencies are compared with the isolated ones."""
     reqs = make_stream(seed, rate, duration, tuple(networks), tuple(cells), tuple(dt_hydro), steps)
     outs = []
     for prec in precisions:
-        be = GpuBackend(prec, fair_share=fair_share)
+        be = GpuBackend(prec, fair_share=fair_share, chunk_cells=chunk_cells)
         # warm-up: one small request per network (module load, first launches)
         warm = [Request(10**6 + i, r.network, r.y0[:, :64].copy(), r.dt_hydro, 1, 0.0, r.rtol, r.atol,
                         r.dt_min, r.dt_in) for i, r in enumerate({r.network: r for r in reqs}.values())]
@@ -307,7 +322,7 @@ def measure(rate: float = 200.0, duration: float = 0.25, steps: int = 50, cells=
         recs, res = Scheduler(be, budget, slots).run(reqs, realtime=True)
         mix = summarize(recs, res)
         offered = sum(r.ncells * r.steps for r in reqs) / duration
-        out = {"form": prec, "requests": len(reqs), "rate": rate, "steps": steps,
+        out = {"form": prec, "requests": len(reqs), "rate": rate, "steps": steps, "chunk_cells": chunk_cells,
                "cells": list(cells), "dt_hydro": list(dt_hydro), "seed": seed,
                "budget_gb": budget / 1e9, "slots": slots, "fair_share": fair_share,
                "mix": mix,
@@ -367,10 +382,12 @@ def main(argv=None):
     p.add_argument("--isolated", action="store_true", help="also time every request alone")
     p.add_argument("--no-fair-share", action="store_true",
                    help="every launch may take the whole device (no 1/k block share, one stream priority)")
+    p.add_argument("--chunk-cells", type=int, default=0,
+                   help="launch a larger request's step as ranges of at most this many cells (0: whole)")
     a = p.parse_args(argv)
     for out in measure(a.rate, a.duration, a.steps, (a.min_cells, a.max_cells), (a.dt_min, a.dt_max),
                        a.networks.split(","), a.precisions.split(","), a.budget, a.slots, a.seed,
-                       a.isolated, not a.no_fair_share):
+                       a.isolated, not a.no_fair_share, a.chunk_cells):
         print(json.dumps(out), flush=True)
 
 

@@ -107,6 +107,8 @@ def lib():
         L.odevec_convert.argtypes = [ctypes.c_char_p, i64, i32, P, P, P, P]
         L.odevec_convert.restype = i32
         L.odevec_last_error.restype = ctypes.c_char_p
+        L.odevec_solve_range.argtypes = [P, i64, i64, P, P, P, P, P, P, P, P, i32, P]
+        L.odevec_solve_range.restype = i32
         L.odevec_solve_many.argtypes = [ctypes.POINTER(_Job), i32, P]
         L.odevec_solve_many.restype = i32
         _lib = L
@@ -337,3 +339,28 @@ def SolveODE(ode: Odevec, time, dt, t_stop, y, Mask=None, stream=None, want_stat
         raise OdevecError("SolveODE: %d cells failed (first status %s)"
                           % (bad, STATUS_NAMES.get(int(status[status != 0][0]))), status)
     return t, d
+
+
+def SolveODERange(ode: Odevec, c0: int, c1: int, t, dt, t_stop, y, status, Mask=None, stream=None,
+                  workspace=None, resume=False):
+    """SolveODE on cells [c0, c1) of full-size CUDA tensors (odevec_solve_range):
+    y (neq, ncells), t, dt, t_stop, status (int32) and Mask (uint8, or None)
+    with one entry per cell, workspace from :func:`Workspace` for all ncells
+    (or None).  Only the range is read and written; a large solve cut into
+    ranges gives the results of the whole solve.  Asynchronous on `stream`."""
+    import torch
+    ncells = int(y.shape[1])
+    if not (0 <= c0 <= c1 <= ncells):
+        raise ValueError("range [%d, %d) outside %d cells" % (c0, c1, ncells))
+    for a in (y, t, dt, t_stop, status) + ((Mask,) if Mask is not None else ()):
+        if not (torch.is_tensor(a) and a.is_cuda and a.is_contiguous()):
+            raise ValueError("SolveODERange takes contiguous CUDA tensors")
+    o = ode._opts()
+    _check(lib().odevec_set_options(ode.handle, ctypes.byref(o)))
+    off = lambda a, k: None if a is None else ctypes.c_void_p(a.data_ptr() + k * a.element_size())
+    st = stream if stream is not None else torch.cuda.current_stream(y.device)
+    with torch.cuda.device(y.device):
+        _check(lib().odevec_solve_range(ode.handle, c1 - c0, ncells, off(y, c0), off(t, c0), off(dt, c0),
+                                        off(t_stop, c0), off(Mask, c0), off(status, c0), None,
+                                        off(workspace, c0), {False: 0, True: 1, 2: 2, "en_old": 2}[resume],
+                                        ctypes.c_void_p(st.cuda_stream)))

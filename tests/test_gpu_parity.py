@@ -423,3 +423,36 @@ def test_warp_per_cell_fast_forms(gpu_lib, oracle):
         assert err(g) <= max(100 * wl.rtol, 2 * ref), (precision, err(g), ref)
     # the automatic staging gives the warp kernel's bits as well
     assert_bitwise(run_gpu(gpu_lib, wl, "fp64"), run_gpu(gpu_lib, wl, "fp64", staging=7), "automatic staging")
+
+
+@pytest.mark.parametrize("precision", ["fp64", "fp32_lu"])
+def test_ranges_equal_whole_solve(gpu_lib, precision):
+    """odevec_solve_range: a solve cut into three ranges of cells (row stride
+    of the full arrays, resident workspace, two hydro steps) gives the bits of
+    the whole solve."""
+    import torch
+    S = gpu_lib
+    wl = W.primordial(ncells=1000, seed=17)
+
+    def run(ranges):
+        ode = S.Odevec(wl.network, RelativeTolerance=wl.rtol, AbsoluteTolerance=wl.atol, MinimalTimestep=wl.dt_min,
+                       nvector=1, precision=precision, raise_on_failure=False)
+        S.InitOdevec(ode)
+        y = torch.tensor(wl.y, device="cuda")
+        t = torch.tensor(wl.t0, device="cuda")
+        d = torch.tensor(wl.dt0, device="cuda")
+        ws = S.Workspace(ode, wl.ncells)
+        status = torch.zeros(wl.ncells, dtype=torch.int32, device="cuda")
+        for step in range(2):
+            ts = torch.tensor(wl.t_stop * (step + 1), device="cuda")
+            for c0, c1 in ranges:
+                S.SolveODERange(ode, c0, c1, t, d, ts, y, status, workspace=ws, resume=step > 0)
+        torch.cuda.synchronize()
+        out = [a.cpu().numpy() for a in (y, t, d, status)]
+        S.CloseOdevec(ode)
+        return out
+    whole = run([(0, wl.ncells)])
+    parts = run([(0, 300), (300, 301), (301, wl.ncells)])
+    assert np.all(whole[3] == 0)
+    for a, b in zip(parts, whole):
+        assert np.array_equal(a, b)
