@@ -299,6 +299,17 @@ struct Cell {
     bool ujac, nuo, first, msk, fz_neg;
     int status, attempts, steps, ltef, convf, newt, jacs, ppass;
 
+    /* x / N for the full species count: for a power of two N the product
+       by 2^-k, which rounds exactly as the division does (one rounding of
+       the same exact value), without the division's instruction sequence */
+    __device__ __forceinline__ static double div_n(double x)
+    {
+        if constexpr ((N & (N - 1)) == 0)
+            return x * (1.0 / N);
+        else
+            return x / N;
+    }
+
     /* WeightedNorm1 (src/odevec.F90:669-684) over the solver state; the
        lane's own sum of squares is left in s_lane */
     __device__ __forceinline__ double wnorm(const double* e, double& s_lane) const
@@ -309,7 +320,7 @@ struct Cell {
             s = s + e[j] * e[j] * w2[j];
         s = s + fz_add;
         s_lane = s;
-        double v = msk ? sqrt(s / N) : -HUGE_VAL;
+        double v = msk ? sqrt(div_n(s)) : -HUGE_VAL;
         return group_max<G>(v);
     }
     __device__ __forceinline__ double wnorm(const double* e) const
@@ -328,7 +339,7 @@ struct Cell {
             s = s + e * e * w2[j];
         }
         s = s + fz_add;
-        double v = msk ? sqrt(s / N) : -HUGE_VAL;
+        double v = msk ? sqrt(div_n(s)) : -HUGE_VAL;
         return group_max<G>(v);
     }
 
@@ -700,7 +711,7 @@ struct Cell {
         const double mx = group_max<G>(msk ? s : -HUGE_VAL);
         /* W0**(-2.0): a real exponent other than -1, 0, 1 or 2 is a pow() call
            in the reference's compiled Fortran, not 1/(W0*W0) */
-        const double d = sqrt(tol / (ov_pow(W0, -2.0) + mx / N));
+        const double d = sqrt(tol / (ov_pow(W0, -2.0) + div_n(mx)));
         const double span = fabs(tstop - t);
         return d < span ? d : span;
     }
