@@ -1369,9 +1369,10 @@ constexpr bool hist_fits_max()
    constant-coefficient CSC variants); 8 = as 6 in soft lockstep; 9, 10 =
    soft lockstep in one block of 256 or 320 with the history in shared
    memory; 11 = soft lockstep in one block of 192 with history and LU in
-   shared memory (where they fit); 12 = as 9 in one block of 384.  With
-   per-cell control stagings 2-12 refill idle lanes on every 16th trip,
-   staging 1 on every trip.  Stages 2-12 exist for per-cell control (G = 1). */
+   shared memory (where they fit); 12 = as 9 in one block of 384; 13, 14 =
+   16 or 8 lanes per cell (wpc_kernel.cuh, as 7).  With per-cell control
+   stagings 2-12 refill idle lanes on every 16th trip, staging 1 on every
+   trip.  Stages 2-14 exist for per-cell control (G = 1). */
 #define OV_STAGE_CASE(NET, LU, ST)                                                               \
     if (stage == ST)                                                                             \
         return launch<NET, 1, LU, ST>(a, block, grid, s);
@@ -1420,10 +1421,18 @@ constexpr bool hist_fits_max()
             if constexpr (shm_fits<NET, double, 192>()) {                                        \
                 OV_STAGE_CASE(NET, double, 11)                                                   \
             }                                                                                    \
-            if constexpr (wpc_ok<NET, double>()) {                                               \
-                if (stage == 7)                                                                  \
-                    return launch_wpc<NET, double>(a, grid, s);                                  \
-            }                                                                                    \
+            if constexpr (wpc_ok<NET, double, 32>()) {                                       \
+                if (stage == 7)                                                              \
+                    return launch_wpc<NET, double, 32>(a, grid, s);                          \
+            }                                                                                \
+            if constexpr (wpc_ok<NET, double, 16>()) {                                       \
+                if (stage == 13)                                                             \
+                    return launch_wpc<NET, double, 16>(a, grid, s);                          \
+            }                                                                                \
+            if constexpr (wpc_ok<NET, double, 8>()) {                                        \
+                if (stage == 14)                                                             \
+                    return launch_wpc<NET, double, 8>(a, grid, s);                           \
+            }                                                                                \
             if constexpr (shm_fits<NET, double, 128>()) {                                        \
                 OV_STAGE_CASE(NET, double, 2)                                                    \
             }                                                                                    \
@@ -1448,10 +1457,18 @@ constexpr bool hist_fits_max()
                 if constexpr (shm_fits<NET, float, 192>()) {                                     \
                     OV_STAGE_CASE(NET, float, 11)                                                \
                 }                                                                                \
-                if constexpr (wpc_ok<NET, float>()) {                                            \
-                    if (stage == 7)                                                              \
-                        return launch_wpc<NET, float>(a, grid, s);                               \
-                }                                                                                \
+                if constexpr (wpc_ok<NET, float, 32>()) {                                    \
+                    if (stage == 7)                                                          \
+                        return launch_wpc<NET, float, 32>(a, grid, s);                       \
+                }                                                                            \
+                if constexpr (wpc_ok<NET, float, 16>()) {                                    \
+                    if (stage == 13)                                                         \
+                        return launch_wpc<NET, float, 16>(a, grid, s);                       \
+                }                                                                            \
+                if constexpr (wpc_ok<NET, float, 8>()) {                                     \
+                    if (stage == 14)                                                         \
+                        return launch_wpc<NET, float, 8>(a, grid, s);                        \
+                }                                                                            \
                 if constexpr (shm_fits<NET, float, 128>()) {                                     \
                     OV_STAGE_CASE(NET, float, 2)                                                 \
                 }                                                                                \

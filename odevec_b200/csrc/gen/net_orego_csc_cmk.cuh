@@ -72,12 +72,48 @@ static __device__ const long long ov_wpc_orego_csc_cmk_sol_op[192] = {
     -1LL, -1LL, -1LL, -1LL, -1LL, -1LL, -1LL, -1LL,
     -1LL, -1LL, -1LL, -1LL, -1LL, -1LL, -1LL, -1LL,
     -1LL, -1LL, -1LL, -1LL, -1LL, -1LL, -1LL, -1LL};
+static __device__ const long long ov_wpc_orego_csc_cmk_fac_op16[64] = {
+    2305840810190438408LL, -1LL, -1LL, -1LL, -1LL, -1LL, -1LL, -1LL,
+    -1LL, -1LL, -1LL, -1LL, -1LL, -1LL, -1LL, -1LL,
+    2199031644171LL, -1LL, -1LL, -1LL, -1LL, -1LL, -1LL, -1LL,
+    -1LL, -1LL, -1LL, -1LL, -1LL, -1LL, -1LL, -1LL,
+    2305840810194632714LL, -1LL, -1LL, -1LL, -1LL, -1LL, -1LL, -1LL,
+    -1LL, -1LL, -1LL, -1LL, -1LL, -1LL, -1LL, -1LL,
+    6597080252429LL, -1LL, -1LL, -1LL, -1LL, -1LL, -1LL, -1LL,
+    -1LL, -1LL, -1LL, -1LL, -1LL, -1LL, -1LL, -1LL};
+static __device__ const long long ov_wpc_orego_csc_cmk_sol_op16[96] = {
+    2199021158400LL, -1LL, -1LL, -1LL, -1LL, -1LL, -1LL, -1LL,
+    -1LL, -1LL, -1LL, -1LL, -1LL, -1LL, -1LL, -1LL,
+    2199023255555LL, -1LL, -1LL, -1LL, -1LL, -1LL, -1LL, -1LL,
+    -1LL, -1LL, -1LL, -1LL, -1LL, -1LL, -1LL, -1LL,
+    6597067669506LL, -1LL, -1LL, -1LL, -1LL, -1LL, -1LL, -1LL,
+    -1LL, -1LL, -1LL, -1LL, -1LL, -1LL, -1LL, -1LL,
+    6597071863813LL, -1LL, -1LL, -1LL, -1LL, -1LL, -1LL, -1LL,
+    -1LL, -1LL, -1LL, -1LL, -1LL, -1LL, -1LL, -1LL,
+    15393160691716LL, -1LL, -1LL, -1LL, -1LL, -1LL, -1LL, -1LL,
+    -1LL, -1LL, -1LL, -1LL, -1LL, -1LL, -1LL, -1LL,
+    8796097216513LL, 10995120472067LL, -1LL, -1LL, -1LL, -1LL, -1LL, -1LL,
+    -1LL, -1LL, -1LL, -1LL, -1LL, -1LL, -1LL, -1LL};
+static __device__ const long long ov_wpc_orego_csc_cmk_fac_op8[32] = {
+    2305840810190438408LL, -1LL, -1LL, -1LL, -1LL, -1LL, -1LL, -1LL,
+    2199031644171LL, -1LL, -1LL, -1LL, -1LL, -1LL, -1LL, -1LL,
+    2305840810194632714LL, -1LL, -1LL, -1LL, -1LL, -1LL, -1LL, -1LL,
+    6597080252429LL, -1LL, -1LL, -1LL, -1LL, -1LL, -1LL, -1LL};
+static __device__ const long long ov_wpc_orego_csc_cmk_sol_op8[48] = {
+    2199021158400LL, -1LL, -1LL, -1LL, -1LL, -1LL, -1LL, -1LL,
+    2199023255555LL, -1LL, -1LL, -1LL, -1LL, -1LL, -1LL, -1LL,
+    6597067669506LL, -1LL, -1LL, -1LL, -1LL, -1LL, -1LL, -1LL,
+    6597071863813LL, -1LL, -1LL, -1LL, -1LL, -1LL, -1LL, -1LL,
+    15393160691716LL, -1LL, -1LL, -1LL, -1LL, -1LL, -1LL, -1LL,
+    8796097216513LL, 10995120472067LL, -1LL, -1LL, -1LL, -1LL, -1LL, -1LL};
 static __device__ const int ov_wpc_orego_csc_cmk_srow[3] = {
     2, 1, 0};
 static __device__ const int ov_wpc_orego_csc_cmk_dyn[3] = {
     0, 1, 2};
 struct ov_wpc_orego_csc_cmk {
   static constexpr int NTERM = 9, NPROG = 7, DEPTH = 4, NFL = 4, NSL = 6;
+  static constexpr int NFL16 = 4, NSL16 = 6;
+  static constexpr int NFL8 = 4, NSL8 = 6;
   __device__ static const int* rhs_ptr() { return ov_wpc_orego_csc_cmk_rhs_ptr; }
   __device__ static const int* rhs_fac() { return ov_wpc_orego_csc_cmk_rhs_fac; }
   __device__ static const int* jac_ptr() { return ov_wpc_orego_csc_cmk_jac_ptr; }
@@ -89,6 +125,10 @@ struct ov_wpc_orego_csc_cmk {
   __device__ static const double* jac_const() { return ov_wpc_orego_csc_cmk_jac_const; }
   __device__ static const long long* fac_op() { return ov_wpc_orego_csc_cmk_fac_op; }
   __device__ static const long long* sol_op() { return ov_wpc_orego_csc_cmk_sol_op; }
+  __device__ static const long long* fac_op16() { return ov_wpc_orego_csc_cmk_fac_op16; }
+  __device__ static const long long* sol_op16() { return ov_wpc_orego_csc_cmk_sol_op16; }
+  __device__ static const long long* fac_op8() { return ov_wpc_orego_csc_cmk_fac_op8; }
+  __device__ static const long long* sol_op8() { return ov_wpc_orego_csc_cmk_sol_op8; }
 };
 
 struct ov_net_orego_csc_cmk {

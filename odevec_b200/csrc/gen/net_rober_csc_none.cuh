@@ -73,12 +73,51 @@ static __device__ const long long ov_wpc_rober_csc_none_sol_op[224] = {
     -1LL, -1LL, -1LL, -1LL, -1LL, -1LL, -1LL, -1LL,
     -1LL, -1LL, -1LL, -1LL, -1LL, -1LL, -1LL, -1LL,
     -1LL, -1LL, -1LL, -1LL, -1LL, -1LL, -1LL, -1LL};
+static __device__ const long long ov_wpc_rober_csc_none_fac_op16[64] = {
+    2305840810190438404LL, 2305840810190438410LL, -1LL, -1LL, -1LL, -1LL, -1LL, -1LL,
+    -1LL, -1LL, -1LL, -1LL, -1LL, -1LL, -1LL, -1LL,
+    2199027449863LL, 2199033741325LL, -1LL, -1LL, -1LL, -1LL, -1LL, -1LL,
+    -1LL, -1LL, -1LL, -1LL, -1LL, -1LL, -1LL, -1LL,
+    2305840810196729868LL, -1LL, -1LL, -1LL, -1LL, -1LL, -1LL, -1LL,
+    -1LL, -1LL, -1LL, -1LL, -1LL, -1LL, -1LL, -1LL,
+    8796105605135LL, -1LL, -1LL, -1LL, -1LL, -1LL, -1LL, -1LL,
+    -1LL, -1LL, -1LL, -1LL, -1LL, -1LL, -1LL, -1LL};
+static __device__ const long long ov_wpc_rober_csc_none_sol_op16[112] = {
+    2199021158400LL, -1LL, -1LL, -1LL, -1LL, -1LL, -1LL, -1LL,
+    -1LL, -1LL, -1LL, -1LL, -1LL, -1LL, -1LL, -1LL,
+    2199023255555LL, -1LL, -1LL, -1LL, -1LL, -1LL, -1LL, -1LL,
+    -1LL, -1LL, -1LL, -1LL, -1LL, -1LL, -1LL, -1LL,
+    8796090925058LL, -1LL, -1LL, -1LL, -1LL, -1LL, -1LL, -1LL,
+    -1LL, -1LL, -1LL, -1LL, -1LL, -1LL, -1LL, -1LL,
+    8796095119365LL, -1LL, -1LL, -1LL, -1LL, -1LL, -1LL, -1LL,
+    -1LL, -1LL, -1LL, -1LL, -1LL, -1LL, -1LL, -1LL,
+    17592183947268LL, -1LL, -1LL, -1LL, -1LL, -1LL, -1LL, -1LL,
+    -1LL, -1LL, -1LL, -1LL, -1LL, -1LL, -1LL, -1LL,
+    10995120472065LL, 13194143727619LL, -1LL, -1LL, -1LL, -1LL, -1LL, -1LL,
+    -1LL, -1LL, -1LL, -1LL, -1LL, -1LL, -1LL, -1LL,
+    4398048608257LL, -1LL, -1LL, -1LL, -1LL, -1LL, -1LL, -1LL,
+    -1LL, -1LL, -1LL, -1LL, -1LL, -1LL, -1LL, -1LL};
+static __device__ const long long ov_wpc_rober_csc_none_fac_op8[32] = {
+    2305840810190438404LL, 2305840810190438410LL, -1LL, -1LL, -1LL, -1LL, -1LL, -1LL,
+    2199027449863LL, 2199033741325LL, -1LL, -1LL, -1LL, -1LL, -1LL, -1LL,
+    2305840810196729868LL, -1LL, -1LL, -1LL, -1LL, -1LL, -1LL, -1LL,
+    8796105605135LL, -1LL, -1LL, -1LL, -1LL, -1LL, -1LL, -1LL};
+static __device__ const long long ov_wpc_rober_csc_none_sol_op8[56] = {
+    2199021158400LL, -1LL, -1LL, -1LL, -1LL, -1LL, -1LL, -1LL,
+    2199023255555LL, -1LL, -1LL, -1LL, -1LL, -1LL, -1LL, -1LL,
+    8796090925058LL, -1LL, -1LL, -1LL, -1LL, -1LL, -1LL, -1LL,
+    8796095119365LL, -1LL, -1LL, -1LL, -1LL, -1LL, -1LL, -1LL,
+    17592183947268LL, -1LL, -1LL, -1LL, -1LL, -1LL, -1LL, -1LL,
+    10995120472065LL, 13194143727619LL, -1LL, -1LL, -1LL, -1LL, -1LL, -1LL,
+    4398048608257LL, -1LL, -1LL, -1LL, -1LL, -1LL, -1LL, -1LL};
 static __device__ const int ov_wpc_rober_csc_none_srow[3] = {
     0, 1, 2};
 static __device__ const int ov_wpc_rober_csc_none_dyn[3] = {
     0, 1, 2};
 struct ov_wpc_rober_csc_none {
   static constexpr int NTERM = 6, NPROG = 8, DEPTH = 4, NFL = 4, NSL = 7;
+  static constexpr int NFL16 = 4, NSL16 = 7;
+  static constexpr int NFL8 = 4, NSL8 = 7;
   __device__ static const int* rhs_ptr() { return ov_wpc_rober_csc_none_rhs_ptr; }
   __device__ static const int* rhs_fac() { return ov_wpc_rober_csc_none_rhs_fac; }
   __device__ static const int* jac_ptr() { return ov_wpc_rober_csc_none_jac_ptr; }
@@ -90,6 +129,10 @@ struct ov_wpc_rober_csc_none {
   __device__ static const double* jac_const() { return ov_wpc_rober_csc_none_jac_const; }
   __device__ static const long long* fac_op() { return ov_wpc_rober_csc_none_fac_op; }
   __device__ static const long long* sol_op() { return ov_wpc_rober_csc_none_sol_op; }
+  __device__ static const long long* fac_op16() { return ov_wpc_rober_csc_none_fac_op16; }
+  __device__ static const long long* sol_op16() { return ov_wpc_rober_csc_none_sol_op16; }
+  __device__ static const long long* fac_op8() { return ov_wpc_rober_csc_none_fac_op8; }
+  __device__ static const long long* sol_op8() { return ov_wpc_rober_csc_none_sol_op8; }
 };
 
 struct ov_net_rober_csc_none {

@@ -1,25 +1,29 @@
-/* Warp-per-cell BDF kernel for networks too large for one thread per cell.
+/* Lanes-per-cell BDF kernel for networks too large for one thread per cell.
  *
- * One warp integrates one cell at a time (per-cell control, G = 1); warps
- * take cells from the global counter.  Lane l holds the solver-state
- * species l, l+32, ...: their Nordsieck history, correction, previous
- * correction, error weights and FP32 scale factors in registers.  The
- * cell's full state vector, the packed LU and the solve vector live in the
- * warp's slice of shared memory.  Control is uniform across the warp, so
- * the reference's nested loops (src/odevec.F90: step loop :207, predictor
- * :259, corrector :321) are written as loops.
+ * K lanes of a warp (K = 32, 16 or 8; 32/K cells per warp) integrate one
+ * cell at a time (per-cell control, G = 1); each group of K lanes takes
+ * cells from the global counter on its own.  Lane k of a group holds the
+ * solver-state species k, k+K, ...: their Nordsieck history, correction,
+ * previous correction, error weights and FP32 scale factors in registers.
+ * The cell's full state vector, the packed LU and the solve vector live in
+ * the group's slice of shared memory.  Control is uniform across a group,
+ * so the reference's nested loops (src/odevec.F90: step loop :207,
+ * predictor :259, corrector :321) are written as loops; every exchange
+ * inside a group (__syncwarp, shuffles, votes) names the group's lanes only,
+ * so the groups of one warp may be at different points of those loops.
  *
  * The network code comes from tables generated from the same emitted
  * straight-line C that the thread-per-cell kernel and the CPU oracle
  * compile (odevec_b200/wpc.py): right-hand-side terms per species, postfix
  * programs for the entries of P = I - dt*beta*J, and the LU factorisation
- * and triangular-solve statements grouped in dependency levels.  Norms are
- * summed in species order by lane 0.  Every value is therefore produced by
- * the same IEEE operations in the same order as in the thread kernel, and
- * the FP64 form without fused multiply-add is bit-identical to the oracle.
+ * and triangular-solve statements grouped in dependency levels, one row of
+ * K slots per level.  Norms are summed in species order by the group's
+ * first lane.  Every value is therefore produced by the same IEEE
+ * operations in the same order as in the thread kernel, and the FP64 form
+ * without fused multiply-add is bit-identical to the oracle.
  *
  * All loops are bounded as in the thread kernel (max_attempts, 4 Newton
- * iterations, 10 consecutive Newton failures); no warp waits on another. */
+ * iterations, 10 consecutive Newton failures); no group waits on another. */
 #pragma once
 
 namespace ov {
@@ -28,25 +32,56 @@ namespace OV_MODE_NS {
 /* x^y out of line: the step-size selection calls it three times */
 static __device__ __noinline__ double pow_dev(double x, double y) { return ov_pow(x, y); }
 
-template <class Net, class LUT>
+/* Shared memory of one cell's group and the block shape for K lanes per
+   cell: 8 warps per block; K = 32 three blocks per SM (80 registers),
+   K = 16 two (128 registers), K = 8 one (255 registers: 8 species' history
+   per lane) */
+template <class Net, class LUT, int K>
 struct WpcLayout {
     static constexpr int N = Net::NEQ, ND = Net::ND, NNZ = Net::NNZ;
     /* doubles: state y[N], reduction scratch[ND], scale[ND], inverse scale[ND];
        then LUT: packed LU[NNZ], solve vector[N] */
     static constexpr size_t dbl_bytes = (size_t)(N + 3 * ND) * 8;
-    static constexpr size_t warp_bytes = (dbl_bytes + (size_t)(NNZ + N) * sizeof(LUT) + 15) / 16 * 16;
+    static constexpr size_t group_bytes = (dbl_bytes + (size_t)(NNZ + N) * sizeof(LUT) + 15) / 16 * 16;
     static constexpr int WARPS = 8;
-    static constexpr size_t block_bytes = warp_bytes * WARPS;
+    static constexpr int GROUPS = WARPS * (32 / K); /* cells in flight per block */
+    static constexpr int MINB = K == 32 ? 3 : (K == 16 ? 2 : 1);
+    static constexpr size_t block_bytes = group_bytes * GROUPS;
 };
 
-template <class Net, class LUT>
+/* the level rows laid out for K lanes */
+template <class W, int K>
+struct WpcLevels;
+template <class W>
+struct WpcLevels<W, 32> {
+    static constexpr int NFL = W::NFL, NSL = W::NSL;
+    __device__ static const long long* fac() { return W::fac_op(); }
+    __device__ static const long long* sol() { return W::sol_op(); }
+};
+template <class W>
+struct WpcLevels<W, 16> {
+    static constexpr int NFL = W::NFL16, NSL = W::NSL16;
+    __device__ static const long long* fac() { return W::fac_op16(); }
+    __device__ static const long long* sol() { return W::sol_op16(); }
+};
+template <class W>
+struct WpcLevels<W, 8> {
+    static constexpr int NFL = W::NFL8, NSL = W::NSL8;
+    __device__ static const long long* fac() { return W::fac_op8(); }
+    __device__ static const long long* sol() { return W::sol_op8(); }
+};
+
+template <class Net, class LUT, int K>
 struct WCell {
     using W = typename Net::Wpc;
+    using Lv = WpcLevels<W, K>;
     static constexpr int N = Net::NEQ, ND = Net::ND, NF = Net::NF, NNZ = Net::NNZ;
-    static constexpr int NS = (ND + 31) / 32; /* solver species per lane */
+    static constexpr int NS = (ND + K - 1) / K; /* solver species per lane */
     static constexpr bool SCALED = sizeof(LUT) == 4;
 
-    int lane;
+    int sub;        /* lane within the cell's group, 0..K-1 */
+    int glead;      /* warp lane of the group's first lane */
+    unsigned gmask; /* the group's lanes */
     double* yv;   /* [N] full state */
     double* red;  /* [ND] */
     double* scv;  /* [ND] */
@@ -66,17 +101,17 @@ struct WCell {
     /* sum over solver indices 0..ND-1 in order of the per-index values p */
     __device__ __forceinline__ double ordered_sum(const double (&p)[NS])
     {
-        __syncwarp();
+        __syncwarp(gmask);
 #pragma unroll
         for (int m = 0; m < NS; ++m)
             if (own(m))
-                red[lane + 32 * m] = p[m];
-        __syncwarp();
+                red[sub + K * m] = p[m];
+        __syncwarp(gmask);
         double s = 0.0;
-        if (lane == 0)
+        if (sub == 0)
             for (int j = 0; j < ND; ++j)
                 s = s + red[j];
-        s = __shfl_sync(FULL, s, 0);
+        s = __shfl_sync(gmask, s, glead);
         return s;
     }
 
@@ -129,7 +164,7 @@ struct WCell {
                 f[m] = 0.0;
                 continue;
             }
-            const int j = lane + 32 * m;
+            const int j = sub + K * m;
             const int p0 = ptr[j], p1 = ptr[j + 1];
             double acc = 0.0;
             for (int tt = p0; tt < p1; ++tt) {
@@ -220,12 +255,12 @@ struct WCell {
 
     __device__ __forceinline__ void set_y_from(const double (&v)[NS])
     {
-        __syncwarp();
+        __syncwarp(gmask);
 #pragma unroll
         for (int m = 0; m < NS; ++m)
             if (own(m) && msk)
                 yv[sp[m]] = v[m];
-        __syncwarp();
+        __syncwarp(gmask);
     }
 
     __device__ __forceinline__ void interpolate()
@@ -315,7 +350,7 @@ struct WCell {
 #pragma unroll
         for (int m = 0; m < NS; ++m)
             neg |= own(m) && yns[0][m] < 0.0;
-        return __any_sync(FULL, msk && neg);
+        return __any_sync(gmask, msk && neg);
     }
 
     __device__ __forceinline__ bool any_negative_y() const
@@ -324,7 +359,7 @@ struct WCell {
 #pragma unroll
         for (int m = 0; m < NS; ++m)
             neg |= own(m) && yv[sp[m]] < 0.0;
-        return __any_sync(FULL, msk && neg);
+        return __any_sync(gmask, msk && neg);
     }
 
     /* GetJac + LUDecompose (src/odevec.F90:301-315) from the tables */
@@ -339,16 +374,16 @@ struct WCell {
                     hexp = hexp > 480 ? 480 : (hexp < -480 ? -480 : hexp);
                     sc[m] = ov_pow2i(hexp);
                     isc[m] = ov_pow2i(-hexp);
-                    scv[lane + 32 * m] = sc[m];
-                    iscv[lane + 32 * m] = isc[m];
+                    scv[sub + K * m] = sc[m];
+                    iscv[sub + K * m] = isc[m];
                 }
         }
-        __syncwarp();
+        __syncwarp(gmask);
         const double beta = lcoef(q, 0);
         const int* ptr = W::jac_ptr();
         const int* code = W::jac_code();
         const double* cst = W::jac_const();
-        for (int e = lane; e < NNZ; e += 32) {
+        for (int e = sub; e < NNZ; e += K) {
             double st[W::DEPTH];
             int top = 0;
             for (int pc = ptr[e]; pc < ptr[e + 1]; ++pc) {
@@ -373,13 +408,14 @@ struct WCell {
                 a[e] = (LUT)(st[0]);
             }
         }
-        __syncwarp();
-        /* one row of 32 statement slots per level (a negative slot is
-           empty); the rows run in order with the warp reconverged between */
-        const long long* ops = W::fac_op();
+        __syncwarp(gmask);
+        /* one row of K statement slots per level (a negative slot is
+           empty); the rows run in order with the cell's lanes synchronised
+           between */
+        const long long* ops = Lv::fac();
 #pragma unroll 4
-        for (int l = 0; l < W::NFL; ++l) {
-            const long long o = ops[l * 32 + lane];
+        for (int l = 0; l < Lv::NFL; ++l) {
+            const long long o = ops[l * K + sub];
             if (o >= 0) {
                 const int x = (int)((o >> 1) & 0xfffff), y = (int)((o >> 21) & 0xfffff);
                 if ((o & 1) == 0)
@@ -387,7 +423,7 @@ struct WCell {
                 else
                     a[x] = a[x] - a[y] * a[(int)((o >> 41) & 0xfffff)];
             }
-            __syncwarp();
+            __syncwarp(gmask);
         }
     }
 
@@ -400,15 +436,15 @@ struct WCell {
             if (own(m)) {
                 const double res = h * f[m] - (yns[1][m] + en[m]);
                 if constexpr (SCALED)
-                    dv[srow[lane + 32 * m]] = (LUT)(res * sc[m]);
+                    dv[srow[sub + K * m]] = (LUT)(res * sc[m]);
                 else
-                    dv[srow[lane + 32 * m]] = (LUT)(res * 1.0);
+                    dv[srow[sub + K * m]] = (LUT)(res * 1.0);
             }
-        __syncwarp();
-        const long long* ops = W::sol_op();
+        __syncwarp(gmask);
+        const long long* ops = Lv::sol();
 #pragma unroll 4
-        for (int l = 0; l < W::NSL; ++l) {
-            const long long o = ops[l * 32 + lane];
+        for (int l = 0; l < Lv::NSL; ++l) {
+            const long long o = ops[l * K + sub];
             if (o >= 0) {
                 const int x = (int)((o >> 1) & 0xfffff), k = (int)((o >> 41) & 0xfffff);
                 if ((o & 1) == 0)
@@ -416,7 +452,7 @@ struct WCell {
                 else
                     dv[x] = dv[x] - dv[(int)((o >> 21) & 0xfffff)] * a[k];
             }
-            __syncwarp();
+            __syncwarp(gmask);
         }
         const double l0 = lcoef(q, 0);
         double v[NS];
@@ -424,9 +460,9 @@ struct WCell {
         for (int m = 0; m < NS; ++m) {
             if (own(m)) {
                 if constexpr (SCALED)
-                    den[m] = (double)dv[srow[lane + 32 * m]] * isc[m];
+                    den[m] = (double)dv[srow[sub + K * m]] * isc[m];
                 else
-                    den[m] = (double)dv[srow[lane + 32 * m]] * 1.0;
+                    den[m] = (double)dv[srow[sub + K * m]] * 1.0;
                 en[m] = en[m] + den[m];
                 v[m] = yns[0][m] + l0 * en[m];
             } else {
@@ -451,7 +487,7 @@ struct WCell {
 #pragma unroll
         for (int m = 0; m < NS; ++m)
             nan |= own(m) && ((d[m] != d[m]) | (w2[m] != w2[m]));
-        if (__any_sync(FULL, nan)) {
+        if (__any_sync(gmask, nan)) {
             failed = true;
             return;
         }
@@ -496,15 +532,15 @@ struct WCell {
 #pragma unroll
             for (int m = 0; m < NS; ++m)
                 if (own(m))
-                    ws[((int64_t)k * ND + lane + 32 * m) * n + cell] = yns[k][m];
+                    ws[((int64_t)k * ND + sub + K * m) * n + cell] = yns[k][m];
         const int f = (MAXQ + 1) * ND;
 #pragma unroll
         for (int m = 0; m < NS; ++m)
             if (own(m)) {
-                ws[((int64_t)f + lane + 32 * m) * n + cell] = eno[m];
-                ws[((int64_t)f + ND + lane + 32 * m) * n + cell] = w2[m];
+                ws[((int64_t)f + sub + K * m) * n + cell] = eno[m];
+                ws[((int64_t)f + ND + sub + K * m) * n + cell] = w2[m];
             }
-        if (lane == 0) {
+        if (sub == 0) {
             const int g = f + 2 * ND;
             const double scl[12] = {tint, h, crate, jchg, (double)q, (double)swu, (double)lju, (double)fet,
                                     (double)fc, ujac ? 1.0 : 0.0, nuo ? 1.0 : 0.0, first ? 1.0 : 0.0};
@@ -519,13 +555,13 @@ struct WCell {
         for (int k = 0; k <= MAXQ; ++k)
 #pragma unroll
             for (int m = 0; m < NS; ++m)
-                yns[k][m] = own(m) ? ws[((int64_t)k * ND + lane + 32 * m) * n + cell] : 0.0;
+                yns[k][m] = own(m) ? ws[((int64_t)k * ND + sub + K * m) * n + cell] : 0.0;
         const int f = (MAXQ + 1) * ND;
 #pragma unroll
         for (int m = 0; m < NS; ++m)
             if (own(m)) {
-                eno[m] = ws[((int64_t)f + lane + 32 * m) * n + cell];
-                w2[m] = ws[((int64_t)f + ND + lane + 32 * m) * n + cell];
+                eno[m] = ws[((int64_t)f + sub + K * m) * n + cell];
+                w2[m] = ws[((int64_t)f + ND + sub + K * m) * n + cell];
             }
         const int g = f + 2 * ND;
         t = ws[((int64_t)g + 0) * n + cell];
@@ -576,7 +612,7 @@ struct WCell {
 #pragma unroll
                 for (int m = 0; m < NS; ++m)
                     if (own(m))
-                        eno[m] = A.ws[((int64_t)f0 + lane + 32 * m) * A.stride + cell];
+                        eno[m] = A.ws[((int64_t)f0 + sub + K * m) * A.stride + cell];
             }
 #pragma unroll
             for (int m = 0; m < NS; ++m)
@@ -732,19 +768,24 @@ struct WCell {
     }
 };
 
-template <class Net, class LUT>
-__global__ void __launch_bounds__(256, 3) wpc_kernel(const LaunchArgs A)
+template <class Net, class LUT, int K>
+__global__ void __launch_bounds__(256, (WpcLayout<Net, LUT, K>::MINB)) wpc_kernel(const LaunchArgs A)
 {
-    using L = WpcLayout<Net, LUT>;
-    using C = WCell<Net, LUT>;
+    using L = WpcLayout<Net, LUT, K>;
+    using C = WCell<Net, LUT, K>;
     constexpr int N = Net::NEQ, ND = Net::ND, NNZ = Net::NNZ, NS = C::NS;
+    static_assert(K == 8 || K == 16 || K == 32, "8, 16 or 32 lanes per cell");
     if (A.run_if && *A.run_if == 0)
         return;
     extern __shared__ __align__(16) unsigned char ov_wsmem[];
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    unsigned char* base = ov_wsmem + (size_t)warp * L::warp_bytes;
+    const int lane = threadIdx.x & 31;
+    const int sub = lane % K;
+    const int group = threadIdx.x / K; /* the cell slot of this block */
+    unsigned char* base = ov_wsmem + (size_t)group * L::group_bytes;
     C c;
-    c.lane = lane;
+    c.sub = sub;
+    c.glead = lane - sub;
+    c.gmask = K == 32 ? FULL : (((1u << K) - 1u) << (lane - sub));
     c.yv = reinterpret_cast<double*>(base);
     c.red = c.yv + N;
     c.scv = c.red + ND;
@@ -754,7 +795,7 @@ __global__ void __launch_bounds__(256, 3) wpc_kernel(const LaunchArgs A)
     const int* dyn = Net::Wpc::dyn();
 #pragma unroll
     for (int m = 0; m < NS; ++m) {
-        const int j = lane + 32 * m;
+        const int j = sub + K * m;
         c.sp[m] = j < ND ? dyn[j] : -1;
         c.sc[m] = 1.0;
         c.isc[m] = 1.0;
@@ -762,15 +803,15 @@ __global__ void __launch_bounds__(256, 3) wpc_kernel(const LaunchArgs A)
     const int64_t ncells = A.ncells;
     for (;;) {
         unsigned long long g = 0;
-        if (lane == 0)
+        if (sub == 0)
             g = atomicAdd(A.queue, 1ull);
-        const int64_t cell = (int64_t)__shfl_sync(FULL, g, 0);
+        const int64_t cell = (int64_t)__shfl_sync(c.gmask, g, c.glead);
         if (cell >= ncells)
             break;
-        __syncwarp();
-        for (int s = lane; s < N; s += 32)
+        __syncwarp(c.gmask);
+        for (int s = sub; s < N; s += K)
             c.yv[s] = A.y[(int64_t)s * A.stride + cell];
-        __syncwarp();
+        __syncwarp(c.gmask);
         c.t = A.t[cell];
         c.h = A.dt[cell];
         c.tstop = A.t_stop[cell];
@@ -805,14 +846,14 @@ __global__ void __launch_bounds__(256, 3) wpc_kernel(const LaunchArgs A)
         const bool ok = c.status == OV_OK;
         if (A.ws && ok && write_y)
             c.save_state(A.ws, A.stride, cell);
-        __syncwarp();
+        __syncwarp(c.gmask);
         if ((!ok || write_y) && c.msk) {
 #pragma unroll
             for (int m = 0; m < NS; ++m)
                 if (c.own(m))
                     A.y[(int64_t)c.sp[m] * A.stride + cell] = c.yv[c.sp[m]];
         }
-        if (lane == 0) {
+        if (sub == 0) {
             A.t[cell] = c.t;
             A.dt[cell] = c.h;
             if (A.status)
@@ -832,11 +873,11 @@ __global__ void __launch_bounds__(256, 3) wpc_kernel(const LaunchArgs A)
     }
 }
 
-template <class Net, class LUT>
+template <class Net, class LUT, int K>
 cudaError_t launch_wpc(const LaunchArgs& a, int grid, cudaStream_t stream)
 {
-    using L = WpcLayout<Net, LUT>;
-    auto kern = wpc_kernel<Net, LUT>;
+    using L = WpcLayout<Net, LUT, K>;
+    auto kern = wpc_kernel<Net, LUT, K>;
     constexpr int block = 32 * L::WARPS;
     static int cached = 0;
     if (cached == 0) {
@@ -854,7 +895,7 @@ cudaError_t launch_wpc(const LaunchArgs& a, int grid, cudaStream_t stream)
     }
     if (grid <= 0) {
         grid = cached;
-        const int64_t blocks_needed = (a.ncells + L::WARPS - 1) / L::WARPS;
+        const int64_t blocks_needed = (a.ncells + L::GROUPS - 1) / L::GROUPS;
         if (blocks_needed < grid)
             grid = (int)blocks_needed;
         if (grid < 1)
@@ -864,15 +905,16 @@ cudaError_t launch_wpc(const LaunchArgs& a, int grid, cudaStream_t stream)
     return cudaGetLastError();
 }
 
-/* warp-per-cell tables exist for this variant (constant-coefficient network,
-   CSC packaging, LUmethod 1) and its shared memory fits a block */
-template <class Net, class LUT>
+/* lanes-per-cell tables exist for this variant (constant-coefficient
+   network, CSC packaging, LUmethod 1) and its shared memory fits the SM
+   with the layout's blocks per SM */
+template <class Net, class LUT, int K>
 constexpr bool wpc_ok()
 {
     if constexpr (!Net::HAS_WPC)
         return false;
     else
-        return WpcLayout<Net, LUT>::block_bytes <= 200 * 1024;
+        return WpcLayout<Net, LUT, K>::block_bytes * WpcLayout<Net, LUT, K>::MINB <= 226 * 1024;
 }
 
 }  // namespace OV_MODE_NS

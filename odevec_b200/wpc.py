@@ -1,9 +1,10 @@
 """Tables for the warp-per-cell kernel, derived from the emitted network code.
 
 For networks of more than about 32 species one thread cannot keep a cell's
-state on chip (SYN64: ~9 KB per cell), so a warp integrates one cell: lane l
-holds the solver-state species l, l+32, ... and the network code runs as
-tables the lanes share out.  The tables are produced from exactly the
+state on chip (SYN64: ~9 KB per cell), so K lanes of a warp (K = 32, 16 or
+8; 32/K cells per warp) integrate one cell: lane k of the group holds the
+solver-state species k, k+K, ... and the network code runs as tables the
+lanes share out.  The tables are produced from exactly the
 straight-line C that the thread-per-cell kernel and the CPU oracle compile,
 so the warp kernel performs the same IEEE operations in the same order and
 its FP64 form is bit-identical to them:
@@ -26,6 +27,8 @@ from __future__ import annotations
 
 import re
 from typing import Dict, List, Tuple
+
+LANES = (32, 16, 8)  # lanes per cell the level tables are laid out for
 
 # ------------------------------------------------------------ expression parser
 _TOK = re.compile(r"\s*(?:(\d+\.\d*(?:[eE][-+]?\d+)?|\d+[eE][-+]?\d+|\d+)|(y\[\d+\])|(beta|dt)|([-+*/()]))")
@@ -323,6 +326,12 @@ def solve_levels(ops):
                   lambda o: ("d", o[1]))
 
 
+def level_rows(lev: List[List[int]], width: int) -> List[List[int]]:
+    """Statement rows for `width` lanes: each level cut into rows of at most
+    `width` statements, levels in order."""
+    return [idx[r:r + width] for idx in lev for r in range(0, len(idx), width)]
+
+
 # ------------------------------------------------------------------ emission
 def eligible(sysm) -> bool:
     return sysm.packaging == "CSC" and sysm.lu_method == 1 and not sysm.net.rates
@@ -429,21 +438,22 @@ def emit(sysm, cid: str) -> str:
     L.append(_arr("int", "ov_wpc_%s_jac_code" % cid, code))
     L.append(_arr("double", "ov_wpc_%s_jac_const" % cid, [_dbl(c) for c in t["consts"]], 4))
     L.append(_arr("int", "ov_wpc_%s_jac_rc" % cid, [r | (c << 16) for r, c in zip(t["rows"], t["cols"])]))
-    # factorisation and solve statements: one row of 32 slots per level (a
-    # level of more than 32 statements takes several rows: its statements
-    # are independent, so running them one row after another is the same)
-    def lev_tables(name, ops, lev, enc):
-        rows = []
-        for idx in lev:
-            for r in range(0, len(idx), 32):
-                part = idx[r:r + 32]
-                rows.append([enc(ops[i]) for i in part] + ["-1LL"] * (32 - len(part)))
-        L.append(_arr("long long", "ov_wpc_%s_%s_op" % (cid, name), [v for row in rows for v in row], 8))
+    # factorisation and solve statements: one row of K slots per level for
+    # the K lanes that hold a cell (K = 32, 16, 8); a level of more than K
+    # statements takes several rows: its statements are independent, so
+    # running them one row after another is the same
+    def lev_tables(name, ops, lev, enc, width):
+        rows = [[enc(ops[i]) for i in part] + ["-1LL"] * (width - len(part)) for part in level_rows(lev, width)]
+        sfx = "" if width == 32 else str(width)
+        L.append(_arr("long long", "ov_wpc_%s_%s_op%s" % (cid, name, sfx), [v for row in rows for v in row], 8))
         return len(rows)
 
     enc = lambda o: "%dLL" % (o[0] | (o[1] << 1) | ((o[2] & 0xfffff) << 21) | ((o[3] & 0xfffff) << 41))
-    nfl = lev_tables("fac", t["fops"], t["flev"], enc)
-    nsl = lev_tables("sol", t["sops"], t["slev"], enc)
+    nlev = {}
+    for width in LANES:
+        nlev[width] = (lev_tables("fac", t["fops"], t["flev"], enc, width),
+                       lev_tables("sol", t["sops"], t["slev"], enc, width))
+    nfl, nsl = nlev[32]
     # solver index <-> storage row of the solve vector
     srow = [0] * nd
     for i, j in t["init"].items():
@@ -456,11 +466,16 @@ def emit(sysm, cid: str) -> str:
     L.append("struct ov_wpc_%s {" % cid)
     L.append("  static constexpr int NTERM = %d, NPROG = %d, DEPTH = %d, NFL = %d, NSL = %d;"
              % (len(coef), len(t["progs"]), dmax, nfl, nsl))
+    for width in LANES[1:]:
+        L.append("  static constexpr int NFL%d = %d, NSL%d = %d;" % (width, nlev[width][0], width, nlev[width][1]))
     for nm in ("rhs_ptr", "rhs_fac", "jac_ptr", "jac_code", "jac_rc", "srow", "dyn"):
         L.append("  __device__ static const int* %s() { return ov_wpc_%s_%s; }" % (nm, cid, nm))
     for nm in ("rhs_coef", "jac_const"):
         L.append("  __device__ static const double* %s() { return ov_wpc_%s_%s; }" % (nm, cid, nm))
-    for nm in ("fac_op", "sol_op"):
-        L.append("  __device__ static const long long* %s() { return ov_wpc_%s_%s; }" % (nm, cid, nm))
+    for width in LANES:
+        sfx = "" if width == 32 else str(width)
+        for nm in ("fac_op", "sol_op"):
+            L.append("  __device__ static const long long* %s%s() { return ov_wpc_%s_%s%s; }"
+                     % (nm, sfx, cid, nm, sfx))
     L.append("};")
     return "\n".join(L) + "\n"

@@ -102,9 +102,9 @@ def test_scheduling_does_not_change_results(gpu_lib, precision):
         g = run_gpu(gpu_lib, wl, precision, batch=batch)
         assert_bitwise(g, ref, "batch %s" % (batch,))
     # every staging (6: staging 3's thread-local kernel in one 384-thread
-    # block per SM; 8-11: soft lockstep), with the default batches and with
+    # block per SM; 8-12: soft lockstep), with the default batches and with
     # per-cell blocks
-    for staging in (1, 2, 3, 4, 6, 8, 9, 10) + ((5, 11) if precision == "fp32_lu" else ()):
+    for staging in (1, 2, 3, 4, 6, 8, 9, 10, 12) + ((5, 11) if precision == "fp32_lu" else ()):
         for batch in [(0, 0, 0), (1, 1, -1)]:
             g = run_gpu(gpu_lib, wl, precision, batch=batch, staging=staging)
             assert_bitwise(g, ref, "staging %d batch %s" % (staging, batch))
@@ -364,7 +364,9 @@ def test_empty_and_group_size_errors(gpu_lib):
         S.CloseOdevec(ode)
 
 
-# ------------------------------------------------- warp per cell (staging 7)
+# ------------------------------------ lanes per cell (stagings 7, 13, 14)
+# 32, 16 or 8 lanes hold one cell (1, 2 or 4 cells per warp)
+WPC_STAGINGS = [7, 13, 14]
 WPC_CASES = [
     ("SYN64", dict(ncells=200), "SYN64_CSC_CMK"),
     ("ROBER", dict(ncells=256), "ROBER_CSC_NONE"),
@@ -372,33 +374,37 @@ WPC_CASES = [
 ]
 
 
+@pytest.mark.parametrize("staging", WPC_STAGINGS)
 @pytest.mark.parametrize("name,kw,network", WPC_CASES)
-def test_warp_per_cell_bit_exact_vs_oracle(gpu_lib, oracle, name, kw, network):
-    # one warp per cell evaluates the network from tables of the emitted code
+def test_warp_per_cell_bit_exact_vs_oracle(gpu_lib, oracle, name, kw, network, staging):
+    # K lanes per cell evaluate the network from tables of the emitted code
     # and must reproduce the oracle (and the thread-per-cell kernel) bit for bit
     wl = W.BUILDERS[name](network=network, **kw)
     wl.group = 1
-    g = run_gpu(gpu_lib, wl, "fp64", group=1, staging=7)
+    g = run_gpu(gpu_lib, wl, "fp64", group=1, staging=staging)
     o = run_oracle(oracle, wl, group=1)
     assert np.all(o[3] == 0)
-    assert_bitwise(g, o, "%s warp per cell" % network)
+    assert_bitwise(g, o, "%s lanes per cell, staging %d" % (network, staging))
     assert_bitwise(run_gpu(gpu_lib, wl, "fp64", group=1, staging=3), o, "%s thread per cell" % network)
 
 
-def test_warp_per_cell_options(gpu_lib, oracle):
+@pytest.mark.parametrize("staging", WPC_STAGINGS)
+def test_warp_per_cell_options(gpu_lib, oracle, staging):
     wl = W.syn64(ncells=96)
     mask = (np.arange(96) % 4 != 1).astype(np.uint8)
-    assert_bitwise(run_gpu(gpu_lib, wl, "fp64", mask=mask, staging=7), run_oracle(oracle, wl, mask=mask), "mask")
-    assert_bitwise(run_gpu(gpu_lib, wl, "fp64", check_negatives=True, staging=7),
+    assert_bitwise(run_gpu(gpu_lib, wl, "fp64", mask=mask, staging=staging), run_oracle(oracle, wl, mask=mask),
+                   "mask")
+    assert_bitwise(run_gpu(gpu_lib, wl, "fp64", check_negatives=True, staging=staging),
                    run_oracle(oracle, wl, check_negatives=True), "check negatives")
-    g = run_gpu(gpu_lib, wl, "fp64", max_attempts=9, staging=7)
+    g = run_gpu(gpu_lib, wl, "fp64", max_attempts=9, staging=staging)
     assert np.all(g[3] == 4)
     assert_bitwise(g, run_oracle(oracle, wl, max_attempts=9), "max attempts")
 
 
-def test_warp_per_cell_resident(gpu_lib, oracle):
+@pytest.mark.parametrize("staging", WPC_STAGINGS)
+def test_warp_per_cell_resident(gpu_lib, oracle, staging):
     wl = W.syn64(ncells=64)
-    _resident_steps(gpu_lib, oracle, wl, "fp64", 3, 1, staging=7)
+    _resident_steps(gpu_lib, oracle, wl, "fp64", 3, 1, staging=staging)
 
 
 def test_warp_per_cell_fast_forms(gpu_lib, oracle):
@@ -416,11 +422,12 @@ def test_warp_per_cell_fast_forms(gpu_lib, oracle):
         return np.max(np.abs(g[0] - o[0]) / np.maximum(np.abs(o[0]), floor))
 
     for precision in ("fp64_fma", "fp32_lu"):
-        g = run_gpu(gpu_lib, wl, precision, staging=7)
-        assert np.all(g[3] == 0)
-        assert np.max(np.abs(m @ g[0] - m @ wl.y) / (m @ wl.y)) < 1e-4
         ref = err(run_gpu(gpu_lib, wl, precision, staging=3))
-        assert err(g) <= max(100 * wl.rtol, 2 * ref), (precision, err(g), ref)
+        for staging in WPC_STAGINGS:
+            g = run_gpu(gpu_lib, wl, precision, staging=staging)
+            assert np.all(g[3] == 0)
+            assert np.max(np.abs(m @ g[0] - m @ wl.y) / (m @ wl.y)) < 1e-4
+            assert err(g) <= max(100 * wl.rtol, 2 * ref), (precision, staging, err(g), ref)
     # the automatic staging gives the warp kernel's bits as well
     assert_bitwise(run_gpu(gpu_lib, wl, "fp64"), run_gpu(gpu_lib, wl, "fp64", staging=7), "automatic staging")
 

@@ -93,3 +93,19 @@ def test_table_indices_in_bounds(variant):
     wpc.check_bounds(t)
     text = wpc.emit(s, "x")
     assert "ov_wpc_x_sol_op" in text and "NFL = %d" % len(t["flev"]) in text
+
+
+def test_level_rows_per_lane_count(variant):
+    """The rows for K lanes per cell (K = 32, 16, 8) hold at most K
+    statements of one level each and keep the level order."""
+    tag, s, t = variant
+    text = wpc.emit(s, "x")
+    for width in wpc.LANES:
+        for lev in (t["flev"], t["slev"]):
+            rows = wpc.level_rows(lev, width)
+            assert all(0 < len(r) <= width for r in rows)
+            assert [i for r in rows for i in r] == [i for l in lev for i in l]
+            assert len(rows) == sum(-(-len(l) // width) for l in lev)
+        if width != 32:
+            assert "NFL%d = %d" % (width, len(wpc.level_rows(t["flev"], width))) in text
+            assert "ov_wpc_x_sol_op%d" % width in text
