@@ -100,11 +100,12 @@ typedef struct odevec_opts {
        history in shared memory (where it fits); 11 = soft lockstep in one
        block of 192 with history and LU in shared memory (where they fit,
        typically with FP32 factors); 12 = as 9 in one block of 384; 13, 14 =
-       as 7 with 16 or 8 lanes per cell (2 or 4 cells per warp) (2-14:
-       per-cell control only).  In 2-6 and 8-12 idle lanes take new cells on
-       every 16th trip of the cell loop, so cells are set up several at a
-       time (in 8-12 in all warps of a block at once); staging 1 refills on
-       every trip.  block_threads (a multiple of 32 up to
+       as 7 with 16 or 8 lanes per cell (2 or 4 cells per warp); 15, 16 = as
+       8 in one block of 256 or 512 threads (networks above 32 solver
+       species) (2-16: per-cell control only).  In 2-6 and 8-16 idle lanes
+       take new cells on every 16th trip of the cell loop, so cells are set
+       up several at a time (in 8-12, 15, 16 in all warps of a block at
+       once); staging 1 refills on every trip.  block_threads (a multiple of 32 up to
        the block of the staging) and grid_blocks: 0 = automatic (persistent
        grid filling every SM) */
     int32_t staging;

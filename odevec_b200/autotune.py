@@ -4,9 +4,9 @@ What it chooses, per network variant, precision form and GPU model:
 
 * the staging -- where a cell's Nordsieck history and LU live (thread-local
   arrays in registers / local memory, or shared memory), the block size
-  (cells per block: 128, 192, 256, 320 or 384 threads), the blocks per SM and
-  soft lockstep, or one warp per cell (staging 7, for the variants that have
-  its tables);
+  (cells per block: 128, 192, 256, 320, 384 or 512 threads), the blocks per
+  SM and soft lockstep, or 32, 16 or 8 lanes per cell (stagings 7, 13, 14,
+  for the variants that have their tables);
 * for staging 1, the batching of the Jacobian and step-size blocks
   (jac_batch, ss_batch, max_wait); the other stagings run those blocks on
   fixed trips.
@@ -29,7 +29,7 @@ from typing import Callable, Dict, List, Optional, Tuple
 HERE = os.path.dirname(os.path.abspath(__file__))
 TABLE = os.path.join(HERE, "tuning.json")
 
-STAGINGS = (1, 2, 3, 4, 6, 7, 8, 9, 10, 11, 12, 13, 14)
+STAGINGS = (1, 2, 3, 4, 6, 7, 8, 9, 10, 11, 12, 13, 14, 15, 16)
 FP32_STAGINGS = (5,)
 BATCHES = ((24, 24, 8), (16, 16, 4), (32, 32, 16), (8, 8, 4), (4, 4, 2), (2, 2, 1), (1, 1, -1))
 # the batch options act on staging 1 only; the other stagings run the Jacobian
@@ -158,7 +158,10 @@ def main(argv=None):
     out = {}
     for net in nets:
         name = net.split("_")[0]
-        n = a.cells if name != "SYN64" else max(1, a.cells // 8)
+        # SYN64 solves are ~70x slower per cell: half the sample, still
+        # several cells per resident lane (a sample smaller than the resident
+        # lanes favours the stagings with the most threads, not the fastest)
+        n = a.cells if name != "SYN64" else max(1, a.cells // 2)
         wl = W.BUILDERS[name](ncells=n, network=net)
         if wl.group != 1:
             continue  # lockstep groups have a single compiled configuration

@@ -194,6 +194,11 @@ template <> struct StageCfg<11> { static constexpr int SHM = 1; static constexpr
 /* as 9 with 384 threads (12 warps) per SM: the history of 384 cells fills
    the shared memory (221 KB for 12 species) */
 template <> struct StageCfg<12> { static constexpr int SHM = 2; static constexpr bool SOFT = true;  static constexpr int BS = 384, MINB = 1, REFILL = 16, PERIOD = 4; };
+/* as 8 (thread-local arrays, soft lockstep) in one block of 256 threads per
+   SM (255 registers) or of 512 (128 registers): for networks above 32
+   solver species, whose arrays live in local memory either way */
+template <> struct StageCfg<15> { static constexpr int SHM = 0; static constexpr bool SOFT = true;  static constexpr int BS = 256, MINB = 1, REFILL = 16, PERIOD = 4; };
+template <> struct StageCfg<16> { static constexpr int SHM = 0; static constexpr bool SOFT = true;  static constexpr int BS = 512, MINB = 1, REFILL = 16, PERIOD = 4; };
 
 /* Soft lockstep.  The warps of a block wait for each other at the top of
    every trip of the cell loop, so they run the same phase code at the same
@@ -1370,9 +1375,10 @@ constexpr bool hist_fits_max()
    soft lockstep in one block of 256 or 320 with the history in shared
    memory; 11 = soft lockstep in one block of 192 with history and LU in
    shared memory (where they fit); 12 = as 9 in one block of 384; 13, 14 =
-   16 or 8 lanes per cell (wpc_kernel.cuh, as 7).  With per-cell control
-   stagings 2-12 refill idle lanes on every 16th trip, staging 1 on every
-   trip.  Stages 2-14 exist for per-cell control (G = 1). */
+   16 or 8 lanes per cell (wpc_kernel.cuh, as 7); 15, 16 = as 8 in one block
+   of 256 or 512 (networks above 32 solver species).  With per-cell control
+   stagings 2-6 and 8-16 refill idle lanes on every 16th trip, staging 1 on
+   every trip.  Stages 2-16 exist for per-cell control (G = 1). */
 #define OV_STAGE_CASE(NET, LU, ST)                                                               \
     if (stage == ST)                                                                             \
         return launch<NET, 1, LU, ST>(a, block, grid, s);
@@ -1409,6 +1415,10 @@ constexpr bool hist_fits_max()
             OV_STAGE_CASE(NET, double, 4)                                                        \
             OV_STAGE_CASE(NET, double, 6)                                                        \
             OV_STAGE_CASE(NET, double, 8)                                                        \
+            if constexpr (NET::ND > 32) {                                                    \
+                OV_STAGE_CASE(NET, double, 15)                                               \
+                OV_STAGE_CASE(NET, double, 16)                                               \
+            }                                                                                \
             if constexpr (hist_fits<NET, 256>()) {                                               \
                 OV_STAGE_CASE(NET, double, 9)                                                    \
             }                                                                                    \
@@ -1445,6 +1455,10 @@ constexpr bool hist_fits_max()
                 OV_STAGE_CASE(NET, float, 4)                                                     \
                 OV_STAGE_CASE(NET, float, 6)                                                     \
                 OV_STAGE_CASE(NET, float, 8)                                                     \
+                if constexpr (NET::ND > 32) {                                                \
+                    OV_STAGE_CASE(NET, float, 15)                                            \
+                    OV_STAGE_CASE(NET, float, 16)                                            \
+                }                                                                            \
                 if constexpr (hist_fits<NET, 256>()) {                                           \
                     OV_STAGE_CASE(NET, float, 9)                                                 \
                 }                                                                                \

@@ -134,7 +134,7 @@ def network_info(tag):
 
 # resident blocks per SM of each staging (block size x blocks: the launch
 # shape the kernel is compiled for; 0 = the library's automatic choice, 3)
-BLOCKS_PER_SM = {0: 3, 1: 2, 2: 1, 3: 3, 4: 4, 5: 1, 6: 1, 7: 3, 8: 1, 9: 1, 10: 1, 11: 1, 12: 1, 13: 2, 14: 1}
+BLOCKS_PER_SM = {0: 3, 1: 2, 2: 1, 3: 3, 4: 4, 5: 1, 6: 1, 7: 3, 8: 1, 9: 1, 10: 1, 11: 1, 12: 1, 13: 2, 14: 1, 15: 1, 16: 1}
 
 
 class Odevec:
