@@ -241,6 +241,18 @@ def test_syn64_mass_conservation(gpu_lib):
     assert np.max(np.abs(m @ g[0] - m @ wl.y) / (m @ wl.y)) < 1e-4
 
 
+def test_syn64_stagings_bit_exact(gpu_lib, oracle):
+    """The 64-species network on every thread-per-cell shape it compiles
+    (the soft-lockstep 256- and 512-thread blocks exist for networks above
+    32 solver species only), with more cells than one block holds, equals
+    the oracle bit for bit."""
+    wl = W.syn64(ncells=700)
+    o = run_oracle(oracle, wl)
+    assert np.all(o[3] == 0)
+    for staging in (1, 3, 6, 8, 15, 16):
+        assert_bitwise(run_gpu(gpu_lib, wl, "fp64", staging=staging), o, "SYN64 staging %d" % staging)
+
+
 def _resident_steps(gpu_lib, oracle, wl, precision, nsteps, group, staging=0):
     """Advance the same cells through nsteps successive t_stop values with the
     integrator state kept on the device; compare every step with the oracle's
