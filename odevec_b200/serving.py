@@ -23,12 +23,16 @@ launch time.
 
 Sharing the device: the solve kernel is persistent (its blocks stay resident
 until the request's cells run out), so a launch that takes every SM would
-hold back every request behind it.  With fair sharing, each launch gets
-1/k of the device's resident blocks when k requests are in flight (all of
-them when it runs alone; never fewer than one block per SM), and requests
-of at most `small_cells` cells run
-on a higher-priority stream, so their blocks are placed first whenever
-blocks retire.
+hold back every request behind it.  With fair sharing, the device's
+resident blocks are shared by water-filling over the requests in flight:
+in order of demand (the blocks a request's cells fill), each request gets
+its demand or an equal part of what is left, whichever is smaller -- small
+requests get what they can use and the large ones share the rest (never
+fewer than one block per SM; everything when a request runs alone).
+Requests of at most `small_cells` cells run on a higher-priority stream, so
+their blocks are placed first whenever blocks retire; with `chunk_cells` a
+large request's step is a series of shorter range launches, so blocks
+retire often.
 
 Failures: where the reference stops the program (src/odevec.F90:272-275,
 380-390), a cell here gets a nonzero status.  A failed cell keeps its
@@ -134,7 +138,7 @@ class Scheduler:
                 h = self.backend.admit(r)
                 active[r.rid] = {"req": r, "h": h, "step": 0, "ready": max(r.arrival, 0.0), "need": need,
                                  "launched": now()}
-                self.backend.launch(h, 0, len(active))
+                self.backend.launch(h, 0, [s["req"] for s in active.values()])
             # completions
             done_any = False
             for rid in list(active):
@@ -149,7 +153,7 @@ class Scheduler:
                     if st["step"] < r.steps:
                         st["ready"] = tdone
                         st["launched"] = now()
-                        self.backend.launch(st["h"], st["step"], len(active))
+                        self.backend.launch(st["h"], st["step"], [s["req"] for s in active.values()])
                     else:
                         results[rid] = self.backend.release(st["h"])
                         used -= st["need"]
@@ -173,6 +177,18 @@ def summarize(records: List[StepRecord], results: Optional[Dict[int, Result]] = 
             "service_p99_ms": 1e3 * float(np.percentile(svc, 99))} | (
         {} if results is None else
         {"failed_cells": sum(results[rid].failed for rid in {r.rid for r in records} if rid in results)})
+
+
+def water_fill(demands: Dict[int, int], capacity: int) -> Dict[int, int]:
+    """Shares of `capacity` blocks: in order of demand (ties by id), each
+    gets its demand or an equal part of what is left, whichever is smaller."""
+    out = {}
+    left, todo = int(capacity), len(demands)
+    for rid, d in sorted(demands.items(), key=lambda kv: (kv[1], kv[0])):
+        out[rid] = min(int(d), left // todo)
+        left -= out[rid]
+        todo -= 1
+    return out
 
 
 class GpuBackend:
@@ -230,15 +246,30 @@ class GpuBackend:
                  "ev": None}
         return h
 
-    def launch(self, h, step: int, active: int = 1):
+    def share(self, r, active, staging: int) -> int:
+        """Blocks for a launch of request r among the requests in flight
+        `active` (r included; a count means that many equal requests).
+        Water-filling in order of demand; at least one block per SM, since a
+        persistent grid keeps its size after the others finish and a
+        narrower one would leave SMs idle."""
+        capacity = self.sms * self.S.BLOCKS_PER_SM.get(staging, 3)
+        if not isinstance(active, (list, tuple)):
+            return max(self.sms, capacity // max(int(active), 1))
+        bs = self.S.CELLS_PER_BLOCK.get(staging, 128)
+        demands = {}
+        for p in active:
+            n = p.ncells if not self.chunk_cells else min(p.ncells, self.chunk_cells)
+            demands[p.rid] = -(-n // bs)
+        if r.rid not in demands:
+            return capacity  # r runs alone
+        return max(self.sms, water_fill(demands, capacity)[r.rid])
+
+    def launch(self, h, step: int, active=1):
+        """active: the requests in flight (this one included), or their count."""
         torch = self.torch
         r = h["r"]
         if self.fair_share:
-            # 1/k of the resident blocks of the staging this request runs with,
-            # but at least one block per SM: a persistent grid keeps its size
-            # after other requests finish, so a narrower one would leave SMs idle
-            capacity = self.sms * self.S.BLOCKS_PER_SM.get(h["ode"].staging, 3)
-            h["ode"].grid_blocks = max(self.sms, capacity // max(active, 1))
+            h["ode"].grid_blocks = self.share(r, active, h["ode"].staging)
         with torch.cuda.stream(h["stream"]):
             h["ts"].fill_(r.dt_hydro * (step + 1))
             if step > 0:

@@ -134,3 +134,15 @@ def test_gpu_failed_cell_matches_oracle_backend(gpu_lib, oracle):
         assert np.array_equal(f32[0].y[:, c], ref[0].y[:, c], equal_nan=True)
     ok = f32[0].status == 0
     assert np.all(np.isfinite(f32[0].y[:, ok]))
+
+
+def test_water_fill_shares():
+    """Small requests get the blocks their cells fill; large ones share the
+    rest equally; nothing exceeds the capacity."""
+    from odevec_b200.serving import water_fill
+    assert water_fill({0: 2048, 1: 8, 2: 8}, 444) == {0: 428, 1: 8, 2: 8}
+    assert water_fill({0: 2048, 1: 2048}, 444) == {0: 222, 1: 222}
+    assert water_fill({0: 100, 1: 2048, 2: 2048}, 444) == {0: 100, 1: 172, 2: 172}
+    assert water_fill({5: 3}, 444) == {5: 3}
+    s = water_fill({i: 10 * i + 1 for i in range(20)}, 444)
+    assert sum(s.values()) <= 444 and all(s[i] <= 10 * i + 1 for i in s)
