@@ -151,7 +151,12 @@ int32_t odevec_solve(odevec_solver* s, int64_t ncells, double* y, double* t, dou
 
 /* SolveODE on host arrays: copies the inputs to the solver's device buffers,
    solves, copies y, t, dt, status and stats back, and synchronises.  This is
-   the drop-in for a CPU caller such as the reference's Fortran drivers. */
+   the drop-in for a CPU caller such as the reference's Fortran drivers.  An
+   array in pinned host memory that is mapped into the device's address space
+   (cudaHostAlloc / cudaMallocHost, or cudaHostRegister with mapping) is not
+   copied: the kernel reads a cell's inputs from it when it sets the cell up
+   and writes the cell's results when it finishes, so the transfers overlap
+   the solve.  Results are the same either way. */
 int32_t odevec_solve_host(odevec_solver* s, int64_t ncells, double* y, double* t, double* dt,
                           const double* t_stop, const uint8_t* mask, int32_t* status,
                           int32_t* stats);

@@ -910,6 +910,14 @@ __device__ __forceinline__ void bdf_run(const LaunchArgs& A)
                 c.y[j] = A.y[(int64_t)j * stride + cell];
             c.t = A.t[cell];
             c.h = A.dt[cell];
+            if (A.save_y) {
+                /* the inputs, for the FP32-LU form's escalation */
+#pragma unroll
+                for (int j = 0; j < N; ++j)
+                    A.save_y[(int64_t)j * ncells + cell] = c.y[j];
+                A.save_t[cell] = c.t;
+                A.save_dt[cell] = c.h;
+            }
             c.tstop = A.t_stop[cell];
             c.msk = A.mask ? (A.mask[cell] != 0) : true;
             c.status = OV_OK;

@@ -442,6 +442,7 @@ static int32_t solve_impl(odevec_solver* s, int64_t ncells, int64_t stride, doub
     a.ws = ws;
     a.resume = resume;
     a.run_if = nullptr;
+    a.save_y = a.save_t = a.save_dt = nullptr;
     cudaStream_t st = (cudaStream_t)stream;
     cudaError_t err = cudaMemsetAsync(s->d_queue, 0, sizeof(unsigned long long), st);
     if (err != cudaSuccess)
@@ -471,14 +472,12 @@ static int32_t solve_impl(odevec_solver* s, int64_t ncells, int64_t stride, doub
                 return fail(OV_API_ENOMEM, "odevec_solve: escalation buffers: %s", cudaGetErrorString(err));
             s->fb_cells = ncells;
         }
-        const size_t n = (size_t)ncells;
-        err = stride == ncells
-                  ? cudaMemcpyAsync(s->fb_y, y, sizeof(double) * n * neq, cudaMemcpyDeviceToDevice, st)
-                  : cudaMemcpy2DAsync(s->fb_y, sizeof(double) * n, y, sizeof(double) * (size_t)stride,
-                                      sizeof(double) * n, neq, cudaMemcpyDeviceToDevice, st);
-        if (err == cudaSuccess) err = cudaMemcpyAsync(s->fb_t, t, sizeof(double) * n, cudaMemcpyDeviceToDevice, st);
-        if (err == cudaSuccess) err = cudaMemcpyAsync(s->fb_dt, dt, sizeof(double) * n, cudaMemcpyDeviceToDevice, st);
-        if (err == cudaSuccess) err = cudaMemsetAsync(s->d_queue + 1, 0, sizeof(unsigned long long), st);
+        /* the kernel saves each cell's inputs as it loads them (packed by
+           ncells), so the inputs are read once, wherever they live */
+        a.save_y = s->fb_y;
+        a.save_t = s->fb_t;
+        a.save_dt = s->fb_dt;
+        err = cudaMemsetAsync(s->d_queue + 1, 0, sizeof(unsigned long long), st);
         if (err != cudaSuccess)
             return fail(OV_API_ECUDA, "odevec_solve: %s", cudaGetErrorString(err));
         if (!a.status)
@@ -496,6 +495,7 @@ static int32_t solve_impl(odevec_solver* s, int64_t ncells, int64_t stride, doub
             b.mask = s->fb_mask;
             b.stats = nullptr;
             b.run_if = s->d_queue + 1;
+            b.save_y = b.save_t = b.save_dt = nullptr;
             err = cudaMemsetAsync(s->d_queue, 0, sizeof(unsigned long long), st);
             /* the FP64 re-solve runs rarely and only for failed cells: it
                uses the thread-local staging compiled for every variant (some
@@ -511,6 +511,32 @@ static int32_t solve_impl(odevec_solver* s, int64_t ncells, int64_t stride, doub
     if (err != cudaSuccess)
         return fail(OV_API_ECUDA, "odevec_solve launch: %s", cudaGetErrorString(err));
     return OV_API_OK;
+}
+
+/* The device address of host array p of `bytes` bytes when it is pinned and
+   mapped into the device's address space (cudaHostAlloc, or cudaHostRegister
+   with mapping), so that a kernel reads and writes it in place; else null.
+   Both ends are checked: an array lies inside one allocation. */
+static void* mapped_host(const void* p, size_t bytes)
+{
+    if (!p || bytes == 0)
+        return nullptr;
+    cudaPointerAttributes a0, a1;
+    if (cudaPointerGetAttributes(&a0, p) != cudaSuccess) {
+        cudaGetLastError();
+        return nullptr;
+    }
+    if (a0.type != cudaMemoryTypeHost || !a0.devicePointer)
+        return nullptr;
+    const char* last = static_cast<const char*>(p) + bytes - 1;
+    if (cudaPointerGetAttributes(&a1, last) != cudaSuccess) {
+        cudaGetLastError();
+        return nullptr;
+    }
+    if (a1.type != cudaMemoryTypeHost
+        || static_cast<const char*>(a1.devicePointer) != static_cast<const char*>(a0.devicePointer) + bytes - 1)
+        return nullptr;
+    return a0.devicePointer;
 }
 
 int32_t odevec_solve_host(odevec_solver* s, int64_t ncells, double* y, double* t, double* dt,
@@ -531,24 +557,44 @@ int32_t odevec_solve_host(odevec_solver* s, int64_t ncells, double* y, double* t
     const size_t n = (size_t)ncells;
     cudaStream_t st = s->stream;
     cudaError_t e = cudaSetDevice(s->device);
-    /* one copy per array; y is contiguous [neq][ncells] */
-    if (e == cudaSuccess) e = cudaMemcpyAsync(s->d_y, y, sizeof(double) * n * neq, cudaMemcpyHostToDevice, st);
-    if (e == cudaSuccess) e = cudaMemcpyAsync(s->d_t, t, sizeof(double) * n, cudaMemcpyHostToDevice, st);
-    if (e == cudaSuccess) e = cudaMemcpyAsync(s->d_dt, dt, sizeof(double) * n, cudaMemcpyHostToDevice, st);
-    if (e == cudaSuccess) e = cudaMemcpyAsync(s->d_tstop, t_stop, sizeof(double) * n, cudaMemcpyHostToDevice, st);
-    if (e == cudaSuccess && mask) e = cudaMemcpyAsync(s->d_mask, mask, n, cudaMemcpyHostToDevice, st);
+    if (e != cudaSuccess)
+        return fail(OV_API_ECUDA, "odevec_solve_host: %s", cudaGetErrorString(e));
+    /* An array in pinned, mapped host memory is read and written by the
+       kernel in place: a cell's inputs are read when the cell is set up and
+       its results written when it finishes, so those transfers overlap the
+       solve.  Any other array goes through the solver's device buffer, one
+       copy each way; y is contiguous [neq][ncells]. */
+    const size_t yb = sizeof(double) * n * neq, vb = sizeof(double) * n;
+    double* my = static_cast<double*>(mapped_host(y, yb));
+    double* mt = static_cast<double*>(mapped_host(t, vb));
+    double* mdt = static_cast<double*>(mapped_host(dt, vb));
+    const double* mts = static_cast<const double*>(mapped_host(t_stop, vb));
+    const uint8_t* mm = mask ? static_cast<const uint8_t*>(mapped_host(mask, n)) : nullptr;
+    int32_t* mst = status ? static_cast<int32_t*>(mapped_host(status, sizeof(int32_t) * n)) : nullptr;
+    int32_t* msa = stats ? static_cast<int32_t*>(mapped_host(stats, sizeof(int32_t) * n * OV_NSTATS)) : nullptr;
+    double* ky = my ? my : s->d_y;
+    double* kt = mt ? mt : s->d_t;
+    double* kdt = mdt ? mdt : s->d_dt;
+    const double* kts = mts ? mts : s->d_tstop;
+    const uint8_t* km = mask ? (mm ? mm : s->d_mask) : nullptr;
+    int32_t* kst = mst ? mst : s->d_status;
+    int32_t* ksa = stats ? (msa ? msa : s->d_stats) : nullptr;
+    if (!my) e = cudaMemcpyAsync(s->d_y, y, yb, cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess && !mt) e = cudaMemcpyAsync(s->d_t, t, vb, cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess && !mdt) e = cudaMemcpyAsync(s->d_dt, dt, vb, cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess && !mts) e = cudaMemcpyAsync(s->d_tstop, t_stop, vb, cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess && mask && !mm) e = cudaMemcpyAsync(s->d_mask, mask, n, cudaMemcpyHostToDevice, st);
     if (e != cudaSuccess)
         return fail(OV_API_ECUDA, "odevec_solve_host copy-in: %s", cudaGetErrorString(e));
-    int32_t rc = odevec_solve(s, ncells, s->d_y, s->d_t, s->d_dt, s->d_tstop, mask ? s->d_mask : nullptr,
-                              s->d_status, stats ? s->d_stats : nullptr, st);
+    int32_t rc = odevec_solve(s, ncells, ky, kt, kdt, kts, km, kst, ksa, st);
     if (rc)
         return rc;
-    e = cudaMemcpyAsync(y, s->d_y, sizeof(double) * n * neq, cudaMemcpyDeviceToHost, st);
-    if (e == cudaSuccess) e = cudaMemcpyAsync(t, s->d_t, sizeof(double) * n, cudaMemcpyDeviceToHost, st);
-    if (e == cudaSuccess) e = cudaMemcpyAsync(dt, s->d_dt, sizeof(double) * n, cudaMemcpyDeviceToHost, st);
-    if (e == cudaSuccess && status)
+    if (!my) e = cudaMemcpyAsync(y, s->d_y, yb, cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess && !mt) e = cudaMemcpyAsync(t, s->d_t, vb, cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess && !mdt) e = cudaMemcpyAsync(dt, s->d_dt, vb, cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess && status && !mst)
         e = cudaMemcpyAsync(status, s->d_status, sizeof(int32_t) * n, cudaMemcpyDeviceToHost, st);
-    if (e == cudaSuccess && stats)
+    if (e == cudaSuccess && stats && !msa)
         e = cudaMemcpyAsync(stats, s->d_stats, sizeof(int32_t) * n * OV_NSTATS, cudaMemcpyDeviceToHost, st);
     if (e == cudaSuccess)
         e = cudaStreamSynchronize(st);
@@ -787,6 +833,7 @@ extern "C" int32_t odevec_solve_noalloc(const char* network, const odevec_opts* 
     a.ws = nullptr;
     a.resume = 0;
     a.run_if = nullptr;
+    a.save_y = a.save_t = a.save_dt = nullptr;
     const NetEntry& e = g_nets[ni];
     const int lu = o.precision == OV_PREC_FP32_LU ? 1 : 0;
     ov::launch_fn fn = o.precision == OV_PREC_FP64 ? e.exact : e.fma;

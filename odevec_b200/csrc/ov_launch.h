@@ -41,6 +41,13 @@ struct LaunchArgs {
     /* if non-null, the kernel returns at once unless *run_if != 0 (a count
        written by an earlier kernel on the same stream) */
     const unsigned long long* run_if;
+    /* if non-null, every cell's inputs y (all species), t and dt are copied
+       here as the cell is loaded ([neq][ncells], [ncells], [ncells], packed):
+       the FP32-LU form's escalation restores failed cells from them, without
+       a separate copy of the inputs (which may be host memory) */
+    double* save_y;
+    double* save_t;
+    double* save_dt;
 };
 
 /* Several solves of different networks in one launch (the multi-network

@@ -809,11 +809,18 @@ __global__ void __launch_bounds__(256, (WpcLayout<Net, LUT, K>::MINB)) wpc_kerne
         if (cell >= ncells)
             break;
         __syncwarp(c.gmask);
-        for (int s = sub; s < N; s += K)
+        for (int s = sub; s < N; s += K) {
             c.yv[s] = A.y[(int64_t)s * A.stride + cell];
+            if (A.save_y) /* the inputs, for the FP32-LU form's escalation */
+                A.save_y[(int64_t)s * ncells + cell] = c.yv[s];
+        }
         __syncwarp(c.gmask);
         c.t = A.t[cell];
         c.h = A.dt[cell];
+        if (A.save_y && sub == 0) {
+            A.save_t[cell] = c.t;
+            A.save_dt[cell] = c.h;
+        }
         c.tstop = A.t_stop[cell];
         c.msk = A.mask ? (A.mask[cell] != 0) : true;
         c.status = OV_OK;

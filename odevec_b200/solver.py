@@ -263,7 +263,7 @@ def Workspace(ode: Odevec, ncells: int, device=None):
 
 
 def SolveODE(ode: Odevec, time, dt, t_stop, y, Mask=None, stream=None, want_stats=True,
-             workspace=None, resume=False):
+             workspace=None, resume=False, in_place=False):
     """Integrates every cell from ``time`` to ``t_stop`` (src/odevec.F90:158-214).
 
     ``y``: species-major storage of ``ncells x neq`` values: a torch CUDA
@@ -278,6 +278,12 @@ def SolveODE(ode: Odevec, time, dt, t_stop, y, Mask=None, stream=None, want_stat
     True/1 continues from the saved state; ``"en_old"``/2 starts fresh but
     keeps the previous call's last Newton correction, as the reference's
     solver object does between SolveODE calls (this%en_old is never reset).
+
+    NumPy arrays go through ``odevec_solve_host``; those in pinned host
+    memory are read and written by the kernel in place (no copies).
+    ``in_place`` (NumPy only): ``time`` and ``dt`` are per-cell float64
+    arrays updated in place, as the Fortran SolveODE's intent(inout)
+    arguments are, instead of returned copies.
     """
     resume_code = {False: 0, True: 1, 2: 2, "en_old": 2}[resume]
     h = ode.handle
@@ -329,8 +335,16 @@ def SolveODE(ode: Odevec, time, dt, t_stop, y, Mask=None, stream=None, want_stat
         raise ValueError("y must be a C-contiguous float64 NumPy array or a CUDA tensor")
     if ncells > ode.max_cells:
         raise ValueError("ncells %d > max_cells %d given at InitOdevec" % (ncells, ode.max_cells))
-    t = _as_cells(time, ncells, "time").copy()
-    d = _as_cells(dt, ncells, "dt").copy()
+    if in_place:
+        for a, nm in ((time, "time"), (dt, "dt")):
+            if not (isinstance(a, np.ndarray) and a.dtype == np.float64 and a.flags.c_contiguous
+                    and a.flags.writeable and a.shape == (ncells,)):
+                raise ValueError("in_place needs %s as a writable C-contiguous float64 array of %d cells"
+                                 % (nm, ncells))
+        t, d = time, dt
+    else:
+        t = _as_cells(time, ncells, "time").copy()
+        d = _as_cells(dt, ncells, "dt").copy()
     ts = _as_cells(t_stop, ncells, "t_stop")
     m = None if Mask is None else np.ascontiguousarray(Mask, dtype=np.uint8)
     status = np.zeros(ncells, np.int32)

@@ -117,6 +117,64 @@ def test_host_entry_point_matches_device(gpu_lib, oracle):
     assert_bitwise(g, o, "host path")
 
 
+def _pinned(a, keep):
+    """A copy of NumPy array a in pinned (page-locked, mapped) host memory."""
+    import torch
+    dt = {np.dtype(np.float64): torch.float64, np.dtype(np.uint8): torch.uint8}[a.dtype]
+    buf = torch.empty(a.shape, dtype=dt).pin_memory()
+    keep.append(buf)
+    x = buf.numpy()
+    x[...] = a
+    return x
+
+
+@pytest.mark.parametrize("precision,max_attempts", [("fp64", 0), ("fp32_lu", 0), ("fp32_lu", 5)])
+def test_host_entry_point_pinned_arrays_in_place(gpu_lib, oracle, precision, max_attempts):
+    """odevec_solve_host with y, time, dt, t_stop and mask in pinned host
+    memory: the kernel reads and writes them in place (no copies), with the
+    results of the copy path.  With max_attempts 5 every FP32-LU cell fails, is
+    restored from the inputs the kernel saved as it loaded them, and is
+    solved again in FP64 (the fp64_fma form): the results are that form's."""
+    S = gpu_lib
+    wl = W.primordial(ncells=300, network="PRIMORDIAL_CSC_FF")
+    mask = (np.arange(300) % 7 != 3).astype(np.uint8)
+    keep = []
+
+    def solve(prec, pinned):
+        ode = S.Odevec(wl.network, max_cells=wl.ncells, RelativeTolerance=wl.rtol, AbsoluteTolerance=wl.atol,
+                       MinimalTimestep=wl.dt_min, nvector=1, precision=prec, raise_on_failure=False,
+                       max_attempts=max_attempts)
+        S.InitOdevec(ode)
+        try:
+            y = _pinned(wl.y, keep) if pinned else wl.y.copy()
+            ts = _pinned(wl.t_stop, keep) if pinned else wl.t_stop.copy()
+            m = _pinned(mask, keep) if pinned else mask.copy()
+            if pinned:  # time and dt pinned too, updated in place
+                t0, d0 = _pinned(wl.t0, keep), _pinned(wl.dt0, keep)
+                t, d = S.SolveODE(ode, t0, d0, ts, y, Mask=m, in_place=True)
+                assert t is t0 and d is d0
+            else:
+                t, d = S.SolveODE(ode, wl.t0, wl.dt0, ts, y, Mask=m)
+            return y.copy(), t.copy(), d.copy(), ode.status.copy(), ode.stats.copy()
+        finally:
+            S.CloseOdevec(ode)
+
+    pinned = solve(precision, True)
+    assert_bitwise(pinned, solve(precision, False), "pinned vs pageable host arrays")
+    if precision == "fp64":
+        assert_bitwise(pinned, run_oracle(oracle, wl, mask=mask), "pinned host arrays vs oracle")
+    if max_attempts:
+        # all but the few cells that finish within 5 attempts end with
+        # MAX_STEPS after the FP64 re-solve too, and equal the fp64_fma form
+        failed = pinned[3] == 4
+        assert failed.sum() >= 250 and not np.any(failed & (mask == 0))
+        fma = solve("fp64_fma", True)
+        assert np.array_equal(fma[3][failed], pinned[3][failed])
+        assert np.array_equal(pinned[0][:, failed], fma[0][:, failed])
+        assert np.array_equal(pinned[1][failed], fma[1][failed])
+        assert np.array_equal(pinned[2][failed], fma[2][failed])
+
+
 def _relerr(a, b, floor):
     m = np.abs(b) > floor
     return np.max(np.abs(a[m] - b[m]) / np.abs(b[m])) if np.any(m) else 0.0
