@@ -199,6 +199,10 @@ template <> struct StageCfg<12> { static constexpr int SHM = 2; static constexpr
    solver species, whose arrays live in local memory either way */
 template <> struct StageCfg<15> { static constexpr int SHM = 0; static constexpr bool SOFT = true;  static constexpr int BS = 256, MINB = 1, REFILL = 16, PERIOD = 4; };
 template <> struct StageCfg<16> { static constexpr int SHM = 0; static constexpr bool SOFT = true;  static constexpr int BS = 512, MINB = 1, REFILL = 16, PERIOD = 4; };
+/* as 12, idle lanes refilled on every 32nd trip only (fewer, larger cell
+   set-ups; measured on PRIMORDIAL: 1.6 % faster with FP32 factors, 4.5 %
+   slower in FP64) */
+template <> struct StageCfg<17> { static constexpr int SHM = 2; static constexpr bool SOFT = true;  static constexpr int BS = 384, MINB = 1, REFILL = 32, PERIOD = 4; };
 
 /* Soft lockstep.  The warps of a block wait for each other at the top of
    every trip of the cell loop, so they run the same phase code at the same
@@ -1384,9 +1388,10 @@ constexpr bool hist_fits_max()
    memory; 11 = soft lockstep in one block of 192 with history and LU in
    shared memory (where they fit); 12 = as 9 in one block of 384; 13, 14 =
    16 or 8 lanes per cell (wpc_kernel.cuh, as 7); 15, 16 = as 8 in one block
-   of 256 or 512 (networks above 32 solver species).  With per-cell control
-   stagings 2-6 and 8-16 refill idle lanes on every 16th trip, staging 1 on
-   every trip.  Stages 2-16 exist for per-cell control (G = 1). */
+   of 256 or 512 (networks above 32 solver species); 17 = as 12 refilling on
+   every 32nd trip.  With per-cell control stagings 2-6 and 8-16 refill idle
+   lanes on every 16th trip, 17 on every 32nd, staging 1 on every trip.
+   Stages 2-17 exist for per-cell control (G = 1). */
 #define OV_STAGE_CASE(NET, LU, ST)                                                               \
     if (stage == ST)                                                                             \
         return launch<NET, 1, LU, ST>(a, block, grid, s);
@@ -1435,6 +1440,7 @@ constexpr bool hist_fits_max()
             }                                                                                    \
             if constexpr (hist_fits_max<NET, 384>()) {                                           \
                 OV_STAGE_CASE(NET, double, 12)                                                   \
+                OV_STAGE_CASE(NET, double, 17)                                               \
             }                                                                                    \
             if constexpr (shm_fits<NET, double, 192>()) {                                        \
                 OV_STAGE_CASE(NET, double, 11)                                                   \
@@ -1475,6 +1481,7 @@ constexpr bool hist_fits_max()
                 }                                                                                \
                 if constexpr (hist_fits_max<NET, 384>()) {                                       \
                     OV_STAGE_CASE(NET, float, 12)                                                \
+                    OV_STAGE_CASE(NET, float, 17)                                            \
                 }                                                                                \
                 if constexpr (shm_fits<NET, float, 192>()) {                                     \
                     OV_STAGE_CASE(NET, float, 11)                                                \
