@@ -200,8 +200,9 @@ template <> struct StageCfg<12> { static constexpr int SHM = 2; static constexpr
 template <> struct StageCfg<15> { static constexpr int SHM = 0; static constexpr bool SOFT = true;  static constexpr int BS = 256, MINB = 1, REFILL = 16, PERIOD = 4; };
 template <> struct StageCfg<16> { static constexpr int SHM = 0; static constexpr bool SOFT = true;  static constexpr int BS = 512, MINB = 1, REFILL = 16, PERIOD = 4; };
 /* as 12, idle lanes refilled on every 32nd trip only (fewer, larger cell
-   set-ups; measured on PRIMORDIAL: 1.6 % faster with FP32 factors, 4.5 %
-   slower in FP64) */
+   set-ups; measured on PRIMORDIAL's long solves: 1.6 % faster with FP32
+   factors, 4.5 % slower in FP64; slower on short operator-split solves,
+   whose lanes then wait longer for new cells) */
 template <> struct StageCfg<17> { static constexpr int SHM = 2; static constexpr bool SOFT = true;  static constexpr int BS = 384, MINB = 1, REFILL = 32, PERIOD = 4; };
 
 /* Soft lockstep.  The warps of a block wait for each other at the top of
@@ -1252,7 +1253,11 @@ __global__ void __launch_bounds__(StageCfg<STAGE>::BS, StageCfg<STAGE>::MINB)
 }
 
 /* ---- several networks in one launch ---------------------------------- */
-constexpr int MULTI_STAGE = 3; /* thread-local arrays, three 128-thread blocks per SM */
+/* thread-local arrays, one 384-thread block per SM in soft lockstep: the
+   register budget of staging 3, without the instruction-fetch stalls of a
+   large network's code (SYN64: 1.35x over staging 1); every warp of a block
+   runs the same job at a time, so the lockstep keeps them on the same code */
+constexpr int MULTI_STAGE = 8;
 
 template <class LUT, class... Nets>
 struct MultiDispatch {

@@ -265,8 +265,8 @@ def run_schedule(sch: Schedule, precision: str = "fp64", graph: bool = False, ch
 
 def main(argv=None):
     """python -m odevec_b200.driver --schedule rober|orego|primordial [--cells N]
-    [--graph] [--precision P]: runs a reference driver's ladder and prints the
-    wall time per call."""
+    [--graph] [--precision P] [--staging S]: runs a reference driver's ladder
+    and prints the wall time per call."""
     import argparse
     import json
     import time
@@ -278,6 +278,7 @@ def main(argv=None):
     p.add_argument("--chunk", type=int, default=64)
     p.add_argument("--precision", default="fp64")
     p.add_argument("--t-end", type=float, default=360.0, help="OREGO ladder end")
+    p.add_argument("--staging", type=int, default=0, help="launch shape (0: the tuning table)")
     a = p.parse_args(argv)
     if a.schedule == "rober":
         sch = rober_schedule(a.cells)
@@ -286,7 +287,7 @@ def main(argv=None):
     else:
         sch = primordial_schedule(a.cells)
     ode = S.Odevec(sch.network, RelativeTolerance=sch.rtol, AbsoluteTolerance=sch.atol, MinimalTimestep=sch.dt_min,
-                   nvector=sch.group, precision=a.precision, raise_on_failure=False)
+                   nvector=sch.group, precision=a.precision, raise_on_failure=False, staging=a.staging)
     S.InitOdevec(ode)
     y0 = torch.tensor(sch.y0, device="cuda")
     y = y0.clone()
@@ -306,7 +307,7 @@ def main(argv=None):
     st = st.cpu().numpy()
     S.CloseOdevec(ode)
     print(json.dumps({"schedule": a.schedule, "network": sch.network, "cells": a.cells, "calls": len(sch.t_stops),
-                      "graph": a.graph, "precision": a.precision, "seconds": el,
+                      "graph": a.graph, "precision": a.precision, "staging": a.staging, "seconds": el,
                       "ms_per_call": 1e3 * el / len(sch.t_stops), "failed_cells": int((st != 0).sum())}))
 
 
