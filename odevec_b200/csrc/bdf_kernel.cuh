@@ -295,10 +295,14 @@ struct Cell {
     static constexpr bool SCALED = sizeof(LUT) == 4;
 
     typename Staging<Net, LUT, SHM, BS>::Hist yns; /* Nordsieck history y_NS(0:5) */
-    double en[ND], eno[ND], w2[ND];
-    double y[N];
+    /* 16-byte aligned, so that neighbouring entries can move in one 128-bit
+       access when the arrays live in local memory */
+    alignas(16) double en[ND];
+    alignas(16) double eno[ND];
+    alignas(16) double w2[ND];
+    alignas(16) double y[N];
     typename Staging<Net, LUT, SHM, BS>::LU a; /* packed LU of the iteration matrix */
-    double rT[NR];
+    alignas(16) double rT[NR];
     /* FP32 LU: the scale of species j is 2^sce[j] (kept as an exponent, the
        factors are formed only while the Jacobian and the solve run) */
     short sce[SCALED ? ND : 1];
@@ -846,8 +850,8 @@ __device__ __forceinline__ void bdf_run(const LaunchArgs& A)
             c.a = LaneCol<LUT, BS>{reinterpret_cast<LUT*>(ov_smem + Staging<Net, LUT, 1, BS>::hist_bytes)
                                    + threadIdx.x};
     }
-    double history[SHM != 0 ? 1 : MAXQ + 1][ND];
-    LUT lu_local[SHM == 1 ? 1 : C::NNZ];
+    alignas(16) double history[SHM != 0 ? 1 : MAXQ + 1][ND];
+    alignas(16) LUT lu_local[SHM == 1 ? 1 : C::NNZ];
     if constexpr (SHM == 0)
         c.yns = history;
     if constexpr (SHM != 1)
