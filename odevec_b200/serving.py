@@ -338,14 +338,15 @@ def make_stream(seed: int = 5, rate: float = 200.0, duration: float = 1.0,
 def measure(rate: float = 200.0, duration: float = 0.25, steps: int = 50, cells=(1000, 262144),
             dt_hydro=(1e6, 1e11), networks=("ROBER_DENSE_NONE", "PRIMORDIAL_CSC_FF", "SYN64_CSC_CMK"),
             precisions=("fp32_lu", "fp64"), budget: float = 120e9, slots: int = 16, seed: int = 5,
-            isolated: bool = False, fair_share: bool = True, chunk_cells: int = 0) -> List[dict]:
+            isolated: bool = False, fair_share: bool = True, chunk_cells: int = 0,
+            staging: int = 3) -> List[dict]:
     """Runs a Poisson request stream through the scheduler on the GPU, per
     precision form; with isolated, every request is run again alone and the
     mix's step latencies are compared with the isolated ones."""
     reqs = make_stream(seed, rate, duration, tuple(networks), tuple(cells), tuple(dt_hydro), steps)
     outs = []
     for prec in precisions:
-        be = GpuBackend(prec, fair_share=fair_share, chunk_cells=chunk_cells)
+        be = GpuBackend(prec, fair_share=fair_share, chunk_cells=chunk_cells, staging=staging)
         # warm-up: one small request per network (module load, first launches)
         warm = [Request(10**6 + i, r.network, r.y0[:, :64].copy(), r.dt_hydro, 1, 0.0, r.rtol, r.atol,
                         r.dt_min, r.dt_in) for i, r in enumerate({r.network: r for r in reqs}.values())]
@@ -354,6 +355,7 @@ def measure(rate: float = 200.0, duration: float = 0.25, steps: int = 50, cells=
         mix = summarize(recs, res)
         offered = sum(r.ncells * r.steps for r in reqs) / duration
         out = {"form": prec, "requests": len(reqs), "rate": rate, "steps": steps, "chunk_cells": chunk_cells,
+               "staging": staging,
                "cells": list(cells), "dt_hydro": list(dt_hydro), "seed": seed,
                "budget_gb": budget / 1e9, "slots": slots, "fair_share": fair_share,
                "mix": mix,
@@ -415,10 +417,11 @@ def main(argv=None):
                    help="every launch may take the whole device (no 1/k block share, one stream priority)")
     p.add_argument("--chunk-cells", type=int, default=0,
                    help="launch a larger request's step as ranges of at most this many cells (0: whole)")
+    p.add_argument("--staging", type=int, default=3, help="launch shape of every request's solves")
     a = p.parse_args(argv)
     for out in measure(a.rate, a.duration, a.steps, (a.min_cells, a.max_cells), (a.dt_min, a.dt_max),
                        a.networks.split(","), a.precisions.split(","), a.budget, a.slots, a.seed,
-                       a.isolated, not a.no_fair_share, a.chunk_cells):
+                       a.isolated, not a.no_fair_share, a.chunk_cells, a.staging):
         print(json.dumps(out), flush=True)
 
 
