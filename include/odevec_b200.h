@@ -199,6 +199,28 @@ int32_t odevec_solve_range(odevec_solver* s, int64_t ncells, int64_t stride, dou
                            double* dt, const double* t_stop, const uint8_t* mask, int32_t* status,
                            int32_t* stats, double* workspace, int32_t resume, void* stream);
 
+/* Interruptible solves, no counterpart in the reference: a serving loop
+   lets a short request start while a long launch runs.
+   odevec_set_yield(s, flag): the kernels of s's later solves read *flag
+   (int32 in device memory -- set it with a small cudaMemcpyAsync on another
+   stream, which the copy engine runs while the kernel holds the SMs; pinned
+   host memory mapped into the device works too but made a PRIMORDIAL solve
+   3x slower; NULL: none) whenever idle cells would take new work, except on
+   a launch's first such occasion.  While it is nonzero they start no new cell, and the
+   launch ends once the cells it runs are done; the others are untouched.
+   odevec_cells_started(s, stream, &n) synchronises `stream` and reads how
+   many cells the solve has started (n >= ncells: all of them; n may exceed
+   ncells).  odevec_solve_continue takes odevec_solve_range's arguments
+   (the same arrays as the solve it continues) and starts the cells not yet
+   started.  With OV_PREC_FP32_LU the escalation of failed cells runs after
+   the launch that completes the solve.  Results are those of one
+   uninterrupted solve: every cell runs once, on its own. */
+int32_t odevec_set_yield(odevec_solver* s, const int32_t* flag);
+int32_t odevec_solve_continue(odevec_solver* s, int64_t ncells, int64_t stride, double* y, double* t,
+                              double* dt, const double* t_stop, const uint8_t* mask, int32_t* status,
+                              int32_t* stats, double* workspace, int32_t resume, void* stream);
+int32_t odevec_cells_started(odevec_solver* s, void* stream, int64_t* started);
+
 /* The operator-split caller's format (tests/primordial.f90:79-87, 113-140):
    the hydro code keeps mass fractions x and the gas density rho (g/cm^3) per
    cell; the network integrates number densities n (1/cm^3).  direction

@@ -881,8 +881,19 @@ __device__ __forceinline__ void bdf_run(const LaunchArgs& A)
                runs for several lanes and warps at once instead of stretching
                trip after trip for one lane */
             const bool refill = StageCfg<STAGE>::REFILL <= 1 || trip % StageCfg<STAGE>::REFILL == 0u;
+            /* a yield request, seen on a refill trip after the first (so
+               that every launch starts cells), turns the idle lanes into
+               exhausted ones: the warp leaves once its running cells end */
+            int stop = 0;
+            if (refill && trip > 0u && A.yield) {
+                if (lane == 0)
+                    stop = *(volatile const int32_t*)A.yield;
+                stop = __shfl_sync(FULL, stop, 0);
+            }
             ++trip;
-            const unsigned need = refill ? __ballot_sync(FULL, ph == PH_IDLE) : 0u;
+            if (stop && ph == PH_IDLE)
+                ph = PH_EXHAUSTED;
+            const unsigned need = refill && !stop ? __ballot_sync(FULL, ph == PH_IDLE) : 0u;
             if (need) {
                 const int leader = __ffs(need) - 1;
                 unsigned long long base = 0;
@@ -901,12 +912,23 @@ __device__ __forceinline__ void bdf_run(const LaunchArgs& A)
             }
         } else {
             if (ph == PH_IDLE) { /* warp-uniform */
-                unsigned long long g = 0;
-                if (lane == 0)
-                    g = atomicAdd(A.queue, 1ull);
-                g = __shfl_sync(FULL, g, 0);
-                cell = (int64_t)g * 32 + lane;
-                ph = (int64_t)g * 32 < ncells ? PH_START : PH_EXHAUSTED;
+                int stop = 0;
+                if (trip > 0u && A.yield) { /* yield requests as above */
+                    if (lane == 0)
+                        stop = *(volatile const int32_t*)A.yield;
+                    stop = __shfl_sync(FULL, stop, 0);
+                }
+                ++trip;
+                if (stop) {
+                    ph = PH_EXHAUSTED;
+                } else {
+                    unsigned long long g = 0;
+                    if (lane == 0)
+                        g = atomicAdd(A.queue, 1ull);
+                    g = __shfl_sync(FULL, g, 0);
+                    cell = (int64_t)g * 32 + lane;
+                    ph = (int64_t)g * 32 < ncells ? PH_START : PH_EXHAUSTED;
+                }
             }
             if (ph == PH_EXHAUSTED)
                 break;

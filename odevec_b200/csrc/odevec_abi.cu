@@ -169,7 +169,11 @@ struct odevec_solver {
     double *fb_y, *fb_t, *fb_dt;
     int32_t* fb_status;
     uint8_t* fb_mask;
+    /* odevec_set_yield: the kernels stop starting cells while *yield != 0 */
+    const int32_t* yield;
 };
+/* d_queue words: [0] the solve's work counter, [1] cells that failed with
+   FP32 factors, [2] the FP64 re-solve's work counter */
 
 namespace {
 /* cells whose FP32-LU solve failed get their inputs back and a retry mask;
@@ -202,8 +206,12 @@ __global__ void __launch_bounds__(256) ov_convert(int64_t ncells, int direction,
 __global__ void ov_escalate(int64_t ncells, int64_t stride, int neq, double* y, double* t, double* dt,
                             const double* y_in, const double* t_in, const double* dt_in,
                             const int32_t* status, const uint8_t* mask, uint8_t* retry,
-                            unsigned long long* nfail)
+                            unsigned long long* nfail, const unsigned long long* started)
 {
+    /* after a launch that yielded before starting every cell nothing is
+       final yet: the pass runs after the launch that completes the solve */
+    if (*started < (unsigned long long)ncells)
+        return;
     /* y rows have the launch's stride, the saved inputs y_in are packed */
     for (int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; c < ncells;
          c += (int64_t)gridDim.x * blockDim.x) {
@@ -358,7 +366,7 @@ int32_t odevec_set_options(odevec_solver* s, const odevec_opts* opts)
 
 static int32_t solve_impl(odevec_solver* s, int64_t ncells, int64_t stride, double* y, double* t,
                           double* dt, const double* t_stop, const uint8_t* mask, int32_t* status,
-                          int32_t* stats, double* ws, int32_t resume, void* stream);
+                          int32_t* stats, double* ws, int32_t resume, void* stream, bool cont = false);
 
 int32_t odevec_solve(odevec_solver* s, int64_t ncells, double* y, double* t, double* dt,
                      const double* t_stop, const uint8_t* mask, int32_t* status, int32_t* stats,
@@ -400,9 +408,42 @@ int32_t odevec_solve_range(odevec_solver* s, int64_t ncells, int64_t stride, dou
     return solve_impl(s, ncells, stride, y, t, dt, t_stop, mask, status, stats, workspace, resume, stream);
 }
 
+int32_t odevec_set_yield(odevec_solver* s, const int32_t* flag)
+{
+    if (!s)
+        return fail(OV_API_EINVAL, "solver is null");
+    s->yield = flag;
+    return OV_API_OK;
+}
+
+int32_t odevec_solve_continue(odevec_solver* s, int64_t ncells, int64_t stride, double* y, double* t, double* dt,
+                              const double* t_stop, const uint8_t* mask, int32_t* status, int32_t* stats,
+                              double* workspace, int32_t resume, void* stream)
+{
+    if (resume < 0 || resume > 2)
+        return fail(OV_API_EINVAL, "odevec_solve_continue: resume must be 0, 1 or 2 (got %d)", resume);
+    if (resume && !workspace)
+        return fail(OV_API_EINVAL, "odevec_solve_continue: resume needs a workspace");
+    return solve_impl(s, ncells, stride, y, t, dt, t_stop, mask, status, stats, workspace, resume, stream, true);
+}
+
+int32_t odevec_cells_started(odevec_solver* s, void* stream, int64_t* started)
+{
+    if (!s || !started)
+        return fail(OV_API_EINVAL, "solver or started is null");
+    unsigned long long v = 0;
+    cudaError_t e = cudaMemcpyAsync(&v, s->d_queue, sizeof v, cudaMemcpyDeviceToHost, (cudaStream_t)stream);
+    if (e == cudaSuccess)
+        e = cudaStreamSynchronize((cudaStream_t)stream);
+    if (e != cudaSuccess)
+        return fail(OV_API_ECUDA, "odevec_cells_started: %s", cudaGetErrorString(e));
+    *started = (int64_t)v;
+    return OV_API_OK;
+}
+
 static int32_t solve_impl(odevec_solver* s, int64_t ncells, int64_t stride, double* y, double* t,
                           double* dt, const double* t_stop, const uint8_t* mask, int32_t* status,
-                          int32_t* stats, double* ws, int32_t resume, void* stream)
+                          int32_t* stats, double* ws, int32_t resume, void* stream, bool cont)
 {
     if (!s)
         return fail(OV_API_EINVAL, "solver is null");
@@ -443,8 +484,11 @@ static int32_t solve_impl(odevec_solver* s, int64_t ncells, int64_t stride, doub
     a.resume = resume;
     a.run_if = nullptr;
     a.save_y = a.save_t = a.save_dt = nullptr;
+    a.yield = s->yield;
     cudaStream_t st = (cudaStream_t)stream;
-    cudaError_t err = cudaMemsetAsync(s->d_queue, 0, sizeof(unsigned long long), st);
+    /* a continuation keeps the work counter (and the failure count) of the
+       solve it continues */
+    cudaError_t err = cont ? cudaSuccess : cudaMemsetAsync(s->d_queue, 0, sizeof(unsigned long long), st);
     if (err != cudaSuccess)
         return fail(OV_API_ECUDA, "odevec_solve: %s", cudaGetErrorString(err));
     const int lu = o.precision == OV_PREC_FP32_LU ? 1 : 0;
@@ -458,6 +502,9 @@ static int32_t solve_impl(odevec_solver* s, int64_t ncells, int64_t stride, doub
         /* FP32 factors can be too inaccurate for a badly conditioned cell
            (Newton then fails until dt < dt_min): such cells are solved again
            from their inputs with FP64 factors */
+        if (cont && s->fb_cells < ncells)
+            return fail(OV_API_EINVAL, "odevec_solve_continue: no solve of %lld cells to continue",
+                        (long long)ncells);
         if (s->fb_cells < ncells) {
             cudaFree(s->fb_y); cudaFree(s->fb_t); cudaFree(s->fb_dt); cudaFree(s->fb_status); cudaFree(s->fb_mask);
             s->fb_y = nullptr; s->fb_t = nullptr; s->fb_dt = nullptr; s->fb_status = nullptr; s->fb_mask = nullptr;
@@ -477,7 +524,7 @@ static int32_t solve_impl(odevec_solver* s, int64_t ncells, int64_t stride, doub
         a.save_y = s->fb_y;
         a.save_t = s->fb_t;
         a.save_dt = s->fb_dt;
-        err = cudaMemsetAsync(s->d_queue + 1, 0, sizeof(unsigned long long), st);
+        err = cont ? cudaSuccess : cudaMemsetAsync(s->d_queue + 1, 0, sizeof(unsigned long long), st);
         if (err != cudaSuccess)
             return fail(OV_API_ECUDA, "odevec_solve: %s", cudaGetErrorString(err));
         if (!a.status)
@@ -488,7 +535,7 @@ static int32_t solve_impl(odevec_solver* s, int64_t ncells, int64_t stride, doub
         int blocks = 0;
         cudaDeviceGetAttribute(&blocks, cudaDevAttrMultiProcessorCount, s->device);
         ov_escalate<<<blocks * 4, 256, 0, st>>>(ncells, stride, neq, y, t, dt, s->fb_y, s->fb_t, s->fb_dt,
-                                                a.status, mask, s->fb_mask, s->d_queue + 1);
+                                                a.status, mask, s->fb_mask, s->d_queue + 1, s->d_queue);
         err = cudaGetLastError();
         if (err == cudaSuccess) {
             ov::LaunchArgs b = a;
@@ -496,7 +543,9 @@ static int32_t solve_impl(odevec_solver* s, int64_t ncells, int64_t stride, doub
             b.stats = nullptr;
             b.run_if = s->d_queue + 1;
             b.save_y = b.save_t = b.save_dt = nullptr;
-            err = cudaMemsetAsync(s->d_queue, 0, sizeof(unsigned long long), st);
+            b.yield = nullptr; /* the re-solve runs to the end */
+            b.queue = s->d_queue + 2;
+            err = cudaMemsetAsync(s->d_queue + 2, 0, sizeof(unsigned long long), st);
             /* the FP64 re-solve runs rarely and only for failed cells: it
                uses the thread-local staging compiled for every variant (some
                stagings exist for FP32 factors only) */
@@ -834,6 +883,7 @@ extern "C" int32_t odevec_solve_noalloc(const char* network, const odevec_opts* 
     a.resume = 0;
     a.run_if = nullptr;
     a.save_y = a.save_t = a.save_dt = nullptr;
+    a.yield = nullptr;
     const NetEntry& e = g_nets[ni];
     const int lu = o.precision == OV_PREC_FP32_LU ? 1 : 0;
     ov::launch_fn fn = o.precision == OV_PREC_FP64 ? e.exact : e.fma;

@@ -48,6 +48,13 @@ struct LaunchArgs {
     double* save_y;
     double* save_t;
     double* save_dt;
+    /* if non-null and nonzero when a warp (or lane group) is about to take
+       new cells -- on any refill trip after its first -- it takes none:
+       the launch ends once its running cells are done, the cells not
+       started stay untouched, and a later launch on the same work counter
+       continues with them (read with a volatile load: device memory or
+       pinned, mapped host memory) */
+    const int32_t* yield;
 };
 
 /* Several solves of different networks in one launch (the multi-network

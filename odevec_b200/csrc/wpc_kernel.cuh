@@ -801,7 +801,17 @@ __global__ void __launch_bounds__(256, (WpcLayout<Net, LUT, K>::MINB)) wpc_kerne
         c.isc[m] = 1.0;
     }
     const int64_t ncells = A.ncells;
-    for (;;) {
+    for (bool first_cell = true;; first_cell = false) {
+        /* a yield request (LaunchArgs::yield), seen before any cell but the
+           group's first of this launch, ends the group's work */
+        int stop = 0;
+        if (!first_cell && A.yield) {
+            if (sub == 0)
+                stop = *(volatile const int32_t*)A.yield;
+            stop = __shfl_sync(c.gmask, stop, c.glead);
+        }
+        if (stop)
+            break;
         unsigned long long g = 0;
         if (sub == 0)
             g = atomicAdd(A.queue, 1ull);

@@ -196,7 +196,7 @@ class GpuBackend:
     CUDA stream; launches are asynchronous and completion is an event."""
 
     def __init__(self, precision: str = "fp32_lu", device: str = "cuda", fair_share: bool = True,
-                 small_cells: int = 16384, staging: int = 3, chunk_cells: int = 0):
+                 small_cells: int = 16384, staging: int = 3, chunk_cells: int = 0, yield_to_small: bool = True):
         import torch
         from . import solver as S
         self.S = S
@@ -214,6 +214,20 @@ class GpuBackend:
         # at most this many cells, one after another on its stream, so that a
         # short request arriving meanwhile waits for one range, not the step
         self.chunk_cells = chunk_cells
+        # yield_to_small: a large request's launch stops starting cells when a
+        # new small request arrives (odevec_set_yield), ends once its running
+        # cells are done, and is continued from its work counter when that
+        # launch has completed (odevec_solve_continue).  The flag is a device
+        # word (a flag in pinned host memory made the solve 3x slower), set
+        # by a 4-byte copy on a control stream: the copy engine runs it while
+        # the large launch holds every SM.
+        self.yield_to_small = yield_to_small and not chunk_cells
+        self.live: Dict[int, dict] = {}
+        if self.yield_to_small:
+            lo, hi = torch.cuda.Stream.priority_range()
+            self._ctrl = torch.cuda.Stream(device=device, priority=hi)
+            self._one = torch.ones(1, dtype=torch.int32).pin_memory()
+            self._zero = torch.zeros(1, dtype=torch.int32).pin_memory()
         self.sms = torch.cuda.get_device_properties(device).multi_processor_count
 
     def _solver(self, r: Request):
@@ -243,8 +257,31 @@ class GpuBackend:
                  "ws": self.S.Workspace(ode, r.ncells, self.device),
                  "failed": torch.zeros(r.ncells, dtype=torch.int32, device=self.device),
                  "mask": torch.ones(r.ncells, dtype=torch.uint8, device=self.device),
-                 "ev": None}
+                 "ev": None, "flag": None, "running": False}
+            if self.yield_to_small and r.ncells > self.small_cells:
+                h["flag"] = torch.zeros(1, dtype=torch.int32, device=self.device)
+                h["status"] = torch.zeros(r.ncells, dtype=torch.int32, device=self.device)
+                self.S.set_yield(ode, h["flag"])
+        self.live[r.rid] = h
         return h
+
+    def _launch_whole(self, h, step: int, cont: bool):
+        """A large request's step (or its continuation after a yield) as one
+        range launch over all its cells, with a persistent status array."""
+        torch = self.torch
+        r = h["r"]
+        with torch.cuda.stream(h["stream"]):
+            h["flag"].copy_(self._zero, non_blocking=True)
+            if not cont:
+                h["status"].zero_()
+            self.S.SolveODERange(h["ode"], 0, r.ncells, h["t"], h["dt"], h["ts"], h["y"], h["status"],
+                                 Mask=h["mask"], stream=h["stream"], workspace=h["ws"], resume=h["step"] > 0,
+                                 cont=cont)
+            torch.where(h["failed"] != 0, h["failed"], h["status"], out=h["failed"])
+            ev = torch.cuda.Event()
+            ev.record(h["stream"])
+            h["ev"] = ev
+            h["running"] = True
 
     def share(self, r, active, staging: int) -> int:
         """Blocks for a launch of request r among the requests in flight
@@ -270,10 +307,21 @@ class GpuBackend:
         r = h["r"]
         if self.fair_share:
             h["ode"].grid_blocks = self.share(r, active, h["ode"].staging)
+        if r.ncells <= self.small_cells and step == 0:
+            # a new small request: running large launches stop starting cells
+            # and continue, once done, with a share that counts it
+            with torch.cuda.stream(self._ctrl):
+                for o in self.live.values():
+                    if o is not h and o["flag"] is not None and o["running"]:
+                        o["flag"].copy_(self._one, non_blocking=True)
         with torch.cuda.stream(h["stream"]):
             h["ts"].fill_(r.dt_hydro * (step + 1))
             if step > 0:
                 h["mask"].copy_(h["failed"] == 0)
+            if h["flag"] is not None:
+                h["step"] = step
+                self._launch_whole(h, step, cont=False)
+                return
             if self.chunk_cells and r.ncells > self.chunk_cells:
                 if "status" not in h:
                     h["status"] = torch.empty(r.ncells, dtype=torch.int32, device=self.device)
@@ -294,10 +342,24 @@ class GpuBackend:
             h["ev"] = ev
 
     def finished(self, h) -> bool:
-        return h["ev"] is not None and h["ev"].query()
+        if h["ev"] is None or not h["ev"].query():
+            return False
+        if h["flag"] is not None and h["running"]:
+            h["running"] = False
+            if self.S.cells_started(h["ode"], h["stream"]) < h["r"].ncells:
+                # it yielded: start the rest with a share of the requests now in flight
+                if self.fair_share:
+                    h["ode"].grid_blocks = self.share(h["r"], [o["r"] for o in self.live.values()],
+                                                      h["ode"].staging)
+                self._launch_whole(h, h["step"], cont=True)
+                return False
+        return True
 
     def release(self, h):
         h["stream"].synchronize()
+        self.live.pop(h["r"].rid, None)
+        if h["flag"] is not None:
+            self.S.set_yield(h["ode"], None)
         res = Result(h["y"].cpu().numpy(), h["failed"].cpu().numpy())
         self.S.CloseOdevec(h["ode"])
         return res

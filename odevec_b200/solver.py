@@ -111,6 +111,12 @@ def lib():
         L.odevec_solve_range.restype = i32
         L.odevec_solve_many.argtypes = [ctypes.POINTER(_Job), i32, P]
         L.odevec_solve_many.restype = i32
+        L.odevec_set_yield.argtypes = [P, P]
+        L.odevec_set_yield.restype = i32
+        L.odevec_solve_continue.argtypes = [P, i64, i64, P, P, P, P, P, P, P, P, i32, P]
+        L.odevec_solve_continue.restype = i32
+        L.odevec_cells_started.argtypes = [P, P, ctypes.POINTER(i64)]
+        L.odevec_cells_started.restype = i32
         _lib = L
     return _lib
 
@@ -360,12 +366,14 @@ def SolveODE(ode: Odevec, time, dt, t_stop, y, Mask=None, stream=None, want_stat
 
 
 def SolveODERange(ode: Odevec, c0: int, c1: int, t, dt, t_stop, y, status, Mask=None, stream=None,
-                  workspace=None, resume=False):
+                  workspace=None, resume=False, cont=False):
     """SolveODE on cells [c0, c1) of full-size CUDA tensors (odevec_solve_range):
     y (neq, ncells), t, dt, t_stop, status (int32) and Mask (uint8, or None)
     with one entry per cell, workspace from :func:`Workspace` for all ncells
     (or None).  Only the range is read and written; a large solve cut into
-    ranges gives the results of the whole solve.  Asynchronous on `stream`."""
+    ranges gives the results of the whole solve.  Asynchronous on `stream`.
+    ``cont``: continue the previous call on the same range after it yielded
+    (odevec_solve_continue; see :func:`set_yield`)."""
     import torch
     ncells = int(y.shape[1])
     if not (0 <= c0 <= c1 <= ncells):
@@ -378,7 +386,29 @@ def SolveODERange(ode: Odevec, c0: int, c1: int, t, dt, t_stop, y, status, Mask=
     off = lambda a, k: None if a is None else ctypes.c_void_p(a.data_ptr() + k * a.element_size())
     st = stream if stream is not None else torch.cuda.current_stream(y.device)
     with torch.cuda.device(y.device):
-        _check(lib().odevec_solve_range(ode.handle, c1 - c0, ncells, off(y, c0), off(t, c0), off(dt, c0),
+        fn = lib().odevec_solve_continue if cont else lib().odevec_solve_range
+        _check(fn(ode.handle, c1 - c0, ncells, off(y, c0), off(t, c0), off(dt, c0),
                                         off(t_stop, c0), off(Mask, c0), off(status, c0), None,
                                         off(workspace, c0), {False: 0, True: 1, 2: 2, "en_old": 2}[resume],
                                         ctypes.c_void_p(st.cuda_stream)))
+
+
+def set_yield(ode: Odevec, flag=None):
+    """Registers a yield flag (a one-element int32 CUDA tensor, or None;
+    set it from another stream with a copy, e.g. ``flag.copy_(one_pinned,
+    non_blocking=True)``, so that no SM is needed to write it):
+    while it holds a nonzero value, the kernels of this solver's later solves
+    start no new cells and their launch ends once the running cells are done
+    (odevec_set_yield).  The solver keeps the pointer: keep the tensor alive."""
+    ode._yield_flag = flag
+    _check(lib().odevec_set_yield(ode.handle, None if flag is None else ctypes.c_void_p(flag.data_ptr())))
+
+
+def cells_started(ode: Odevec, stream=None) -> int:
+    """Cells the current solve has started (>= ncells: all); synchronises
+    `stream` (odevec_cells_started)."""
+    import torch
+    st = stream if stream is not None else torch.cuda.current_stream()
+    n = ctypes.c_int64(0)
+    _check(lib().odevec_cells_started(ode.handle, ctypes.c_void_p(st.cuda_stream), ctypes.byref(n)))
+    return int(n.value)

@@ -533,3 +533,57 @@ def test_ranges_equal_whole_solve(gpu_lib, precision):
     assert np.all(whole[3] == 0)
     for a, b in zip(parts, whole):
         assert np.array_equal(a, b)
+
+
+@pytest.mark.parametrize("name,network,ncells,precision,max_attempts,staging", [
+    ("PRIMORDIAL", "PRIMORDIAL_CSC_FF", 100000, "fp64", 0, 0),
+    ("PRIMORDIAL", "PRIMORDIAL_CSC_FF", 100000, "fp32_lu", 0, 0),
+    ("PRIMORDIAL", "PRIMORDIAL_CSC_FF", 100000, "fp32_lu", 5, 0),   # every cell escalated
+    ("PRIMORDIAL", "PRIMORDIAL_CSC_FF", 60000, "fp64", 0, 1),       # refill on every trip
+    ("SYN64", "SYN64_CSC_CMK", 5000, "fp64", 0, 7),                 # 32 lanes per cell
+    ("ROBER", "ROBER_DENSE_NONE", 65536, "fp64", 0, 0),             # lockstep groups of 32
+])
+def test_yield_and_continue_equal_one_solve(gpu_lib, name, network, ncells, precision, max_attempts, staging):
+    """odevec_set_yield / odevec_solve_continue: with the yield flag set
+    before the launch, a launch starts only its first round of cells and
+    ends; continuations start the rest.  The results equal one uninterrupted
+    solve bit for bit, the FP32-LU escalation included."""
+    import torch
+    S = gpu_lib
+    wl = W.BUILDERS[name](ncells=ncells, network=network)
+    if name == "ROBER":
+        wl.group = 32
+
+    def run(yielding):
+        ode = S.Odevec(wl.network, RelativeTolerance=wl.rtol, AbsoluteTolerance=wl.atol, MinimalTimestep=wl.dt_min,
+                       nvector=wl.group, precision=precision, max_attempts=max_attempts, raise_on_failure=False,
+                       staging=staging)
+        S.InitOdevec(ode)
+        try:
+            y = torch.tensor(wl.y, device="cuda")
+            t, d, ts = (torch.tensor(a, device="cuda") for a in (wl.t0, wl.dt0, wl.t_stop))
+            st = torch.zeros(ncells, dtype=torch.int32, device="cuda")
+            launches = 1
+            if yielding:
+                flag = torch.ones(1, dtype=torch.int32, device="cuda")
+                S.set_yield(ode, flag)
+            S.SolveODERange(ode, 0, ncells, t, d, ts, y, st)
+            if yielding:
+                assert S.cells_started(ode) < ncells  # the first launch yielded
+                while S.cells_started(ode) < ncells:
+                    S.SolveODERange(ode, 0, ncells, t, d, ts, y, st, cont=True)
+                    launches += 1
+                    assert launches < 400
+                S.set_yield(ode, None)
+            torch.cuda.synchronize()
+            return [a.cpu().numpy() for a in (y, t, d, st)], launches
+        finally:
+            S.CloseOdevec(ode)
+
+    ref, _ = run(False)
+    got, launches = run(True)
+    assert launches >= 2
+    for what, a, b in zip(("y", "t", "dt", "status"), got, ref):
+        assert np.array_equal(a, b, equal_nan=True), what
+    if max_attempts:
+        assert np.sum(ref[3] == 4) >= 0.9 * ncells
