@@ -48,6 +48,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <type_traits>
+
 #include "../../include/odevec_b200.h"
 #include "ov_common.h"
 #include "ov_launch.h"
@@ -204,6 +206,10 @@ template <> struct StageCfg<16> { static constexpr int SHM = 0; static constexpr
    factors, 4.5 % slower in FP64; slower on short operator-split solves,
    whose lanes then wait longer for new cells) */
 template <> struct StageCfg<17> { static constexpr int SHM = 2; static constexpr bool SOFT = true;  static constexpr int BS = 384, MINB = 1, REFILL = 32, PERIOD = 4; };
+/* as 15 and 8 (soft lockstep, 256 or 384 threads) with the state vector y
+   in shared memory (networks above 32 solver species) */
+template <> struct StageCfg<18> { static constexpr int SHM = 4; static constexpr bool SOFT = true;  static constexpr int BS = 256, MINB = 1, REFILL = 16, PERIOD = 4; };
+template <> struct StageCfg<19> { static constexpr int SHM = 4; static constexpr bool SOFT = true;  static constexpr int BS = 384, MINB = 1, REFILL = 16, PERIOD = 4; };
 
 /* Soft lockstep.  The warps of a block wait for each other at the top of
    every trip of the cell loop, so they run the same phase code at the same
@@ -278,6 +284,16 @@ struct Staging<Net, LUT, 1, BS> { /* shared memory, [entry][lane] */
 };
 
 template <class Net, class LUT, int BS>
+struct Staging<Net, LUT, 4, BS> { /* the state vector y in shared memory, history and LU thread-local */
+    using Hist = double (*)[Net::ND];
+    using LU = LUT*;
+    /* one row of NEQ + 1 doubles per thread: the odd row length spreads a
+       warp's accesses to one species over the banks */
+    static constexpr int YROW = Net::NEQ + 1;
+    static constexpr size_t smem_bytes = sizeof(double) * YROW * BS;
+};
+
+template <class Net, class LUT, int BS>
 struct Staging<Net, LUT, 2, BS> { /* history in shared memory, LU thread-local */
     using Hist = LaneHist<Net::ND, BS>;
     using LU = LUT*;
@@ -300,7 +316,9 @@ struct Cell {
     alignas(16) double en[ND];
     alignas(16) double eno[ND];
     alignas(16) double w2[ND];
-    alignas(16) double y[N];
+    /* the full state: a thread-local array, or (SHM 4) this thread's row in
+       shared memory, which the network code reloads instead of spilling */
+    alignas(16) std::conditional_t<SHM == 4, double*, double[N]> y;
     typename Staging<Net, LUT, SHM, BS>::LU a; /* packed LU of the iteration matrix */
     alignas(16) double rT[NR];
     /* FP32 LU: the scale of species j is 2^sce[j] (kept as an exponent, the
@@ -843,16 +861,19 @@ __device__ __forceinline__ void bdf_run(const LaunchArgs& A)
         return;
 
     C c;
-    if constexpr (SHM != 0) {
+    if constexpr (SHM == 4) {
+        extern __shared__ __align__(16) unsigned char ov_smem[];
+        c.y = reinterpret_cast<double*>(ov_smem) + (size_t)threadIdx.x * Staging<Net, LUT, 4, BS>::YROW;
+    } else if constexpr (SHM != 0) {
         extern __shared__ __align__(16) unsigned char ov_smem[];
         c.yns = LaneHist<ND, BS>{reinterpret_cast<double*>(ov_smem) + threadIdx.x};
         if constexpr (SHM == 1)
             c.a = LaneCol<LUT, BS>{reinterpret_cast<LUT*>(ov_smem + Staging<Net, LUT, 1, BS>::hist_bytes)
                                    + threadIdx.x};
     }
-    alignas(16) double history[SHM != 0 ? 1 : MAXQ + 1][ND];
+    alignas(16) double history[(SHM == 0 || SHM == 4) ? MAXQ + 1 : 1][ND];
     alignas(16) LUT lu_local[SHM == 1 ? 1 : C::NNZ];
-    if constexpr (SHM == 0)
+    if constexpr (SHM == 0 || SHM == 4)
         c.yns = history;
     if constexpr (SHM != 1)
         c.a = lu_local;
@@ -1396,6 +1417,13 @@ constexpr bool hist_fits()
     return Staging<Net, double, 2, BS>::smem_bytes <= 200 * 1024;
 }
 
+/* the state vectors of a block within the 227 KB a block may hold */
+template <class Net, int BS>
+constexpr bool y_fits()
+{
+    return Staging<Net, double, 4, BS>::smem_bytes <= 226 * 1024;
+}
+
 /* the history alone within the 227 KB a block may hold (less the soft
    lockstep words) */
 template <class Net, int BS>
@@ -1420,9 +1448,10 @@ constexpr bool hist_fits_max()
    shared memory (where they fit); 12 = as 9 in one block of 384; 13, 14 =
    16 or 8 lanes per cell (wpc_kernel.cuh, as 7); 15, 16 = as 8 in one block
    of 256 or 512 (networks above 32 solver species); 17 = as 12 refilling on
-   every 32nd trip.  With per-cell control stagings 2-6 and 8-16 refill idle
+   every 32nd trip; 18, 19 = as 8 in one block of 256 or 384 with the state
+   vector in shared memory (networks above 32 solver species).  With per-cell control stagings 2-6 and 8-16 refill idle
    lanes on every 16th trip, 17 on every 32nd, staging 1 on every trip.
-   Stages 2-17 exist for per-cell control (G = 1). */
+   Stages 2-19 exist for per-cell control (G = 1). */
 #define OV_STAGE_CASE(NET, LU, ST)                                                               \
     if (stage == ST)                                                                             \
         return launch<NET, 1, LU, ST>(a, block, grid, s);
@@ -1462,6 +1491,12 @@ constexpr bool hist_fits_max()
             if constexpr (NET::ND > 32) {                                                    \
                 OV_STAGE_CASE(NET, double, 15)                                               \
                 OV_STAGE_CASE(NET, double, 16)                                               \
+                if constexpr (y_fits<NET, 256>()) {                                          \
+                    OV_STAGE_CASE(NET, double, 18)                                           \
+                }                                                                            \
+                if constexpr (y_fits<NET, 384>()) {                                          \
+                    OV_STAGE_CASE(NET, double, 19)                                           \
+                }                                                                            \
             }                                                                                \
             if constexpr (hist_fits<NET, 256>()) {                                               \
                 OV_STAGE_CASE(NET, double, 9)                                                    \
@@ -1503,6 +1538,12 @@ constexpr bool hist_fits_max()
                 if constexpr (NET::ND > 32) {                                                \
                     OV_STAGE_CASE(NET, float, 15)                                            \
                     OV_STAGE_CASE(NET, float, 16)                                            \
+                    if constexpr (y_fits<NET, 256>()) {                                      \
+                        OV_STAGE_CASE(NET, float, 18)                                        \
+                    }                                                                        \
+                    if constexpr (y_fits<NET, 384>()) {                                      \
+                        OV_STAGE_CASE(NET, float, 19)                                        \
+                    }                                                                        \
                 }                                                                            \
                 if constexpr (hist_fits<NET, 256>()) {                                           \
                     OV_STAGE_CASE(NET, float, 9)                                                 \

@@ -301,13 +301,14 @@ def test_syn64_mass_conservation(gpu_lib):
 
 def test_syn64_stagings_bit_exact(gpu_lib, oracle):
     """The 64-species network on every thread-per-cell shape it compiles
-    (the soft-lockstep 256- and 512-thread blocks exist for networks above
-    32 solver species only), with more cells than one block holds, equals
-    the oracle bit for bit."""
+    (the soft-lockstep 256- and 512-thread blocks and the shapes with the
+    state vector in shared memory exist for networks above 32 solver species
+    only), with more cells than one block holds, equals the oracle bit for
+    bit."""
     wl = W.syn64(ncells=700)
     o = run_oracle(oracle, wl)
     assert np.all(o[3] == 0)
-    for staging in (1, 3, 6, 8, 15, 16):
+    for staging in (1, 3, 6, 8, 15, 16, 18, 19):
         assert_bitwise(run_gpu(gpu_lib, wl, "fp64", staging=staging), o, "SYN64 staging %d" % staging)
 
 
