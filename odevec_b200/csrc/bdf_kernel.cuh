@@ -1300,11 +1300,25 @@ __global__ void __launch_bounds__(StageCfg<STAGE>::BS, StageCfg<STAGE>::MINB)
 }
 
 /* ---- several networks in one launch ---------------------------------- */
-/* thread-local arrays, one 384-thread block per SM in soft lockstep: the
+/* one 384-thread block per SM in soft lockstep, each thread's state vector
+   in shared memory (rows sized for the largest network of the set): the
    register budget of staging 3, without the instruction-fetch stalls of a
-   large network's code (SYN64: 1.35x over staging 1); every warp of a block
-   runs the same job at a time, so the lockstep keeps them on the same code */
-constexpr int MULTI_STAGE = 8;
+   large network's code, and with the large network's state reloaded from
+   shared memory instead of spilled (SYN64: 1.49x over staging 1); every
+   warp of a block runs the same job at a time, so the lockstep keeps them
+   on the same code */
+constexpr int MULTI_STAGE = 19;
+
+template <class LUT, class... Nets>
+constexpr size_t multi_smem_bytes()
+{
+    size_t m = 0;
+    ((m = Staging<Nets, LUT, StageCfg<MULTI_STAGE>::SHM, StageCfg<MULTI_STAGE>::BS>::smem_bytes > m
+              ? Staging<Nets, LUT, StageCfg<MULTI_STAGE>::SHM, StageCfg<MULTI_STAGE>::BS>::smem_bytes
+              : m),
+     ...);
+    return m;
+}
 
 template <class LUT, class... Nets>
 struct MultiDispatch {
@@ -1341,12 +1355,19 @@ cudaError_t launch_multi(MultiArgs& P, cudaStream_t stream)
 {
     using Cfg = StageCfg<MULTI_STAGE>;
     auto kern = bdf_multi_kernel<LUT, Nets...>;
+    constexpr size_t smem = multi_smem_bytes<LUT, Nets...>();
+    static_assert(smem <= 226 * 1024, "the set's largest state vectors exceed a block's shared memory");
     static int cached_grid = 0;
     if (cached_grid == 0) {
         int dev = 0, sms = 0, per_sm = 0;
         cudaGetDevice(&dev);
+        if (smem > 48 * 1024) {
+            cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+            if (e != cudaSuccess)
+                return e;
+        }
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, Cfg::BS, 0);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, Cfg::BS, smem);
         cached_grid = sms * (per_sm > 0 ? per_sm : 1);
     }
     int64_t total = 0;
@@ -1364,7 +1385,7 @@ cudaError_t launch_multi(MultiArgs& P, cudaStream_t stream)
         start += nb;
     }
     P.block_start[P.njobs] = start;
-    kern<<<start, Cfg::BS, 0, stream>>>(P);
+    kern<<<start, Cfg::BS, smem, stream>>>(P);
     return cudaGetLastError();
 }
 template <class Net, int G, class LUT, int STAGE>
