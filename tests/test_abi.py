@@ -73,6 +73,23 @@ def test_solve_argument_errors(L):
     assert L.odevec_close(None) == 0
 
 
+def test_yield_and_continue_argument_errors(L):
+    """Interruptible-solve entry points reject a null solver, a bad resume
+    code and a resume without workspace before touching the GPU."""
+    P = ctypes.c_void_p(16)
+    n = ctypes.c_int64(0)
+    assert L.odevec_set_yield(None, None) == -1
+    assert L.odevec_cells_started(None, None, ctypes.byref(n)) == -1
+    cont = L.odevec_solve_continue
+    assert cont(None, 10, 10, P, P, P, P, None, None, None, None, 0, None) == -1
+    assert cont(None, 10, 10, P, P, P, P, None, None, None, None, 3, None) == -1
+    assert b"resume" in L.odevec_last_error()
+    assert cont(None, 10, 10, P, P, P, P, None, None, None, None, 1, None) == -1
+    assert b"workspace" in L.odevec_last_error()
+    rng = L.odevec_solve_range
+    assert rng(None, 10, 10, P, P, P, P, None, None, None, None, 0, None) == -1
+
+
 def test_noalloc_argument_errors(L):
     f = L.odevec_solve_noalloc
     from odevec_b200 import solver
