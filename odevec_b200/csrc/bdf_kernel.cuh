@@ -922,8 +922,13 @@ __device__ __forceinline__ void bdf_run(const LaunchArgs& A)
                     base = atomicAdd(A.queue, (unsigned long long)__popc(need));
                 base = __shfl_sync(FULL, base, leader);
                 if (ph == PH_IDLE) {
-                    cell = (int64_t)(base + __popc(need & ((1u << lane) - 1u)));
-                    ph = cell < ncells ? PH_START : PH_EXHAUSTED;
+                    const int64_t q = (int64_t)(base + __popc(need & ((1u << lane) - 1u)));
+                    if (q < ncells) {
+                        cell = A.order ? (int64_t)A.order[q] : q;
+                        ph = PH_START;
+                    } else {
+                        ph = PH_EXHAUSTED;
+                    }
                 }
             }
             if (__all_sync(FULL, ph == PH_EXHAUSTED)) {

@@ -9,6 +9,7 @@
  * per-cell integration failures are status codes (the reference calls
  * `stop`, src/odevec.F90:114-124, 272-287, 380-390, 585-597). */
 #include <cuda.h>
+#include <cub/device/device_radix_sort.cuh>
 #include <cuda_runtime.h>
 
 #include <cstdarg>
@@ -171,11 +172,38 @@ struct odevec_solver {
     uint8_t* fb_mask;
     /* odevec_set_yield: the kernels stop starting cells while *yield != 0 */
     const int32_t* yield;
+    /* visit order, longest integration span first (per-cell control):
+       16-bit keys and cell indices, double-buffered for the radix sort, its
+       scratch, and the order of the last solve (a continuation reuses it) */
+    int64_t ord_cells;
+    uint16_t* ord_keys;
+    int32_t* ord_vals;
+    void* ord_temp;
+    size_t ord_temp_bytes;
+    const int32_t* ord_cur;
 };
 /* d_queue words: [0] the solve's work counter, [1] cells that failed with
    FP32 factors, [2] the FP64 re-solve's work counter */
+/* solves of fewer cells keep the given visit order: the order costs a
+   sort, and where a persistent grid holds (nearly) every cell at once
+   (19k-57k lanes resident) there is no tail to shorten */
+constexpr int64_t OV_ORDER_MIN_CELLS = 32768;
 
 namespace {
+/* sort keys of the visit order: the top 16 bits of t_stop - t (a
+   non-negative double's bits order as its value: sign, exponent and 4
+   mantissa bits, buckets of 1/16 octave); NaN and non-positive spans 0 */
+__global__ void ov_order_keys(int64_t ncells, const double* t, const double* t_stop, uint16_t* key,
+                              int32_t* idx)
+{
+    for (int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; c < ncells;
+         c += (int64_t)gridDim.x * blockDim.x) {
+        const double span = t_stop[c] - t[c];
+        key[c] = span > 0.0 ? (uint16_t)((unsigned long long)__double_as_longlong(span) >> 48) : (uint16_t)0;
+        idx[c] = (int32_t)c;
+    }
+}
+
 /* cells whose FP32-LU solve failed get their inputs back and a retry mask;
    *nfail counts them */
 /* mass fraction <-> number density (tests/primordial.f90:113-140), one
@@ -366,7 +394,8 @@ int32_t odevec_set_options(odevec_solver* s, const odevec_opts* opts)
 
 static int32_t solve_impl(odevec_solver* s, int64_t ncells, int64_t stride, double* y, double* t,
                           double* dt, const double* t_stop, const uint8_t* mask, int32_t* status,
-                          int32_t* stats, double* ws, int32_t resume, void* stream, bool cont = false);
+                          int32_t* stats, double* ws, int32_t resume, void* stream, bool cont = false,
+                          bool allow_order = true);
 
 int32_t odevec_solve(odevec_solver* s, int64_t ncells, double* y, double* t, double* dt,
                      const double* t_stop, const uint8_t* mask, int32_t* status, int32_t* stats,
@@ -443,7 +472,8 @@ int32_t odevec_cells_started(odevec_solver* s, void* stream, int64_t* started)
 
 static int32_t solve_impl(odevec_solver* s, int64_t ncells, int64_t stride, double* y, double* t,
                           double* dt, const double* t_stop, const uint8_t* mask, int32_t* status,
-                          int32_t* stats, double* ws, int32_t resume, void* stream, bool cont)
+                          int32_t* stats, double* ws, int32_t resume, void* stream, bool cont,
+                          bool allow_order)
 {
     if (!s)
         return fail(OV_API_EINVAL, "solver is null");
@@ -485,12 +515,59 @@ static int32_t solve_impl(odevec_solver* s, int64_t ncells, int64_t stride, doub
     a.run_if = nullptr;
     a.save_y = a.save_t = a.save_dt = nullptr;
     a.yield = s->yield;
+    a.order = nullptr;
     cudaStream_t st = (cudaStream_t)stream;
     /* a continuation keeps the work counter (and the failure count) of the
        solve it continues */
     cudaError_t err = cont ? cudaSuccess : cudaMemsetAsync(s->d_queue, 0, sizeof(unsigned long long), st);
     if (err != cudaSuccess)
         return fail(OV_API_ECUDA, "odevec_solve: %s", cudaGetErrorString(err));
+    /* Visit order: cells with the longest integration span first, so that
+       the persistent grid's last cells are short ones (a continuation keeps
+       the order of the solve it continues).  Results do not depend on it.
+       Per-cell control on device arrays only: a lockstep group is 32
+       consecutive cells, and cells read in scattered order from host memory
+       would cross the host link in small pieces. */
+    if (cont) {
+        a.order = s->ord_cur;
+    } else {
+        s->ord_cur = nullptr;
+        if (allow_order && o.group_size == 1 && ncells >= OV_ORDER_MIN_CELLS && ncells <= (int64_t)INT32_MAX) {
+            if (s->ord_cells < ncells) {
+                cudaFree(s->ord_keys); cudaFree(s->ord_vals); cudaFree(s->ord_temp);
+                s->ord_keys = nullptr; s->ord_vals = nullptr; s->ord_temp = nullptr;
+                s->ord_cells = 0;
+                s->ord_temp_bytes = 0;
+                const size_t n = (size_t)ncells;
+                err = cudaMalloc(&s->ord_keys, 2 * n * sizeof(uint16_t));
+                if (err == cudaSuccess) err = cudaMalloc(&s->ord_vals, 2 * n * sizeof(int32_t));
+                if (err == cudaSuccess) {
+                    cub::DoubleBuffer<uint16_t> kb(s->ord_keys, s->ord_keys + n);
+                    cub::DoubleBuffer<int32_t> vb(s->ord_vals, s->ord_vals + n);
+                    err = cub::DeviceRadixSort::SortPairsDescending(nullptr, s->ord_temp_bytes, kb, vb, (int)n, 0,
+                                                                    16, st);
+                }
+                if (err == cudaSuccess) err = cudaMalloc(&s->ord_temp, s->ord_temp_bytes);
+                if (err != cudaSuccess)
+                    return fail(OV_API_ENOMEM, "odevec_solve: visit order buffers: %s", cudaGetErrorString(err));
+                s->ord_cells = ncells;
+            }
+            const size_t cap = (size_t)s->ord_cells;
+            int sms = 0;
+            cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, s->device);
+            ov_order_keys<<<sms * 4, 256, 0, st>>>(ncells, t, t_stop, s->ord_keys, s->ord_vals);
+            err = cudaGetLastError();
+            cub::DoubleBuffer<uint16_t> kb(s->ord_keys, s->ord_keys + cap);
+            cub::DoubleBuffer<int32_t> vb(s->ord_vals, s->ord_vals + cap);
+            size_t bytes = s->ord_temp_bytes;
+            if (err == cudaSuccess)
+                err = cub::DeviceRadixSort::SortPairsDescending(s->ord_temp, bytes, kb, vb, (int)ncells, 0, 16, st);
+            if (err != cudaSuccess)
+                return fail(OV_API_ECUDA, "odevec_solve: visit order: %s", cudaGetErrorString(err));
+            s->ord_cur = vb.Current();
+            a.order = s->ord_cur;
+        }
+    }
     const int lu = o.precision == OV_PREC_FP32_LU ? 1 : 0;
     ov::launch_fn fn = o.precision == OV_PREC_FP64 ? e.exact : e.fma;
     /* automatic (options left at 0): the tuning table for this GPU, else
@@ -635,7 +712,10 @@ int32_t odevec_solve_host(odevec_solver* s, int64_t ncells, double* y, double* t
     if (e == cudaSuccess && mask && !mm) e = cudaMemcpyAsync(s->d_mask, mask, n, cudaMemcpyHostToDevice, st);
     if (e != cudaSuccess)
         return fail(OV_API_ECUDA, "odevec_solve_host copy-in: %s", cudaGetErrorString(e));
-    int32_t rc = odevec_solve(s, ncells, ky, kt, kdt, kts, km, kst, ksa, st);
+    /* the visit order reads cells in scattered order: only when y, t, dt
+       and t_stop are in device memory */
+    const bool host_in_place = my || mt || mdt || mts;
+    int32_t rc = solve_impl(s, ncells, ncells, ky, kt, kdt, kts, km, kst, ksa, nullptr, 0, st, false, !host_in_place);
     if (rc)
         return rc;
     if (!my) e = cudaMemcpyAsync(y, s->d_y, yb, cudaMemcpyDeviceToHost, st);
@@ -697,6 +777,9 @@ int32_t odevec_close(odevec_solver* s)
     if (!s)
         return OV_API_OK;
     cudaFree(s->d_queue);
+    cudaFree(s->ord_keys);
+    cudaFree(s->ord_vals);
+    cudaFree(s->ord_temp);
     cudaFree(s->d_y);
     cudaFree(s->d_t);
     cudaFree(s->d_dt);
@@ -884,6 +967,7 @@ extern "C" int32_t odevec_solve_noalloc(const char* network, const odevec_opts* 
     a.run_if = nullptr;
     a.save_y = a.save_t = a.save_dt = nullptr;
     a.yield = nullptr;
+    a.order = nullptr;
     const NetEntry& e = g_nets[ni];
     const int lu = o.precision == OV_PREC_FP32_LU ? 1 : 0;
     ov::launch_fn fn = o.precision == OV_PREC_FP64 ? e.exact : e.fma;

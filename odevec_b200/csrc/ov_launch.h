@@ -55,6 +55,10 @@ struct LaunchArgs {
        continues with them (read with a volatile load: device memory or
        pinned, mapped host memory) */
     const int32_t* yield;
+    /* per-cell control only: if non-null, the q-th cell taken from the work
+       counter is cell order[q] (a permutation of 0..ncells-1), so cells are
+       visited in that order; results do not depend on it */
+    const int32_t* order;
 };
 
 /* Several solves of different networks in one launch (the multi-network

@@ -815,9 +815,10 @@ __global__ void __launch_bounds__(256, (WpcLayout<Net, LUT, K>::MINB)) wpc_kerne
         unsigned long long g = 0;
         if (sub == 0)
             g = atomicAdd(A.queue, 1ull);
-        const int64_t cell = (int64_t)__shfl_sync(c.gmask, g, c.glead);
-        if (cell >= ncells)
+        const int64_t q = (int64_t)__shfl_sync(c.gmask, g, c.glead);
+        if (q >= ncells)
             break;
+        const int64_t cell = A.order ? (int64_t)A.order[q] : q;
         __syncwarp(c.gmask);
         for (int s = sub; s < N; s += K) {
             c.yv[s] = A.y[(int64_t)s * A.stride + cell];

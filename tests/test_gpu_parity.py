@@ -588,3 +588,39 @@ def test_yield_and_continue_equal_one_solve(gpu_lib, name, network, ncells, prec
         assert np.array_equal(a, b, equal_nan=True), what
     if max_attempts:
         assert np.sum(ref[3] == 4) >= 0.9 * ncells
+
+
+@pytest.mark.parametrize("name,network,ncells,precision,staging", [
+    ("PRIMORDIAL", "PRIMORDIAL_CSC_FF", 70000, "fp64", 0),
+    ("PRIMORDIAL", "PRIMORDIAL_CSC_FF", 70000, "fp32_lu", 0),
+    ("OREGO", "OREGO_CSC_CMK", 70000, "fp64", 0),
+    ("SYN64", "SYN64_CSC_CMK", 40000, "fp64", 7),   # 32 lanes per cell
+])
+def test_visit_order_keeps_results(gpu_lib, name, network, ncells, precision, staging):
+    """A solve of at least 32,768 cells visits them longest span first (a
+    sort inside odevec_solve); the same cells solved as ranges below that
+    size keep the given order.  Both give the same bits."""
+    import torch
+    S = gpu_lib
+    wl = W.BUILDERS[name](ncells=ncells, network=network)
+
+    def run(ranges):
+        ode = S.Odevec(wl.network, RelativeTolerance=wl.rtol, AbsoluteTolerance=wl.atol, MinimalTimestep=wl.dt_min,
+                       nvector=1, precision=precision, raise_on_failure=False, staging=staging)
+        S.InitOdevec(ode)
+        try:
+            y = torch.tensor(wl.y, device="cuda")
+            t, d, ts = (torch.tensor(a, device="cuda") for a in (wl.t0, wl.dt0, wl.t_stop))
+            st = torch.zeros(ncells, dtype=torch.int32, device="cuda")
+            for c0, c1 in ranges:
+                S.SolveODERange(ode, c0, c1, t, d, ts, y, st)
+            torch.cuda.synchronize()
+            return [a.cpu().numpy() for a in (y, t, d, st)]
+        finally:
+            S.CloseOdevec(ode)
+
+    whole = run([(0, ncells)])
+    parts = run([(0, 30000), (30000, 60000), (60000, ncells)] if ncells > 60000 else [(0, 30000), (30000, ncells)])
+    assert np.all(whole[3] == 0)
+    for what, a, b in zip(("y", "t", "dt", "status"), whole, parts):
+        assert np.array_equal(a, b, equal_nan=True), what
