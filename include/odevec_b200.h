@@ -147,7 +147,9 @@ int32_t odevec_set_options(odevec_solver* s, const odevec_opts* opts);
    default stream).  y, t, dt are read and overwritten: on return t[c] =
    t_stop[c], dt[c] = the last internal step, y = the solution at t_stop.
    mask (nullable): cells with mask 0 are left untouched except t = t_stop.
-   status, stats: nullable outputs. */
+   status, stats: nullable outputs.  With per-cell control and at least
+   32,768 cells the cells are visited longest t_stop - t first (a device
+   sort on the stream); results do not depend on the order. */
 int32_t odevec_solve(odevec_solver* s, int64_t ncells, double* y, double* t, double* dt,
                      const double* t_stop, const uint8_t* mask, int32_t* status, int32_t* stats,
                      void* stream);

@@ -394,8 +394,7 @@ int32_t odevec_set_options(odevec_solver* s, const odevec_opts* opts)
 
 static int32_t solve_impl(odevec_solver* s, int64_t ncells, int64_t stride, double* y, double* t,
                           double* dt, const double* t_stop, const uint8_t* mask, int32_t* status,
-                          int32_t* stats, double* ws, int32_t resume, void* stream, bool cont = false,
-                          bool allow_order = true);
+                          int32_t* stats, double* ws, int32_t resume, void* stream, bool cont = false);
 
 int32_t odevec_solve(odevec_solver* s, int64_t ncells, double* y, double* t, double* dt,
                      const double* t_stop, const uint8_t* mask, int32_t* status, int32_t* stats,
@@ -472,8 +471,7 @@ int32_t odevec_cells_started(odevec_solver* s, void* stream, int64_t* started)
 
 static int32_t solve_impl(odevec_solver* s, int64_t ncells, int64_t stride, double* y, double* t,
                           double* dt, const double* t_stop, const uint8_t* mask, int32_t* status,
-                          int32_t* stats, double* ws, int32_t resume, void* stream, bool cont,
-                          bool allow_order)
+                          int32_t* stats, double* ws, int32_t resume, void* stream, bool cont)
 {
     if (!s)
         return fail(OV_API_EINVAL, "solver is null");
@@ -525,14 +523,15 @@ static int32_t solve_impl(odevec_solver* s, int64_t ncells, int64_t stride, doub
     /* Visit order: cells with the longest integration span first, so that
        the persistent grid's last cells are short ones (a continuation keeps
        the order of the solve it continues).  Results do not depend on it.
-       Per-cell control on device arrays only: a lockstep group is 32
-       consecutive cells, and cells read in scattered order from host memory
-       would cross the host link in small pieces. */
+       Per-cell control only: a lockstep group is 32 consecutive cells.
+       (Pinned host arrays read in place are then read in scattered order:
+       on PRIMORDIAL that costs about what the order gains with FP32
+       factors, and gains 3 % in FP64.) */
     if (cont) {
         a.order = s->ord_cur;
     } else {
         s->ord_cur = nullptr;
-        if (allow_order && o.group_size == 1 && ncells >= OV_ORDER_MIN_CELLS && ncells <= (int64_t)INT32_MAX) {
+        if (o.group_size == 1 && ncells >= OV_ORDER_MIN_CELLS && ncells <= (int64_t)INT32_MAX) {
             if (s->ord_cells < ncells) {
                 cudaFree(s->ord_keys); cudaFree(s->ord_vals); cudaFree(s->ord_temp);
                 s->ord_keys = nullptr; s->ord_vals = nullptr; s->ord_temp = nullptr;
@@ -712,10 +711,7 @@ int32_t odevec_solve_host(odevec_solver* s, int64_t ncells, double* y, double* t
     if (e == cudaSuccess && mask && !mm) e = cudaMemcpyAsync(s->d_mask, mask, n, cudaMemcpyHostToDevice, st);
     if (e != cudaSuccess)
         return fail(OV_API_ECUDA, "odevec_solve_host copy-in: %s", cudaGetErrorString(e));
-    /* the visit order reads cells in scattered order: only when y, t, dt
-       and t_stop are in device memory */
-    const bool host_in_place = my || mt || mdt || mts;
-    int32_t rc = solve_impl(s, ncells, ncells, ky, kt, kdt, kts, km, kst, ksa, nullptr, 0, st, false, !host_in_place);
+    int32_t rc = odevec_solve(s, ncells, ky, kt, kdt, kts, km, kst, ksa, st);
     if (rc)
         return rc;
     if (!my) e = cudaMemcpyAsync(y, s->d_y, yb, cudaMemcpyDeviceToHost, st);
