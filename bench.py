@@ -362,8 +362,10 @@ def run_product(args):
             "e2e": world * N * e2e_steps / e2e_s,
             "clocks": cs.summary(),
             # the solve kernel; FP32-LU adds the escalation kernel and the FP64
-            # re-solve launch (which returns at once when no cell failed)
-            "launches_per_step": 3 if form == "fp32_lu" else 1,
+            # re-solve launch (which returns at once when no cell failed); a
+            # per-cell solve of at least 32,768 cells adds the visit order's
+            # key kernel and the four kernels of its radix sort
+            "launches_per_step": (3 if form == "fp32_lu" else 1) + (5 if wl.group == 1 and N >= 32768 else 0),
         }
         if clocks is None:
             clocks = cs.summary()

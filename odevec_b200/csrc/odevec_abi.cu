@@ -469,6 +469,53 @@ int32_t odevec_cells_started(odevec_solver* s, void* stream, int64_t* started)
     return OV_API_OK;
 }
 
+/* The visit order of a per-cell solve of ncells cells (device arrays t,
+   t_stop): cells with the longest integration span first, computed on
+   `st` into s's buffers (*order = null below OV_ORDER_MIN_CELLS cells);
+   remembered as s->ord_cur for a continuation. */
+static int32_t visit_order(odevec_solver* s, int64_t ncells, const double* t, const double* t_stop,
+                           cudaStream_t st, const int32_t** order)
+{
+    *order = nullptr;
+    s->ord_cur = nullptr;
+    if (ncells < OV_ORDER_MIN_CELLS || ncells > (int64_t)INT32_MAX)
+        return OV_API_OK;
+    cudaError_t err = cudaSuccess;
+    if (s->ord_cells < ncells) {
+        cudaFree(s->ord_keys); cudaFree(s->ord_vals); cudaFree(s->ord_temp);
+        s->ord_keys = nullptr; s->ord_vals = nullptr; s->ord_temp = nullptr;
+        s->ord_cells = 0;
+        s->ord_temp_bytes = 0;
+        const size_t n = (size_t)ncells;
+        err = cudaMalloc(&s->ord_keys, 2 * n * sizeof(uint16_t));
+        if (err == cudaSuccess) err = cudaMalloc(&s->ord_vals, 2 * n * sizeof(int32_t));
+        if (err == cudaSuccess) {
+            cub::DoubleBuffer<uint16_t> kb(s->ord_keys, s->ord_keys + n);
+            cub::DoubleBuffer<int32_t> vb(s->ord_vals, s->ord_vals + n);
+            err = cub::DeviceRadixSort::SortPairsDescending(nullptr, s->ord_temp_bytes, kb, vb, (int)n, 0, 16, st);
+        }
+        if (err == cudaSuccess) err = cudaMalloc(&s->ord_temp, s->ord_temp_bytes);
+        if (err != cudaSuccess)
+            return fail(OV_API_ENOMEM, "odevec_solve: visit order buffers: %s", cudaGetErrorString(err));
+        s->ord_cells = ncells;
+    }
+    const size_t cap = (size_t)s->ord_cells;
+    int sms = 0;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, s->device);
+    ov_order_keys<<<sms * 4, 256, 0, st>>>(ncells, t, t_stop, s->ord_keys, s->ord_vals);
+    err = cudaGetLastError();
+    cub::DoubleBuffer<uint16_t> kb(s->ord_keys, s->ord_keys + cap);
+    cub::DoubleBuffer<int32_t> vb(s->ord_vals, s->ord_vals + cap);
+    size_t bytes = s->ord_temp_bytes;
+    if (err == cudaSuccess)
+        err = cub::DeviceRadixSort::SortPairsDescending(s->ord_temp, bytes, kb, vb, (int)ncells, 0, 16, st);
+    if (err != cudaSuccess)
+        return fail(OV_API_ECUDA, "odevec_solve: visit order: %s", cudaGetErrorString(err));
+    s->ord_cur = vb.Current();
+    *order = s->ord_cur;
+    return OV_API_OK;
+}
+
 static int32_t solve_impl(odevec_solver* s, int64_t ncells, int64_t stride, double* y, double* t,
                           double* dt, const double* t_stop, const uint8_t* mask, int32_t* status,
                           int32_t* stats, double* ws, int32_t resume, void* stream, bool cont)
@@ -529,43 +576,12 @@ static int32_t solve_impl(odevec_solver* s, int64_t ncells, int64_t stride, doub
        factors, and gains 3 % in FP64.) */
     if (cont) {
         a.order = s->ord_cur;
+    } else if (o.group_size == 1) {
+        const int32_t rc = visit_order(s, ncells, t, t_stop, st, &a.order);
+        if (rc)
+            return rc;
     } else {
         s->ord_cur = nullptr;
-        if (o.group_size == 1 && ncells >= OV_ORDER_MIN_CELLS && ncells <= (int64_t)INT32_MAX) {
-            if (s->ord_cells < ncells) {
-                cudaFree(s->ord_keys); cudaFree(s->ord_vals); cudaFree(s->ord_temp);
-                s->ord_keys = nullptr; s->ord_vals = nullptr; s->ord_temp = nullptr;
-                s->ord_cells = 0;
-                s->ord_temp_bytes = 0;
-                const size_t n = (size_t)ncells;
-                err = cudaMalloc(&s->ord_keys, 2 * n * sizeof(uint16_t));
-                if (err == cudaSuccess) err = cudaMalloc(&s->ord_vals, 2 * n * sizeof(int32_t));
-                if (err == cudaSuccess) {
-                    cub::DoubleBuffer<uint16_t> kb(s->ord_keys, s->ord_keys + n);
-                    cub::DoubleBuffer<int32_t> vb(s->ord_vals, s->ord_vals + n);
-                    err = cub::DeviceRadixSort::SortPairsDescending(nullptr, s->ord_temp_bytes, kb, vb, (int)n, 0,
-                                                                    16, st);
-                }
-                if (err == cudaSuccess) err = cudaMalloc(&s->ord_temp, s->ord_temp_bytes);
-                if (err != cudaSuccess)
-                    return fail(OV_API_ENOMEM, "odevec_solve: visit order buffers: %s", cudaGetErrorString(err));
-                s->ord_cells = ncells;
-            }
-            const size_t cap = (size_t)s->ord_cells;
-            int sms = 0;
-            cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, s->device);
-            ov_order_keys<<<sms * 4, 256, 0, st>>>(ncells, t, t_stop, s->ord_keys, s->ord_vals);
-            err = cudaGetLastError();
-            cub::DoubleBuffer<uint16_t> kb(s->ord_keys, s->ord_keys + cap);
-            cub::DoubleBuffer<int32_t> vb(s->ord_vals, s->ord_vals + cap);
-            size_t bytes = s->ord_temp_bytes;
-            if (err == cudaSuccess)
-                err = cub::DeviceRadixSort::SortPairsDescending(s->ord_temp, bytes, kb, vb, (int)ncells, 0, 16, st);
-            if (err != cudaSuccess)
-                return fail(OV_API_ECUDA, "odevec_solve: visit order: %s", cudaGetErrorString(err));
-            s->ord_cur = vb.Current();
-            a.order = s->ord_cur;
-        }
     }
     const int lu = o.precision == OV_PREC_FP32_LU ? 1 : 0;
     ov::launch_fn fn = o.precision == OV_PREC_FP64 ? e.exact : e.fma;
@@ -1068,6 +1084,10 @@ extern "C" int32_t odevec_solve_many(const odevec_job* jobs, int32_t njobs, void
         cudaError_t err = cudaMemsetAsync(J.solver->d_queue, 0, sizeof(unsigned long long), st);
         if (err != cudaSuccess)
             return fail(OV_API_ECUDA, "odevec_solve_many: %s", cudaGetErrorString(err));
+        /* each job's cells longest span first, as odevec_solve visits them */
+        const int32_t rc = visit_order(J.solver, J.ncells, J.t, J.t_stop, st, &a.order);
+        if (rc)
+            return rc;
     }
     const int lu = prec == OV_PREC_FP32_LU ? 1 : 0;
     ov::multi_fn fn = prec == OV_PREC_FP64 ? m->exact : m->fma;
