@@ -292,8 +292,9 @@ int32_t odevec_solve_many(const odevec_job* jobs, int32_t njobs, void* stream);
    call resets the counter to zero on `stream` before the launch; all calls
    share the one counter, so calls that overlap on the GPU (different
    streams, or different host threads) race and must be serialised by the
-   caller.  The FP32-LU escalation of odevec_solve (see no_escalation) needs
-   buffers and is not done here. */
+   caller.  The FP32-LU escalation of odevec_solve (see no_escalation) and
+   its longest-span-first visit order need buffers and are not done here:
+   cells are visited in the given order (results are the same). */
 #define OV_NOALLOC_SCRATCH_BYTES 256
 #define OV_NOALLOC_MAX_CELLS (1LL << 40)
 int32_t odevec_solve_noalloc(const char* network, const odevec_opts* opts, int64_t ncells,
