@@ -95,3 +95,16 @@ def test_gpu_ladder_graph_equals_eager_fp32(gpu_lib):
     b = D.run_schedule(sch, "fp32_lu", graph=True, chunk=32)
     for x, y in zip(a, b):
         assert np.array_equal(x, y)
+
+
+@pytest.mark.gpu
+def test_gpu_ladder_graph_with_visit_order(gpu_lib):
+    """A ladder of more than 32,768 cells: every call sorts its cells
+    longest span first on the stream, inside the captured graphs too; the
+    replayed graphs give the eager ladder's bits."""
+    sch = D.primordial_schedule(40000)
+    sch.t_stops = sch.t_stops[:6]
+    a = D.run_schedule(sch, "fp32_lu", graph=False)
+    b = D.run_schedule(sch, "fp32_lu", graph=True, chunk=3)
+    for x, y in zip(a, b):
+        assert np.array_equal(x, y)
