@@ -43,6 +43,15 @@
 #endif
 #define OV_RESTRICT __restrict__
 
+/* A scheduling fence for long straight-line network code: the compiler
+   moves no memory access across it, so values loaded before it are not
+   kept live (and spilled) for uses long after.  No effect on results. */
+#if defined(__CUDA_ARCH__)
+#define OV_SCHED() asm volatile("" ::: "memory")
+#else
+#define OV_SCHED() ((void)0)
+#endif
+
 OV_HD static OV_INLINE double ov_bits2d(uint64_t b)
 {
 #if defined(__CUDA_ARCH__)

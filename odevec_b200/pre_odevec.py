@@ -420,11 +420,13 @@ def emit_c_header(sysm: System) -> str:
              "const double* OV_RESTRICT k, double* OV_RESTRICT f)" % cid)
     L.append("{")
     L.append("  (void)k;")
+    body = []
     for i in range(n):
         if net.heatcool and i == n - 2:
-            L.append("  f[%d] = ov_%s_hc(y, y[%d], y);  /* heating/cooling */" % (i, cid, i))
+            body.append("  f[%d] = ov_%s_hc(y, y[%d], y);  /* heating/cooling */" % (i, cid, i))
         else:
-            L.append("  f[%d] = %s;" % (i, _cexpr(net.rhs[i], pr)))
+            body.append("  f[%d] = %s;" % (i, _cexpr(net.rhs[i], pr)))
+    L += _fenced(body, SCHED_EVERY_RHS, n - len(frozen_species(sysm)) >= SCHED_MIN_ND, "  ")
     L.append("}")
     L.append("")
     hc_note = (" With heating/cooling difference quotients, entries the reference leaves"
@@ -725,6 +727,26 @@ def _reduce_lines(lines: List[str], kmap: Dict[int, int]) -> List[str]:
     return out
 
 
+# Networks above this many solver-state species get a scheduling fence
+# (OV_SCHED) every SCHED_EVERY statements of their straight-line code (every
+# SCHED_EVERY_RHS species of the right-hand side): their code is long enough
+# that the compiler's hoisted loads otherwise spill.
+SCHED_MIN_ND = 33
+SCHED_EVERY = 32
+SCHED_EVERY_RHS = 8
+
+
+def _fenced(lines: List[str], every: int, on: bool, indent: str = "    ") -> List[str]:
+    if not on:
+        return lines
+    out = []
+    for k, ln in enumerate(lines):
+        out.append(ln)
+        if (k + 1) % every == 0 and k + 1 < len(lines):
+            out.append(indent + "OV_SCHED();")
+    return out
+
+
 def emit_cuda_header(sysm: System) -> str:
     net = sysm.net
     cid = _cid(sysm.tag)
@@ -803,9 +825,8 @@ def emit_cuda_header(sysm: System) -> str:
                            lambda kk, i, j, e: ("a[%d] = (T)(%s);" % (kmap[kk], e)) if kk in kmap else None,
                            "    ", lambda i, j: _cexpr(src[i, j], pr))
     else:
-        for (i, j), kk in items:
-            if kk in kmap and src is not None:
-                L.append("    a[%d] = (T)(%s);" % (kmap[kk], _cexpr(src[i, j], pr)))
+        L += _fenced(["    a[%d] = (T)(%s);" % (kmap[kk], _cexpr(src[i, j], pr))
+                      for (i, j), kk in items if kk in kmap and src is not None], SCHED_EVERY, nd >= SCHED_MIN_ND)
     L.append("  }")
     L.append("  /* a = D P D^-1 rounded to T, D = diag(sc) over solver-state indices */")
     L.append("  template <class T, class A> OV_HD static OV_INLINE void store_scaled(const double* OV_RESTRICT P, "
@@ -827,10 +848,9 @@ def emit_cuda_header(sysm: System) -> str:
                                kmap[kk], e, dpos[sysm.perm[i]], dpos[sysm.perm[j]])) if kk in kmap else None,
                            "    ", lambda i, j: _cexpr(src[i, j], pr))
     else:
-        for (i, j), kk in items:
-            if kk in kmap and src is not None:
-                L.append("    a[%d] = (T)((%s)*sc[%d]*isc[%d]);" % (kmap[kk], _cexpr(src[i, j], pr),
-                                                                 dpos[sysm.perm[i]], dpos[sysm.perm[j]]))
+        L += _fenced(["    a[%d] = (T)((%s)*sc[%d]*isc[%d]);" % (kmap[kk], _cexpr(src[i, j], pr),
+                                                             dpos[sysm.perm[i]], dpos[sysm.perm[j]])
+                      for (i, j), kk in items if kk in kmap and src is not None], SCHED_EVERY, nd >= SCHED_MIN_ND)
     L.append("  }")
     L.append("  /* in-place numeric LU of the packed dynamic block a[0..NNZ-1]; A is a")
     L.append("     pointer or an accessor whose operator[] yields T& */")
@@ -838,8 +858,7 @@ def emit_cuda_header(sysm: System) -> str:
                                          [_remap_a(l, kmap) for l in _lu_solve_lines(sysm, dpos=dpos)])
     L.append("  template <class T, class A> OV_HD static OV_INLINE void lu_factor(A a) {")
     L.append("    (void)a;")
-    for ln in f_lines:
-        L.append("    " + ln)
+    L += _fenced(["    " + ln for ln in f_lines], SCHED_EVERY, nd >= SCHED_MIN_ND)
     L.append("  }")
     L.append("  /* x = P^-1 r on the dynamic block; r, x over solver-state indices.  sc/isc")
     L.append("     scale entry i by sc[i] on the way in and isc[i] on the way out (pass")
@@ -849,8 +868,7 @@ def emit_cuda_header(sysm: System) -> str:
              "const double* OV_RESTRICT isc) {")
     L.append("#define OV_SC(i) (sc ? sc[i] : 1.0)")
     L.append("#define OV_ISC(i) (isc ? isc[i] : 1.0)")
-    for ln in s_lines:
-        L.append("    " + ln)
+    L += _fenced(["    " + ln for ln in s_lines], SCHED_EVERY, nd >= SCHED_MIN_ND)
     L.append("#undef OV_SC")
     L.append("#undef OV_ISC")
     L.append("  }")
