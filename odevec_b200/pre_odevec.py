@@ -732,8 +732,8 @@ def _reduce_lines(lines: List[str], kmap: Dict[int, int]) -> List[str]:
 # SCHED_EVERY_RHS species of the right-hand side): their code is long enough
 # that the compiler's hoisted loads otherwise spill.
 SCHED_MIN_ND = 33
-SCHED_EVERY = 32
-SCHED_EVERY_RHS = 8
+SCHED_EVERY = 16
+SCHED_EVERY_RHS = 4
 
 
 def _fenced(lines: List[str], every: int, on: bool, indent: str = "    ") -> List[str]:
