@@ -210,6 +210,10 @@ template <> struct StageCfg<17> { static constexpr int SHM = 2; static constexpr
    in shared memory (networks above 32 solver species) */
 template <> struct StageCfg<18> { static constexpr int SHM = 4; static constexpr bool SOFT = true;  static constexpr int BS = 256, MINB = 1, REFILL = 16, PERIOD = 4; };
 template <> struct StageCfg<19> { static constexpr int SHM = 4; static constexpr bool SOFT = true;  static constexpr int BS = 384, MINB = 1, REFILL = 16, PERIOD = 4; };
+/* staging 3's shape (three 128-thread blocks per SM, so that blocks of
+   several solves share an SM) with the state vector in shared memory
+   (networks above 32 solver species) */
+template <> struct StageCfg<20> { static constexpr int SHM = 4; static constexpr bool SOFT = false; static constexpr int BS = 128, MINB = 3, REFILL = 16, PERIOD = 4; };
 
 /* Soft lockstep.  The warps of a block wait for each other at the top of
    every trip of the cell loop, so they run the same phase code at the same
@@ -1475,9 +1479,10 @@ constexpr bool hist_fits_max()
    16 or 8 lanes per cell (wpc_kernel.cuh, as 7); 15, 16 = as 8 in one block
    of 256 or 512 (networks above 32 solver species); 17 = as 12 refilling on
    every 32nd trip; 18, 19 = as 8 in one block of 256 or 384 with the state
-   vector in shared memory (networks above 32 solver species).  With per-cell control stagings 2-6 and 8-16 refill idle
+   vector in shared memory, 20 = as 3 with the state vector in shared memory
+   (18-20: networks above 32 solver species).  With per-cell control stagings 2-6 and 8-16 refill idle
    lanes on every 16th trip, 17 on every 32nd, staging 1 on every trip.
-   Stages 2-19 exist for per-cell control (G = 1). */
+   Stages 2-20 exist for per-cell control (G = 1). */
 #define OV_STAGE_CASE(NET, LU, ST)                                                               \
     if (stage == ST)                                                                             \
         return launch<NET, 1, LU, ST>(a, block, grid, s);
@@ -1519,6 +1524,9 @@ constexpr bool hist_fits_max()
                 OV_STAGE_CASE(NET, double, 16)                                               \
                 if constexpr (y_fits<NET, 256>()) {                                          \
                     OV_STAGE_CASE(NET, double, 18)                                           \
+                }                                                                            \
+                if constexpr (y_fits<NET, 128>()) {                                          \
+                    OV_STAGE_CASE(NET, double, 20)                                           \
                 }                                                                            \
                 if constexpr (y_fits<NET, 384>()) {                                          \
                     OV_STAGE_CASE(NET, double, 19)                                           \
@@ -1566,6 +1574,9 @@ constexpr bool hist_fits_max()
                     OV_STAGE_CASE(NET, float, 16)                                            \
                     if constexpr (y_fits<NET, 256>()) {                                      \
                         OV_STAGE_CASE(NET, float, 18)                                        \
+                    }                                                                        \
+                    if constexpr (y_fits<NET, 128>()) {                                      \
+                        OV_STAGE_CASE(NET, float, 20)                                        \
                     }                                                                        \
                     if constexpr (y_fits<NET, 384>()) {                                      \
                         OV_STAGE_CASE(NET, float, 19)                                        \

@@ -230,12 +230,21 @@ class GpuBackend:
             self._zero = torch.zeros(1, dtype=torch.int32).pin_memory()
         self.sms = torch.cuda.get_device_properties(device).multi_processor_count
 
+    def staging_for(self, network: str) -> int:
+        """The launch shape of a request's solves: staging 3's shape for all,
+        with the state vector in shared memory (staging 20) for networks
+        above 32 solver species, whose long code otherwise spills it."""
+        if self.staging != 3:
+            return self.staging
+        nd = (self.S.workspace_doubles(network) - 12) // 8  # 8 doubles per solver species + 12
+        return 20 if nd > 32 else 3
+
     def _solver(self, r: Request):
         # one solver handle per request: each owns its cell counter, so
         # concurrent launches on different streams never share one
         ode = self.S.Odevec(r.network, RelativeTolerance=r.rtol, AbsoluteTolerance=r.atol,
                             MinimalTimestep=r.dt_min, nvector=1, precision=self.precision,
-                            raise_on_failure=False, staging=self.staging)
+                            raise_on_failure=False, staging=self.staging_for(r.network))
         self.S.InitOdevec(ode)
         return ode
 

@@ -308,7 +308,7 @@ def test_syn64_stagings_bit_exact(gpu_lib, oracle):
     wl = W.syn64(ncells=700)
     o = run_oracle(oracle, wl)
     assert np.all(o[3] == 0)
-    for staging in (1, 3, 6, 8, 15, 16, 18, 19):
+    for staging in (1, 3, 6, 8, 15, 16, 18, 19, 20):
         assert_bitwise(run_gpu(gpu_lib, wl, "fp64", staging=staging), o, "SYN64 staging %d" % staging)
 
 

@@ -146,3 +146,18 @@ def test_water_fill_shares():
     assert water_fill({5: 3}, 444) == {5: 3}
     s = water_fill({i: 10 * i + 1 for i in range(20)}, 444)
     assert sum(s.values()) <= 444 and all(s[i] <= 10 * i + 1 for i in s)
+
+
+def test_staging_for_large_networks():
+    """Requests of networks above 32 solver species run staging 3's shape
+    with the state vector in shared memory (staging 20); others staging 3;
+    an explicit staging is kept."""
+    import types
+    from odevec_b200 import solver
+    from odevec_b200.serving import GpuBackend
+    be = types.SimpleNamespace(staging=3, S=solver)
+    assert GpuBackend.staging_for(be, "SYN64_CSC_CMK") == 20
+    assert GpuBackend.staging_for(be, "PRIMORDIAL_CSC_FF") == 3
+    assert GpuBackend.staging_for(be, "ROBER_DENSE_NONE") == 3
+    be.staging = 8
+    assert GpuBackend.staging_for(be, "SYN64_CSC_CMK") == 8
