@@ -81,7 +81,7 @@ typedef struct odevec_opts {
        waiting cells of a warp together once jac_batch / ss_batch of its 32
        cells wait, no other cell can progress, or a cell has waited max_wait
        iterations.  0: defaults (24, 24, 8); 1, 1, -1 runs each cell's block
-       at once.  Stagings 2-20 ignore them: they run the two blocks on fixed
+       at once.  Stagings 2-21 ignore them: they run the two blocks on fixed
        trips (every 4th trip each, the same trips in all warps of a block). */
     int32_t jac_batch;
     int32_t ss_batch;
@@ -105,7 +105,9 @@ typedef struct odevec_opts {
        species); 17 = as 12 refilling on every 32nd trip; 18, 19 = as 8 in
        one block of 256 or 384 threads with the state vector in shared
        memory, 20 = as 3 with the state vector in shared memory (18-20:
-       networks above 32 solver species) (2-20: per-cell control only).  In 2-6 and 8-16 idle lanes take new cells on every
+       networks above 32 solver species); 21 = as 3 with the history in
+       shared memory and each block in soft lockstep (up to 12 solver
+       species) (2-21: per-cell control only).  In 2-6 and 8-16 idle lanes take new cells on every
        16th trip of the cell loop (17: every 32nd), so cells are set up
        several at a time (in 8-12 and 15-17 in all warps of a block at
        once); staging 1 refills on every trip.  block_threads (a multiple of 32 up to

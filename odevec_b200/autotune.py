@@ -29,7 +29,7 @@ from typing import Callable, Dict, List, Optional, Tuple
 HERE = os.path.dirname(os.path.abspath(__file__))
 TABLE = os.path.join(HERE, "tuning.json")
 
-STAGINGS = (1, 2, 3, 4, 6, 7, 8, 9, 10, 11, 12, 13, 14, 15, 16, 17, 18, 19, 20)
+STAGINGS = (1, 2, 3, 4, 6, 7, 8, 9, 10, 11, 12, 13, 14, 15, 16, 17, 18, 19, 20, 21)
 FP32_STAGINGS = (5,)
 BATCHES = ((24, 24, 8), (16, 16, 4), (32, 32, 16), (8, 8, 4), (4, 4, 2), (2, 2, 1), (1, 1, -1))
 # the batch options act on staging 1 only; the other stagings run the Jacobian

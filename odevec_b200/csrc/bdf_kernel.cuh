@@ -214,6 +214,10 @@ template <> struct StageCfg<19> { static constexpr int SHM = 4; static constexpr
    several solves share an SM) with the state vector in shared memory
    (networks above 32 solver species) */
 template <> struct StageCfg<20> { static constexpr int SHM = 4; static constexpr bool SOFT = false; static constexpr int BS = 128, MINB = 3, REFILL = 16, PERIOD = 4; };
+/* staging 3's shape with the history in shared memory and the block's four
+   warps in soft lockstep (where three blocks' histories fit an SM: up to 12
+   solver species) */
+template <> struct StageCfg<21> { static constexpr int SHM = 2; static constexpr bool SOFT = true;  static constexpr int BS = 128, MINB = 3, REFILL = 16, PERIOD = 4; };
 
 /* Soft lockstep.  The warps of a block wait for each other at the top of
    every trip of the cell loop, so they run the same phase code at the same
@@ -1447,6 +1451,13 @@ constexpr bool hist_fits()
     return Staging<Net, double, 2, BS>::smem_bytes <= 200 * 1024;
 }
 
+/* the histories of three blocks of 128 within an SM's shared memory */
+template <class Net>
+constexpr bool hist_fits_3x128()
+{
+    return 3 * (Staging<Net, double, 2, 128>::smem_bytes + 1024) <= 228 * 1024;
+}
+
 /* the state vectors of a block within the 227 KB a block may hold */
 template <class Net, int BS>
 constexpr bool y_fits()
@@ -1480,9 +1491,10 @@ constexpr bool hist_fits_max()
    of 256 or 512 (networks above 32 solver species); 17 = as 12 refilling on
    every 32nd trip; 18, 19 = as 8 in one block of 256 or 384 with the state
    vector in shared memory, 20 = as 3 with the state vector in shared memory
-   (18-20: networks above 32 solver species).  With per-cell control stagings 2-6 and 8-16 refill idle
+   (18-20: networks above 32 solver species); 21 = as 3 with the history in
+   shared memory and the block in soft lockstep (up to 12 solver species).  With per-cell control stagings 2-6 and 8-16 refill idle
    lanes on every 16th trip, 17 on every 32nd, staging 1 on every trip.
-   Stages 2-20 exist for per-cell control (G = 1). */
+   Stages 2-21 exist for per-cell control (G = 1). */
 #define OV_STAGE_CASE(NET, LU, ST)                                                               \
     if (stage == ST)                                                                             \
         return launch<NET, 1, LU, ST>(a, block, grid, s);
@@ -1531,6 +1543,9 @@ constexpr bool hist_fits_max()
                 if constexpr (y_fits<NET, 384>()) {                                          \
                     OV_STAGE_CASE(NET, double, 19)                                           \
                 }                                                                            \
+            }                                                                                \
+            if constexpr (hist_fits_3x128<NET>()) {                                          \
+                OV_STAGE_CASE(NET, double, 21)                                               \
             }                                                                                \
             if constexpr (hist_fits<NET, 256>()) {                                               \
                 OV_STAGE_CASE(NET, double, 9)                                                    \
@@ -1581,6 +1596,9 @@ constexpr bool hist_fits_max()
                     if constexpr (y_fits<NET, 384>()) {                                      \
                         OV_STAGE_CASE(NET, float, 19)                                        \
                     }                                                                        \
+                }                                                                            \
+                if constexpr (hist_fits_3x128<NET>()) {                                      \
+                    OV_STAGE_CASE(NET, float, 21)                                            \
                 }                                                                            \
                 if constexpr (hist_fits<NET, 256>()) {                                           \
                     OV_STAGE_CASE(NET, float, 9)                                                 \

@@ -304,8 +304,8 @@ static int32_t resolve_opts(const NetEntry& e, const odevec_opts* in, odevec_opt
         o.max_wait = o.max_wait < 0 ? 0 : 8;
     if (o.jac_batch > 32 || o.ss_batch > 32)
         return fail(OV_API_EINVAL, "jac_batch and ss_batch must be <= 32");
-    if (o.staging < 0 || o.staging > 20)
-        return fail(OV_API_EINVAL, "staging must be 0..20");
+    if (o.staging < 0 || o.staging > 21)
+        return fail(OV_API_EINVAL, "staging must be 0..21");
     if (o.block_threads < 0 || o.block_threads > 128 || o.block_threads % 32)
         return fail(OV_API_EINVAL, "block_threads must be 32, 64, 96 or 128 (0: automatic)");
     if (o.grid_blocks < 0)

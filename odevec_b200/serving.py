@@ -231,13 +231,17 @@ class GpuBackend:
         self.sms = torch.cuda.get_device_properties(device).multi_processor_count
 
     def staging_for(self, network: str) -> int:
-        """The launch shape of a request's solves: staging 3's shape for all,
-        with the state vector in shared memory (staging 20) for networks
-        above 32 solver species, whose long code otherwise spills it."""
+        """The launch shape of a request's solves: staging 3's shape for all
+        (three 128-thread blocks per SM), with the history in shared memory
+        and soft lockstep (staging 21) where three blocks' histories fit an
+        SM (up to 12 solver species), with the state vector in shared memory
+        (staging 20) for networks above 32 solver species."""
         if self.staging != 3:
             return self.staging
         nd = (self.S.workspace_doubles(network) - 12) // 8  # 8 doubles per solver species + 12
-        return 20 if nd > 32 else 3
+        if nd > 32:
+            return 20
+        return 21 if nd <= 12 else 3
 
     def _solver(self, r: Request):
         # one solver handle per request: each owns its cell counter, so

@@ -140,11 +140,11 @@ def network_info(tag):
 
 # resident blocks per SM of each staging (block size x blocks: the launch
 # shape the kernel is compiled for; 0 = the library's automatic choice, 3)
-BLOCKS_PER_SM = {0: 3, 1: 2, 2: 1, 3: 3, 4: 4, 5: 1, 6: 1, 7: 3, 8: 1, 9: 1, 10: 1, 11: 1, 12: 1, 13: 2, 14: 1, 15: 1, 16: 1, 17: 1, 18: 1, 19: 1, 20: 3}
+BLOCKS_PER_SM = {0: 3, 1: 2, 2: 1, 3: 3, 4: 4, 5: 1, 6: 1, 7: 3, 8: 1, 9: 1, 10: 1, 11: 1, 12: 1, 13: 2, 14: 1, 15: 1, 16: 1, 17: 1, 18: 1, 19: 1, 20: 3, 21: 3}
 # cells one block of each staging holds at a time (thread per cell: the block
 # size; 32, 16 or 8 lanes per cell: 8, 16 or 32 cells in 8 warps)
 CELLS_PER_BLOCK = {0: 128, 1: 128, 2: 128, 3: 128, 4: 128, 5: 192, 6: 384, 7: 8, 8: 384, 9: 256, 10: 320, 11: 192,
-                   12: 384, 13: 16, 14: 32, 15: 256, 16: 512, 17: 384, 18: 256, 19: 384, 20: 128}
+                   12: 384, 13: 16, 14: 32, 15: 256, 16: 512, 17: 384, 18: 256, 19: 384, 20: 128, 21: 128}
 
 
 class Odevec:

@@ -63,7 +63,7 @@ def test_init_argument_errors(L):
     assert L.odevec_init(b"ROBER_DENSE_NONE", 10, ctypes.byref(_opts(precision=9)), ctypes.byref(h)) == -1
     assert L.odevec_init(b"ROBER_DENSE_NONE", 10, ctypes.byref(_opts(block_threads=256)),
                          ctypes.byref(h)) == -1
-    assert L.odevec_init(b"ROBER_DENSE_NONE", 10, ctypes.byref(_opts(staging=21)), ctypes.byref(h)) == -1
+    assert L.odevec_init(b"ROBER_DENSE_NONE", 10, ctypes.byref(_opts(staging=22)), ctypes.byref(h)) == -1
     assert L.odevec_init(b"ROBER_DENSE_NONE", 10, ctypes.byref(_opts()), None) == -1
 
 

@@ -10,7 +10,7 @@ from odevec_b200 import autotune as A
 
 
 def test_search_picks_fastest_and_skips_uncompiled():
-    cost = {1: 3.0, 2: None, 3: 2.0, 4: 2.5, 6: 1.5, 7: 1.9, 8: 1.7, 9: 1.8, 10: 1.9, 11: 2.2, 12: 1.6, 13: 2.0, 14: 2.1, 15: 1.8, 16: 1.9, 17: 1.65, 18: 1.85, 19: 1.95, 20: 2.05, 5: 1.0}
+    cost = {1: 3.0, 2: None, 3: 2.0, 4: 2.5, 6: 1.5, 7: 1.9, 8: 1.7, 9: 1.8, 10: 1.9, 11: 2.2, 12: 1.6, 13: 2.0, 14: 2.1, 15: 1.8, 16: 1.9, 17: 1.65, 18: 1.85, 19: 1.95, 20: 2.05, 21: 2.1, 5: 1.0}
 
     def timer(cfg):
         base = cost[cfg["staging"]]

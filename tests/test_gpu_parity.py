@@ -104,7 +104,7 @@ def test_scheduling_does_not_change_results(gpu_lib, precision):
     # every staging (6: staging 3's thread-local kernel in one 384-thread
     # block per SM; 8-12: soft lockstep), with the default batches and with
     # per-cell blocks
-    for staging in (1, 2, 3, 4, 6, 8, 9, 10, 12, 17) + ((5, 11) if precision == "fp32_lu" else ()):
+    for staging in (1, 2, 3, 4, 6, 8, 9, 10, 12, 17, 21) + ((5, 11) if precision == "fp32_lu" else ()):
         for batch in [(0, 0, 0), (1, 1, -1)]:
             g = run_gpu(gpu_lib, wl, precision, batch=batch, staging=staging)
             assert_bitwise(g, ref, "staging %d batch %s" % (staging, batch))

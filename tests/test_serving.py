@@ -149,15 +149,15 @@ def test_water_fill_shares():
 
 
 def test_staging_for_large_networks():
-    """Requests of networks above 32 solver species run staging 3's shape
-    with the state vector in shared memory (staging 20); others staging 3;
-    an explicit staging is kept."""
+    """Requests run staging 3's shape: with the state vector in shared memory
+    above 32 solver species (staging 20), with the history in shared memory
+    and soft lockstep up to 12 (staging 21); an explicit staging is kept."""
     import types
     from odevec_b200 import solver
     from odevec_b200.serving import GpuBackend
     be = types.SimpleNamespace(staging=3, S=solver)
     assert GpuBackend.staging_for(be, "SYN64_CSC_CMK") == 20
-    assert GpuBackend.staging_for(be, "PRIMORDIAL_CSC_FF") == 3
-    assert GpuBackend.staging_for(be, "ROBER_DENSE_NONE") == 3
+    assert GpuBackend.staging_for(be, "PRIMORDIAL_CSC_FF") == 21
+    assert GpuBackend.staging_for(be, "ROBER_DENSE_NONE") == 21
     be.staging = 8
     assert GpuBackend.staging_for(be, "SYN64_CSC_CMK") == 8
