@@ -209,6 +209,8 @@ class GpuBackend:
         # of up to three requests share an SM.  The single-solve optimum (one
         # block per SM holding its shared memory) would leave SMs to a single
         # request and most of the device idle under many small requests.
+        # staging 3 selects that shape per network (staging_for); any other
+        # value is used for every request as given.
         self.staging = staging
         # chunk_cells > 0: a step of a larger request is launched as ranges of
         # at most this many cells, one after another on its stream, so that a
