@@ -257,7 +257,8 @@ const char* odevec_last_error(void);
    (OV_API_EUNSUPPORTED if none does).  The kernel gives each job a share of
    the blocks in proportion to its cells, and a block whose job has no cells
    left takes cells of the others, so the networks share the device for the
-   whole launch.  Failed FP32-LU cells are not solved again (see
+   whole launch; each job's cells are visited longest t_stop - t first, as
+   in odevec_solve.  Failed FP32-LU cells are not solved again (see
    no_escalation).  Asynchronous on stream. */
 #define OV_MULTI_MAX_JOBS 8
 typedef struct odevec_job {
